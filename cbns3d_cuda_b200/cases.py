@@ -1,0 +1,322 @@
+"""Synthetic test cases and the reference's file formats.
+
+Formats (kept byte-compatible with the reference):
+  * ASCII Plot3D single block: "IM JM KM" then x, y, z with i fastest
+    (src/Block3d.cpp:151-202);
+  * binary checkpoint: float64 t_cur, uint32 IM_G, JM_G, KM_G, then the AoS
+    ghosted state Q[n + 5*(i + IM_G*(j + JM_G*k))] (src/Block3d.cpp:411-474);
+  * input.txt: the 17 positional values python/parser_ini.py writes from an
+    .ini (src/Block3d.cpp:33-93).
+
+Cases (grids in the reference's non-dimensional units: rho_inf = 1, |u_inf| = 1,
+p_inf = 1/(gamma M^2)).  Initial states are evaluated at every node of the
+ghosted box, the grid being extended linearly into the ghost layers.
+"""
+from __future__ import annotations
+
+import configparser
+import dataclasses
+import struct
+from pathlib import Path
+
+import numpy as np
+
+NG = 2
+NEQ = 5
+
+INPUT_ORDER = ["grid_fname", "checkpoint_fname", "CFL", "t_cur", "t_end", "Pr", "Pr_t", "gamma", "Mach", "Re",
+               "T_inf", "angle_attack", "nstep_max", "checkpoint_freq", "i_begin", "i_end", "is_restart"]
+
+
+# ---------------------------------------------------------------- file formats
+def write_plot3d(path, x, y, z):
+    KM, JM, IM = x.shape
+    with open(path, "w") as f:
+        f.write(f"{IM} {JM} {KM}\n")
+        for a in (x, y, z):
+            np.ascontiguousarray(a, dtype=np.float64).reshape(-1).tofile(f, sep="\n", format="%.17g")
+            f.write("\n")
+
+
+def read_plot3d(path):
+    with open(path) as f:
+        IM, JM, KM = (int(v) for v in f.readline().split())
+        data = np.fromfile(f, sep=" ", count=3 * IM * JM * KM)
+    n = IM * JM * KM
+    return [data[m * n:(m + 1) * n].reshape(KM, JM, IM) for m in range(3)]
+
+
+def write_checkpoint(path, t_cur, Q):
+    """Q: (KM_G, JM_G, IM_G, 5) float64."""
+    KG, JG, IG, _ = Q.shape
+    with open(path, "wb") as f:
+        f.write(struct.pack("<d3I", float(t_cur), IG, JG, KG))
+        f.write(np.ascontiguousarray(Q, dtype="<f8").tobytes())
+
+
+def read_checkpoint(path):
+    with open(path, "rb") as f:
+        t, IG, JG, KG = struct.unpack("<d3I", f.read(20))
+        Q = np.frombuffer(f.read(), dtype="<f8").reshape(KG, JG, IG, NEQ).copy()
+    return t, Q
+
+
+def write_input(path, **v):
+    missing = [k for k in INPUT_ORDER if k not in v]
+    if missing:
+        raise ValueError(f"input.txt needs {missing}")
+    with open(path, "w") as f:
+        for k in INPUT_ORDER:
+            val = v[k]
+            if isinstance(val, bool):
+                val = int(val)
+            f.write(f"{val!r}\n" if isinstance(val, float) else f"{val}\n")
+
+
+def parse_ini(ini_path, out_path="input.txt"):
+    """The reference's python/parser_ini.py: every value of the .ini, in
+    section order, one per line."""
+    cfg = configparser.ConfigParser()
+    cfg.optionxform = str
+    cfg.read(ini_path)
+    with open(out_path, "w") as f:
+        for sec in cfg.sections():
+            for key in cfg[sec]:
+                f.write(cfg[sec][key])
+                f.write("\n")
+
+
+# ---------------------------------------------------------------- helpers
+def ghost_extend(a):
+    """Extend a (KM, JM, IM) coordinate array by NG layers on every side by
+    linear extrapolation."""
+    return np.pad(a, NG, mode="reflect", reflect_type="odd")
+
+
+def conservative(rho, u, v, w, p, gamma):
+    """Primitive -> AoS conservative (src/conservative_kernel.cu:13-48)."""
+    E = p / (gamma - 1.0) + 0.5 * rho * (u * u + v * v + w * w)
+    return np.stack([rho, rho * u, rho * v, rho * w, E], axis=-1)
+
+
+def primitive(Q, gamma):
+    r = Q[..., 0]
+    u, v, w = Q[..., 1] / r, Q[..., 2] / r, Q[..., 3] / r
+    p = (gamma - 1.0) * (Q[..., 4] - 0.5 * r * (u * u + v * v + w * w))
+    return r, u, v, w, p
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    params: dict            # keyword arguments of cbns3d_cuda_b200.make_params
+    Q0: np.ndarray | None   # ghosted AoS initial state, or None for the free-stream start
+    t_end: float
+    nsteps: int
+
+    @property
+    def shape(self):
+        KM, JM, IM = self.x.shape
+        return IM, JM, KM
+
+    def write(self, workdir, nsteps=None, checkpoint_freq=None, grid_name="grid.xyz",
+              checkpoint_name="checkpoint.dat"):
+        """Write grid, checkpoint and input.txt for the reference/driver executables."""
+        wd = Path(workdir)
+        wd.mkdir(parents=True, exist_ok=True)
+        write_plot3d(wd / grid_name, self.x, self.y, self.z)
+        if self.Q0 is not None:
+            write_checkpoint(wd / checkpoint_name, 0.0, self.Q0)
+        n = self.nsteps if nsteps is None else nsteps
+        p = self.params
+        write_input(wd / "input.txt", grid_fname=grid_name, checkpoint_fname=checkpoint_name,
+                    CFL=float(p.get("CFL", 0.5)), t_cur=0.0, t_end=float(self.t_end), Pr=float(p.get("Pr", 0.72)),
+                    Pr_t=float(p.get("Pr_t", 0.9)), gamma=float(p.get("gamma", 1.4)), Mach=float(p["Mach"]),
+                    Re=float(p.get("Re", 1.0e4)), T_inf=float(p.get("T_inf", 288.15)),
+                    angle_attack=float(p.get("angle_attack", 0.0)), nstep_max=int(n),
+                    checkpoint_freq=int(checkpoint_freq if checkpoint_freq else max(n, 1)),
+                    i_begin=int(p.get("i_begin", 1)), i_end=int(p.get("i_end", 0)),
+                    is_restart=0 if self.Q0 is not None else 1)
+        return wd
+
+
+# ---------------------------------------------------------------- grids
+def perturbed_box(IM, JM, KM, L=(10.0, 5.0, 2.5), amp=0.1):
+    """x = i dx + amp sin(2 pi j/JM) sin(2 pi k/KM), and the analogous
+    perturbation of y (in i, k) and z (in i, j)."""
+    k, j, i = np.meshgrid(np.arange(KM), np.arange(JM), np.arange(IM), indexing="ij")
+    dx, dy, dz = L[0] / (IM - 1), L[1] / (JM - 1), L[2] / (KM - 1)
+    tp = 2.0 * np.pi
+    x = i * dx + amp * np.sin(tp * j / JM) * np.sin(tp * k / KM)
+    y = j * dy + amp * np.sin(tp * i / IM) * np.sin(tp * k / KM)
+    z = k * dz + amp * np.sin(tp * i / IM) * np.sin(tp * j / JM)
+    return x.astype(np.float64), y.astype(np.float64), z.astype(np.float64)
+
+
+def stretched_skewed_box(IM, JM, KM, half=(1.0, 1.0, 1.0), stretch=1.5, skew=0.05):
+    """Box [-h, h]^3 clustered toward the centre by the inverse-tanh map
+    x = atanh(tanh(s) (2 xi - 1)) / s, then skewed by
+    x += skew * h * sin(pi y/h) sin(pi z/h) (and cyclically for y, z)."""
+    def axis(n, h):
+        e = np.linspace(-1.0, 1.0, n)
+        return h * np.arctanh(np.tanh(stretch) * e) / stretch
+    ax = axis(IM, half[0])
+    ay = axis(JM, half[1])
+    az = axis(KM, half[2])
+    z0, y0, x0 = np.meshgrid(az, ay, ax, indexing="ij")
+    hx, hy, hz = half
+    x = x0 + skew * hx * np.sin(np.pi * y0 / hy) * np.sin(np.pi * z0 / hz)
+    y = y0 + skew * hy * np.sin(np.pi * z0 / hz) * np.sin(np.pi * x0 / hx)
+    z = z0 + skew * hz * np.sin(np.pi * x0 / hx) * np.sin(np.pi * y0 / hy)
+    return x, y, z
+
+
+def skewed_channel(IM, JM, KM, L=(1.0, 1.0, 0.5), skew=0.05):
+    """Uniform box [0,Lx]x[0,Ly]x[0,Lz] with a 5% sinusoidal skew."""
+    k, j, i = np.meshgrid(np.linspace(0, 1, KM), np.linspace(0, 1, JM), np.linspace(0, 1, IM), indexing="ij")
+    x = L[0] * (i + skew * np.sin(2 * np.pi * j) * np.sin(np.pi * k))
+    y = L[1] * (j + skew * np.sin(2 * np.pi * i) * np.sin(np.pi * k))
+    z = L[2] * (k + skew * np.sin(np.pi * i) * np.sin(np.pi * j))
+    return x, y, z
+
+
+def naca0012_ogrid(IM, JM, KM, first=1.0e-5, far=20.0, span=0.1):
+    """O-grid around a closed-trailing-edge NACA 0012 of unit chord.  i runs from
+    just below the trailing edge along the lower, then the upper surface
+    (parameter angles offset by half a cell so i = 0 and IM-1 are distinct points
+    either side of the edge); j runs outward along straight surface normals with
+    geometric spacing, first cell `first` chords, last point `far` chords out;
+    k is spanwise.  The profile is convex, so the normals never cross and the
+    grid is right-handed (J > 0)."""
+    dth = 2.0 * np.pi / IM
+    th = np.linspace(0.5 * dth, 2.0 * np.pi - 0.5 * dth, IM)
+
+    def surf(t):
+        xs = 0.5 * (1.0 + np.cos(t))
+        yt = 5 * 0.12 * (0.2969 * np.sqrt(xs) - 0.1260 * xs - 0.3516 * xs ** 2 + 0.2843 * xs ** 3
+                         - 0.1036 * xs ** 4)
+        return xs, np.where(t <= np.pi, -yt, yt)
+
+    xs, ys = surf(th)
+    h = 1e-6
+    xa, ya = surf(th - h)
+    xb, yb = surf(th + h)
+    tx, ty = xb - xa, yb - ya
+    nrm = np.hypot(tx, ty)
+    nx, ny = -ty / nrm, tx / nrm  # outward normal for this orientation
+    # geometric ratio r with first * (r^(JM-1) - 1)/(r - 1) = far
+    lo, hi = 1.0 + 1e-9, 2.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if first * (r ** (JM - 1) - 1) / (r - 1) > far:
+            hi = r
+        else:
+            lo = r
+    d = first * (r ** np.arange(JM) - 1) / (r - 1)
+    x2 = xs[None, :] + d[:, None] * nx[None, :]
+    y2 = ys[None, :] + d[:, None] * ny[None, :]
+    zk = np.linspace(0.0, span, KM)
+    x = np.broadcast_to(x2, (KM, JM, IM)).copy()
+    y = np.broadcast_to(y2, (KM, JM, IM)).copy()
+    z = np.broadcast_to(zk[:, None, None], (KM, JM, IM)).copy()
+    return x, y, z, r
+
+
+# ---------------------------------------------------------------- initial states
+def isentropic_vortex(xg, yg, Mach, beta, xc, yc, R, gamma=1.4, u_dir=(1.0, 0.0)):
+    """Isentropic vortex of strength beta (in units of the free-stream sound
+    speed) and Gaussian radius R advected by a free stream of Mach number Mach,
+    returned in the reference's units (|u_inf| = 1, p_inf = 1/(gamma M^2))."""
+    dx, dy = (xg - xc) / R, (yg - yc) / R
+    r2 = dx * dx + dy * dy
+    f = np.exp(0.5 * (1.0 - r2))
+    U = Mach * np.sqrt(gamma)  # free-stream speed in sound-speed units (c_inf = sqrt(gamma), p_inf = rho_inf = 1)
+    ua = U * u_dir[0] - beta / (2 * np.pi) * dy * f
+    va = U * u_dir[1] + beta / (2 * np.pi) * dx * f
+    T = 1.0 - (gamma - 1.0) * beta ** 2 / (8.0 * gamma * np.pi ** 2) * np.exp(1.0 - r2)
+    rho = T ** (1.0 / (gamma - 1.0))
+    p = rho * T
+    return rho, ua / U, va / U, np.zeros_like(rho), p / (U * U)
+
+
+def case_vortex(IM=64, JM=32, KM=16, nsteps=100, CFL=0.5, Mach=0.5):
+    """isentropic vortex (strength 5, centre (3, 2.5), radius 1) at
+    Mach 0.5 on the perturbed 10 x 5 x 2.5 box; 100 steps at CFL 0.5.  Reference
+    boundary mode: i faces pressure-reset extrapolation, j faces held at the
+    initial state (i_begin = 1, i_end = 0), k faces zero-gradient."""
+    x, y, z = perturbed_box(IM, JM, KM)
+    xg, yg = ghost_extend(x), ghost_extend(y)
+    g = 1.4
+    rho, u, v, w, p = isentropic_vortex(xg, yg, Mach, 5.0, 3.0, 2.5, 1.0, g)
+    Q = conservative(rho, u, v, w, p, g)
+    params = dict(CFL=CFL, Mach=Mach, gamma=g, i_begin=1, i_end=0, Re=1.0e4, Pr=0.72, T_inf=288.15)
+    return Case("vortex", x, y, z, params, Q, t_end=100.0, nsteps=nsteps)
+
+
+def case_naca(IM=384, JM=128, KM=4, nsteps=2000, CFL=0.8):
+    """viscous NACA 0012 O-grid, M 0.8, AoA 1.25 deg, Re 5e4, Pr 0.72,
+    Sutherland with T_inf = 288.15 K, free-stream start.  Reference boundary
+    mode: wall on the whole j = 0 face (i_begin = 1, i_end = IM)."""
+    x, y, z, _ = naca0012_ogrid(IM, JM, KM)
+    params = dict(CFL=CFL, Mach=0.8, angle_attack=1.25, Re=5.0e4, Pr=0.72, Pr_t=0.9, T_inf=288.15, gamma=1.4,
+                  i_begin=1, i_end=IM, viscous=True)
+    return Case("naca", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)
+
+
+def case_blast(IM=384, JM=384, KM=384, t_end=0.05, CFL=0.5):
+    """spherical blast (p = 10 inside r < 0.1, 0.1 outside, rho = 1,
+    at rest) on the centre-clustered (stretch 1.5), 5%-skewed [-1,1]^3 box.
+    Mach is chosen so that p_inf = 1/(gamma M^2) = 0.1, the ambient pressure
+    the i-face boundary resets to."""
+    x, y, z = stretched_skewed_box(IM, JM, KM)
+    xg, yg, zg = ghost_extend(x), ghost_extend(y), ghost_extend(z)
+    g = 1.4
+    r2 = xg * xg + yg * yg + zg * zg
+    p = np.where(r2 < 0.01, 10.0, 0.1)
+    rho = np.ones_like(p)
+    zero = np.zeros_like(p)
+    Q = conservative(rho, zero, zero, zero, p, g)
+    Mach = float(np.sqrt(1.0 / (g * 0.1)))
+    params = dict(CFL=CFL, Mach=Mach, gamma=g, i_begin=1, i_end=0)
+    return Case("blast", x, y, z, params, Q, t_end=t_end, nsteps=100000)
+
+
+def case_shock_vortex(IM=256, JM=256, KM=128, nsteps=100, CFL=0.5, Ms=1.2, eps=0.3, rc=0.075):
+    """a stationary Mach 1.2 normal shock at x = 0.5 of the 5%-skewed
+    [0,1]x[0,1]x[0,0.5] box, with an isentropic vortex (strength 0.3, radius
+    0.075, centre (0.25, 0.5)) in the upstream flow moving into it."""
+    x, y, z = skewed_channel(IM, JM, KM)
+    xg, yg = ghost_extend(x), ghost_extend(y)
+    g = 1.4
+    # upstream (reference units): rho = 1, u = 1, p = 1/(gamma Ms^2)
+    p1 = 1.0 / (g * Ms * Ms)
+    r21 = ((g + 1) * Ms * Ms) / ((g - 1) * Ms * Ms + 2)
+    p21 = 1 + 2 * g / (g + 1) * (Ms * Ms - 1)
+    rho2, u2, p2 = r21, 1.0 / r21, p1 * p21
+    # vortex: u_theta = eps * c1 * tau * exp(a (1 - tau^2)), Jiang & Shu form, a = 0.204
+    a = 0.204
+    xc, yc = 0.25, 0.5
+    dx, dy = xg - xc, yg - yc
+    rr = np.sqrt(dx * dx + dy * dy)
+    tau = rr / rc
+    c1 = np.sqrt(g * p1 / 1.0)
+    ut = eps * c1 * tau * np.exp(a * (1.0 - tau * tau))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        sn = np.where(rr > 0, dy / rr, 0.0)
+        cs = np.where(rr > 0, dx / rr, 0.0)
+    T1 = p1 / 1.0
+    T = T1 - (g - 1) * (eps * c1) ** 2 / (4 * a * g) * np.exp(2 * a * (1 - tau * tau)) * (1.0 / 1.0)
+    rho_v = (T / T1) ** (1 / (g - 1))
+    p_v = p1 * (T / T1) ** (g / (g - 1))
+    up = xg < 0.5
+    rho = np.where(up, rho_v, rho2)
+    u = np.where(up, 1.0 - ut * sn, u2)
+    v = np.where(up, ut * cs, 0.0)
+    w = np.zeros_like(rho)
+    p = np.where(up, p_v, p2)
+    Q = conservative(rho, u, v, w, p, g)
+    params = dict(CFL=CFL, Mach=Ms, gamma=g, i_begin=1, i_end=0)
+    return Case("shock_vortex", x, y, z, params, Q, t_end=1.0e6, nsteps=nsteps)

@@ -1,0 +1,740 @@
+// abi.cu - the extern "C" entry points declared in include/cbns_b200.h.
+//
+// State buffers.  The reference keeps two conservative arrays, Q and Q_p, and
+// updates Q_p in place in stage 2 (src/runge_kutta_kernel.cu:72-73), which a
+// fused stencil+update kernel cannot do.  The context therefore owns three
+// physical buffers and maps the reference's logical Q and Q_p (and a spare) onto
+// them; a stage whose output would overwrite its own stencil source writes the
+// spare and the two roles swap.  Cells that no kernel ever writes (far-field
+// ghosts held at their initial values) are identical in all three buffers
+// because every state upload or initialisation fills all three.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "../../include/cbns_b200.h"
+#include "bc.cuh"
+#include "cbns_common.cuh"
+#include "setup.cuh"
+#include "stage.cuh"
+#include "step.cuh"
+#include "visc.cuh"
+
+using namespace cbns;
+
+namespace cbns {
+void stage_prepare();
+}
+
+enum { PK_STAGE = 0, PK_BC = 1, PK_VISC = 2, PK_STEP = 3, PK_N = 4 };
+
+struct cbns_ctx {
+  cbns_params prm;
+  Phys ph;
+  Dims d;
+  cudaStream_t own = nullptr, stream = nullptr;
+  double* qb[3] = {nullptr, nullptr, nullptr};
+  int lq = 0, lp = 1, ls = 2;  // physical index of logical Q, Q_p, spare
+  Fields f;
+  double* staging = nullptr;
+  size_t staging_elems = 0;
+  StepState* st = nullptr;
+  bool have_metrics = false, sigma_valid = false;
+  int prims_of = -1;     // physical buffer whose interior primitives the arrays hold
+  int pending_src = -1;  // buffer given to calc_numerical_flux, consumed by update_rk3
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  int g_q = -1, g_p = -1, g_s = -1;
+  int ntile_i = 1, ntile_j = 1, kchunk = 1;
+  bool prof = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PK_N];
+  std::vector<cudaEvent_t> ev_pool;
+  unsigned long long launches = 0;
+  int launches_per_step = 0;
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+thread_local std::string g_last;
+
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      g_last = std::string(#call) + ": " + cudaGetErrorString(e_);                  \
+      return CBNS_ERR_CUDA;                                                         \
+    }                                                                               \
+  } while (0)
+
+int dalloc(cbns_ctx* c, double** p, size_t elems) {
+  void* q = nullptr;
+  if (cudaMalloc(&q, elems * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    g_last = "device allocation failed";
+    return CBNS_ERR_NOMEM;
+  }
+  c->allocs.push_back(q);
+  *p = static_cast<double*>(q);
+  return CBNS_OK;
+}
+
+inline long round_up(long x, long m) { return (x + m - 1) / m * m; }
+
+cudaEvent_t take_event(cbns_ctx* c) {
+  cudaEvent_t e;
+  if (!c->ev_pool.empty()) {
+    e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+  } else {
+    cudaEventCreate(&e);
+  }
+  return e;
+}
+
+// wraps one group of launches with timing events when profiling is on
+struct Prof {
+  cbns_ctx* c;
+  int id;
+  cudaEvent_t a = nullptr;
+  Prof(cbns_ctx* c_, int id_) : c(c_), id(id_) {
+    if (c->prof) {
+      a = take_event(c);
+      cudaEventRecord(a, c->stream);
+    }
+  }
+  ~Prof() {
+    if (c->prof) {
+      cudaEvent_t b = take_event(c);
+      cudaEventRecord(b, c->stream);
+      c->ev[id].push_back({a, b});
+    }
+  }
+};
+
+double* buf(cbns_ctx* c, int logical) { return c->qb[logical == CBNS_QP ? c->lp : c->lq]; }
+int phys(cbns_ctx* c, int logical) { return logical == CBNS_QP ? c->lp : c->lq; }
+
+void fill_met(const cbns_ctx* c, const double* out[10]) {
+  for (int m = 0; m < 10; ++m) out[m] = c->f.met[m];
+}
+
+BCArgs bc_args(cbns_ctx* c, double* q, bool check_done, bool sigma) {
+  BCArgs a;
+  a.d = c->d;
+  a.gamma = c->ph.gamma;
+  a.gam1 = c->ph.gam1;
+  a.gM2 = c->ph.gM2;
+  a.p_inf = c->ph.p_inf;
+  a.i_begin = c->ph.i_begin;
+  a.i_end = c->ph.i_end;
+  a.viscous = c->ph.viscous;
+  a.q = q;
+  fill_met(c, a.met);
+  for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
+  a.st = c->st;
+  a.check_done = check_done;
+  a.sigma = sigma;
+  return a;
+}
+
+ViscArgs visc_args(cbns_ctx* c, bool check_done, bool sigma) {
+  ViscArgs a;
+  a.d = c->d;
+  a.gamma = c->ph.gamma;
+  a.Re_inv = c->ph.Re_inv;
+  a.C_T_inf = c->ph.C_T_inf;
+  a.C_dt_v = c->ph.C_dt_v;
+  a.qc = -c->ph.Pr_inv * c->ph.gam1_inv / c->ph.Mach2;
+  for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
+  fill_met(c, a.met);
+  for (int m = 0; m < 12; ++m) a.vflux[m] = c->f.vflux[m];
+  a.mu = c->f.prim[6];
+  a.st = c->st;
+  a.check_done = check_done;
+  a.sigma = sigma;
+  return a;
+}
+
+StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const double* qp, double* out, bool sigma) {
+  StageArgs a;
+  a.d = c->d;
+  a.gamma = c->ph.gamma;
+  a.gam1 = c->ph.gam1;
+  a.gam1_inv = c->ph.gam1_inv;
+  a.gM2 = c->ph.gM2;
+  a.src = src;
+  a.q0 = q0;
+  a.qp = qp;
+  a.out = out;
+  fill_met(c, a.met);
+  for (int m = 0; m < 12; ++m) a.vflux[m] = c->f.vflux[m];
+  for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
+  a.st = c->st;
+  a.ntile_i = c->ntile_i;
+  a.ntile_j = c->ntile_j;
+  a.kchunk = c->kchunk;
+  a.visdiv = c->ph.visdiv;
+  a.sigma = sigma;
+  return a;
+}
+
+int stage_launch(cbns_ctx* c, const StageArgs& a, int mode) {
+  Prof p(c, PK_STAGE);
+  CK(launch_stage(a, mode, c->ph.viscous != 0, c->ph.precision != CBNS_PREC_FP64, c->stream));
+  c->launches += 1;
+  return CBNS_OK;
+}
+
+int bc_launch(cbns_ctx* c, const BCArgs& a, bool interior_prims) {
+  Prof p(c, PK_BC);
+  int n = 0;
+  CK(launch_bc(a, interior_prims, c->stream, &n));
+  c->launches += n;
+  return CBNS_OK;
+}
+
+int visc_launch(cbns_ctx* c, const ViscArgs& a) {
+  Prof p(c, PK_VISC);
+  CK(launch_visc(a, c->stream));
+  c->launches += 1;
+  return CBNS_OK;
+}
+
+int sigma_launch(cbns_ctx* c) {
+  SigmaArgs a;
+  a.d = c->d;
+  a.gamma = c->ph.gamma;
+  a.gam1 = c->ph.gam1;
+  a.C_dt_v = c->ph.C_dt_v;
+  a.viscous = c->ph.viscous;
+  a.q = c->qb[c->lq];
+  for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
+  a.mu = c->f.prim[6];
+  fill_met(c, a.met);
+  a.st = c->st;
+  Prof p(c, PK_STEP);
+  CK(launch_sigma_nodes(a, c->stream));
+  c->launches += 1;
+  return CBNS_OK;
+}
+
+#define RET(x)                 \
+  do {                         \
+    int r_ = (x);              \
+    if (r_ != CBNS_OK) return r_; \
+  } while (0)
+
+int sync(cbns_ctx* c) {
+  CK(cudaStreamSynchronize(c->stream));
+  return CBNS_OK;
+}
+
+// Copy the logical Q buffer into the other two (set_conservative / calc_conservative
+// copy Q into Q_p, src/set_conservative.cu, src/calc_conservative.cu:39).
+int replicate_q(cbns_ctx* c) {
+  const size_t bytes = (size_t)NEQ * c->d.VOL * sizeof(double);
+  for (int b = 0; b < 3; ++b)
+    if (b != c->lq) CK(cudaMemcpyAsync(c->qb[b], c->qb[c->lq], bytes, cudaMemcpyDeviceToDevice, c->stream));
+  return CBNS_OK;
+}
+
+void drop_graph(cbns_ctx* c) {
+  if (c->gexec) cudaGraphExecDestroy(c->gexec);
+  if (c->graph) cudaGraphDestroy(c->graph);
+  c->gexec = nullptr;
+  c->graph = nullptr;
+}
+
+// One SSP-RK3 step on the fixed buffer roles P0 = Q, P1 = spare, P2 = Q_p.
+int enqueue_step(cbns_ctx* c) {
+  const bool visc = c->ph.viscous != 0;
+  double* P0 = c->qb[c->lq];
+  double* P1 = c->qb[c->ls];
+  double* P2 = c->qb[c->lp];
+  {
+    Prof p(c, PK_STEP);
+    CK(launch_step_prologue(c->st, c->ph.CFL, c->stream));
+    c->launches += 1;
+  }
+  struct S {
+    const double *src, *q0, *qp;
+    double* out;
+  } s[3] = {{P0, P0, P0, P1}, {P1, P0, P1, P2}, {P2, P0, P2, P0}};
+  for (int k = 0; k < 3; ++k) {
+    const bool last = k == 2;
+    RET(stage_launch(c, stage_args(c, s[k].src, s[k].q0, s[k].qp, s[k].out, last && !visc), k + 1));
+    RET(bc_launch(c, bc_args(c, s[k].out, true, last && !visc), false));
+    if (visc) RET(visc_launch(c, visc_args(c, true, last)));
+  }
+  return CBNS_OK;
+}
+
+int check_ready(cbns_ctx* c) {
+  if (!c) return CBNS_ERR_ARG;
+  if (!c->have_metrics) {
+    g_last = "metrics have not been computed (cbns_calc_metrics)";
+    return CBNS_ERR_STATE;
+  }
+  return CBNS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* cbns_status_string(int status) {
+  switch (status) {
+    case CBNS_OK: return "ok";
+    case CBNS_ERR_ARG: return "bad argument";
+    case CBNS_ERR_CUDA: return g_last.empty() ? "CUDA error" : g_last.c_str();
+    case CBNS_ERR_NAN_DT: return "An error occurred while calculating the time step.";
+    case CBNS_ERR_STATE: return g_last.empty() ? "call out of order" : g_last.c_str();
+    case CBNS_ERR_UNSUPPORTED: return "unsupported option";
+    case CBNS_ERR_NOMEM: return "device allocation failed";
+    case CBNS_ERR_TOO_LARGE: return "size beyond the entry point's fixed limit";
+    default: return "unknown status";
+  }
+}
+
+int cbns_create(const cbns_params* p, cbns_ctx** out) {
+  if (!p || !out) return CBNS_ERR_ARG;
+  *out = nullptr;
+  if (p->IM < 4 || p->JM < 4 || p->KM < 4) return CBNS_ERR_ARG;
+  if (p->viscous != 0 && p->viscous != 1) return CBNS_ERR_ARG;
+  if (p->precision < CBNS_PREC_FP64 || p->precision > CBNS_PREC_HYBRID) return CBNS_ERR_ARG;
+  if (p->vis_divergence != CBNS_VISDIV_REFERENCE && p->vis_divergence != CBNS_VISDIV_CENTERED) return CBNS_ERR_ARG;
+  for (int r : p->reserved)
+    if (r != 0) return CBNS_ERR_ARG;
+  if (p->precision == CBNS_PREC_HYBRID) return CBNS_ERR_UNSUPPORTED;
+  const double ng = ((double)p->IM + 4) * ((double)p->JM + 4) * ((double)p->KM + 4);
+  if (ng * 5 > 2.0e9) return CBNS_ERR_TOO_LARGE;
+
+  cbns_ctx* c = new cbns_ctx();
+  c->prm = *p;
+  // derived parameters exactly as src/Block3d.cpp:99-113
+  Phys& h = c->ph;
+  h.gamma = p->gamma;
+  h.Mach2 = p->Mach * p->Mach;
+  h.Re_inv = 1.0 / p->Re;
+  h.Pr_inv = 1.0 / p->Pr;
+  h.gam1 = p->gamma - 1.0;
+  h.gM2 = p->gamma * h.Mach2;
+  h.gam1_inv = 1.0 / h.gam1;
+  h.p_inf = 1.0 / h.gM2;
+  h.C_T_inf = 110.5 / p->T_inf;
+  h.C_dt_v = std::max(4.0 / 3.0, p->gamma * h.Pr_inv) * h.Re_inv;
+  h.CFL = p->CFL;
+  h.angle_attack = p->angle_attack;
+  h.i_begin = p->i_begin;
+  h.i_end = p->i_end;
+  h.viscous = p->viscous;
+  h.visdiv = p->vis_divergence;
+  h.precision = p->precision;
+
+  Dims& d = c->d;
+  d.IM = (int)p->IM;
+  d.JM = (int)p->JM;
+  d.KM = (int)p->KM;
+  d.IG = d.IM + 2 * NG;
+  d.JG = d.JM + 2 * NG;
+  d.KG = d.KM + 2 * NG;
+  d.PX = round_up(LP + d.IG + 16, 16);  // +16: tiles may read a few nodes past IM+1
+  d.PL = d.PX * d.JG;
+  d.VOL = round_up(d.PL * (d.KG + 1), 32);  // one spare plane of padding at the end
+
+  int rc = CBNS_OK;
+  for (int b = 0; b < 3 && rc == CBNS_OK; ++b) rc = dalloc(c, &c->qb[b], (size_t)NEQ * d.VOL);
+  for (int m = 0; m < 10 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.met[m], d.VOL);
+  for (int m = 0; m < 7 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.prim[m], d.VOL);
+  for (int m = 0; m < 12; ++m) c->f.vflux[m] = nullptr;
+  if (p->viscous)
+    for (int m = 0; m < 12 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.vflux[m], d.VOL);
+  const long NGt = (long)d.IG * d.JG * d.KG;
+  c->staging_elems = (size_t)std::max(5 * NGt, 10L * d.IM * d.JM * d.KM);
+  if (rc == CBNS_OK) rc = dalloc(c, &c->staging, c->staging_elems);
+  if (rc == CBNS_OK) {
+    void* s = nullptr;
+    if (cudaMalloc(&s, sizeof(StepState)) != cudaSuccess) rc = CBNS_ERR_NOMEM;
+    else {
+      c->allocs.push_back(s);
+      c->st = static_cast<StepState*>(s);
+      cudaMemset(s, 0, sizeof(StepState));
+    }
+  }
+  if (rc == CBNS_OK && cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) rc = CBNS_ERR_CUDA;
+  if (rc != CBNS_OK) {
+    cbns_destroy(c);
+    return rc;
+  }
+  c->stream = c->own;
+  // zero everything once so padding never holds NaN garbage
+  for (void* a : c->allocs) (void)a;
+  for (int b = 0; b < 3; ++b) cudaMemsetAsync(c->qb[b], 0, (size_t)NEQ * d.VOL * sizeof(double), c->stream);
+  for (int m = 0; m < 10; ++m) cudaMemsetAsync(c->f.met[m], 0, d.VOL * sizeof(double), c->stream);
+  for (int m = 0; m < 7; ++m) cudaMemsetAsync(c->f.prim[m], 0, d.VOL * sizeof(double), c->stream);
+  if (p->viscous)
+    for (int m = 0; m < 12; ++m) cudaMemsetAsync(c->f.vflux[m], 0, d.VOL * sizeof(double), c->stream);
+
+  stage_tiles(d, &c->ntile_i, &c->ntile_j);
+  const int ntiles = c->ntile_i * c->ntile_j;
+  const int nint = d.KM - 2;
+  int nchunk = std::max(1, std::min((4 * 296 + ntiles - 1) / ntiles, nint / 8));
+  c->kchunk = (nint + nchunk - 1) / nchunk;
+  stage_prepare();
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    g_last = "context initialisation failed";
+    cbns_destroy(c);
+    return CBNS_ERR_CUDA;
+  }
+  *out = c;
+  return CBNS_OK;
+}
+
+int cbns_destroy(cbns_ctx* c) {
+  if (!c) return CBNS_ERR_ARG;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  drop_graph(c);
+  for (auto& v : c->ev)
+    for (auto& pr : v) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
+  for (void* a : c->allocs) cudaFree(a);
+  if (c->own) cudaStreamDestroy(c->own);
+  delete c;
+  return CBNS_OK;
+}
+
+int cbns_set_stream(cbns_ctx* c, void* s) {
+  if (!c) return CBNS_ERR_ARG;
+  RET(sync(c));
+  c->stream = s ? static_cast<cudaStream_t>(s) : c->own;
+  drop_graph(c);
+  return CBNS_OK;
+}
+
+int cbns_calc_metrics(cbns_ctx* c, const double* x, const double* y, const double* z) {
+  if (!c || !x || !y || !z) return CBNS_ERR_ARG;
+  const size_t N = (size_t)c->d.IM * c->d.JM * c->d.KM;
+  double* sx = c->staging;
+  CK(cudaMemcpyAsync(sx, x, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(sx + N, y, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(sx + 2 * N, z, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_metrics(c->d, sx, sx + N, sx + 2 * N, c->f.met, c->stream));
+  c->launches += 2;
+  RET(sync(c));
+  c->have_metrics = true;
+  c->sigma_valid = false;
+  return CBNS_OK;
+}
+
+int cbns_get_metrics(cbns_ctx* c, double* xi_x, double* xi_y, double* xi_z, double* eta_x, double* eta_y,
+                     double* eta_z, double* zeta_x, double* zeta_y, double* zeta_z, double* Jac) {
+  RET(check_ready(c));
+  double* outs[10] = {xi_x, xi_y, xi_z, eta_x, eta_y, eta_z, zeta_x, zeta_y, zeta_z, Jac};
+  const size_t N = (size_t)c->d.IM * c->d.JM * c->d.KM;
+  for (int m = 0; m < 10; ++m) {
+    if (!outs[m]) return CBNS_ERR_ARG;
+    CK(launch_gather_nodes(c->d, c->f.met[m], c->staging, c->stream));
+    c->launches += 1;
+    CK(cudaMemcpyAsync(outs[m], c->staging, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    RET(sync(c));
+  }
+  return CBNS_OK;
+}
+
+int cbns_initial_condition(cbns_ctx* c) {
+  if (!c) return CBNS_ERR_ARG;
+  CK(launch_ic(c->d, c->f.prim, c->ph.angle_attack, c->ph.p_inf, c->ph.viscous, c->stream));
+  c->launches += 1;
+  c->prims_of = -1;
+  return sync(c);
+}
+
+int cbns_calc_conservative(cbns_ctx* c, int which) {
+  if (!c || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
+  CK(launch_conservative(c->d, c->f.prim, buf(c, which), c->ph.gam1, c->stream));
+  c->launches += 1;
+  RET(replicate_q(c));
+  c->sigma_valid = false;
+  c->prims_of = -1;
+  return sync(c);
+}
+
+int cbns_set_conservative(cbns_ctx* c, const double* Q) {
+  if (!c || !Q) return CBNS_ERR_ARG;
+  const size_t n = (size_t)NEQ * c->d.IG * c->d.JG * c->d.KG;
+  CK(cudaMemcpyAsync(c->staging, Q, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_aos_to_soa(c->d, c->staging, c->qb[c->lq], c->stream));
+  c->launches += 1;
+  RET(replicate_q(c));
+  c->sigma_valid = false;
+  c->prims_of = -1;
+  return sync(c);
+}
+
+int cbns_get_conservative(cbns_ctx* c, int which, double* Q) {
+  if (!c || !Q || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
+  const size_t n = (size_t)NEQ * c->d.IG * c->d.JG * c->d.KG;
+  CK(launch_soa_to_aos(c->d, buf(c, which), c->staging, c->stream));
+  c->launches += 1;
+  CK(cudaMemcpyAsync(Q, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int cbns_get_primitive(cbns_ctx* c, double* rho, double* u, double* v, double* w, double* p, double* T) {
+  if (!c || !rho || !u || !v || !w || !p) return CBNS_ERR_ARG;
+  if (!c->ph.viscous) {
+    // inviscid runs keep no primitive arrays: recover them from Q
+    CK(launch_primitive(c->d, c->qb[c->lq], c->f.prim, c->ph.gam1, c->ph.gM2, c->stream));
+    c->launches += 1;
+  }
+  double* outs[6] = {rho, u, v, w, p, T};
+  const size_t n = (size_t)c->d.IG * c->d.JG * c->d.KG;
+  for (int m = 0; m < 6; ++m) {
+    if (!outs[m]) continue;
+    CK(launch_gather_ghosted(c->d, c->f.prim[m], c->staging, c->stream));
+    c->launches += 1;
+    CK(cudaMemcpyAsync(outs[m], c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    RET(sync(c));
+  }
+  return CBNS_OK;
+}
+
+int cbns_calc_primitive(cbns_ctx* c, int which) {
+  if (!c || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
+  CK(launch_primitive(c->d, buf(c, which), c->f.prim, c->ph.gam1, c->ph.gM2, c->stream));
+  c->launches += 1;
+  c->prims_of = phys(c, which);
+  return sync(c);
+}
+
+int cbns_set_bc_calc_primitive(cbns_ctx* c, int which) {
+  RET(check_ready(c));
+  if (which != CBNS_Q && which != CBNS_QP) return CBNS_ERR_ARG;
+  const int pb = phys(c, which);
+  const bool interior = c->ph.viscous && c->prims_of != pb;
+  RET(bc_launch(c, bc_args(c, c->qb[pb], false, false), interior));
+  if (c->ph.viscous) c->prims_of = pb;
+  c->sigma_valid = false;
+  return sync(c);
+}
+
+int cbns_calc_numerical_flux(cbns_ctx* c, int which) {
+  RET(check_ready(c));
+  if (which != CBNS_Q && which != CBNS_QP) return CBNS_ERR_ARG;
+  // the fluxes are formed inside the stage kernel launched by cbns_update_rk3
+  c->pending_src = which;
+  return CBNS_OK;
+}
+
+int cbns_calc_viscous_flux_contribution(cbns_ctx* c) {
+  RET(check_ready(c));
+  // the divergence of the node fluxes is taken inside the stage kernel
+  return CBNS_OK;
+}
+
+int cbns_calc_viscous_terms(cbns_ctx* c) {
+  RET(check_ready(c));
+  if (!c->ph.viscous) return CBNS_OK;  // the inviscid build compiles this to nothing
+  RET(visc_launch(c, visc_args(c, false, false)));
+  return sync(c);
+}
+
+int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
+  RET(check_ready(c));
+  if (stage < 1 || stage > 3) return CBNS_ERR_ARG;
+  const int src_l = c->pending_src >= 0 ? c->pending_src : (stage == 1 ? CBNS_Q : CBNS_QP);
+  c->pending_src = -1;
+  const int src = phys(c, src_l);
+  int out = stage == 3 ? c->lq : c->lp;
+  const bool swap = out == src;
+  if (swap) out = c->ls;
+  {
+    Prof p(c, PK_STEP);
+    CK(launch_set_dt(c->st, dt, c->stream));
+    c->launches += 1;
+  }
+  const StageArgs a = stage_args(c, c->qb[src], c->qb[c->lq], c->qb[c->lp], c->qb[out], false);
+  RET(stage_launch(c, a, (int)stage));
+  if (swap) {
+    if (stage == 3) std::swap(c->lq, c->ls);
+    else std::swap(c->lp, c->ls);
+  }
+  if (c->ph.viscous) c->prims_of = out;
+  c->sigma_valid = false;
+  return sync(c);
+}
+
+int cbns_calc_dt(cbns_ctx* c, double* dt) {
+  RET(check_ready(c));
+  if (!dt) return CBNS_ERR_ARG;
+  RET(sigma_launch(c));
+  unsigned long long bits = 0;
+  CK(cudaMemcpyAsync(&bits, &c->st->sigma_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  RET(sync(c));
+  double smax;
+  std::memcpy(&smax, &bits, sizeof(smax));
+  *dt = c->ph.CFL / smax;
+  c->sigma_valid = true;
+  if (std::isnan(*dt)) return CBNS_ERR_NAN_DT;
+  return CBNS_OK;
+}
+
+int cbns_set_time(cbns_ctx* c, double t_cur) {
+  if (!c) return CBNS_ERR_ARG;
+  CK(cudaMemcpyAsync(&c->st->t_cur, &t_cur, sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return sync(c);
+}
+
+int cbns_get_time(cbns_ctx* c, double* t_cur, double* dt_last) {
+  if (!c) return CBNS_ERR_ARG;
+  StepState h;
+  CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  RET(sync(c));
+  if (t_cur) *t_cur = h.t_cur;
+  if (dt_last) *dt_last = h.dt;
+  return CBNS_OK;
+}
+
+static int run_impl(cbns_ctx* c, unsigned nsteps, double t_end, bool wait, unsigned* steps_done) {
+  RET(check_ready(c));
+  {
+    StepState h;
+    CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    RET(sync(c));
+    h.t_end = t_end;
+    h.done = 0;
+    h.nan_dt = 0;
+    h.steps = 0;
+    CK(cudaMemcpyAsync(c->st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+    RET(sync(c));
+  }
+  if (!c->sigma_valid) {
+    RET(sigma_launch(c));
+    c->sigma_valid = true;
+  }
+  if (c->prof) {
+    for (unsigned n = 0; n < nsteps; ++n) RET(enqueue_step(c));
+  } else {
+    if (!c->gexec || c->g_q != c->lq || c->g_p != c->lp || c->g_s != c->ls) {
+      drop_graph(c);
+      const unsigned long long l0 = c->launches;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      const int rc = enqueue_step(c);
+      cudaGraph_t g = nullptr;
+      const cudaError_t ee = cudaStreamEndCapture(c->stream, &g);
+      if (rc != CBNS_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      CK(ee);
+      c->graph = g;
+      CK(cudaGraphInstantiate(&c->gexec, g, 0));
+      c->launches_per_step = (int)(c->launches - l0);
+      c->launches = l0;
+      c->g_q = c->lq;
+      c->g_p = c->lp;
+      c->g_s = c->ls;
+    }
+    for (unsigned n = 0; n < nsteps; ++n) {
+      CK(cudaGraphLaunch(c->gexec, c->stream));
+      c->launches += c->launches_per_step;
+    }
+  }
+  if (c->ph.viscous) c->prims_of = c->lq;
+  if (!wait) return CBNS_OK;
+  StepState h;
+  CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  RET(sync(c));
+  if (steps_done) *steps_done = h.steps;
+  if (h.nan_dt) {
+    c->sigma_valid = false;
+    return CBNS_ERR_NAN_DT;
+  }
+  return CBNS_OK;
+}
+
+int cbns_run(cbns_ctx* c, unsigned nsteps, double t_end, unsigned* steps_done) {
+  return run_impl(c, nsteps, t_end, true, steps_done);
+}
+
+int cbns_run_async(cbns_ctx* c, unsigned nsteps, double t_end) { return run_impl(c, nsteps, t_end, false, nullptr); }
+
+int cbns_eval_rhs(cbns_ctx* c, int which, double* rhs) {
+  RET(check_ready(c));
+  if (!rhs || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
+  const StageArgs a = stage_args(c, buf(c, which), nullptr, nullptr, c->staging, false);
+  RET(stage_launch(c, a, 0));
+  const size_t n = (size_t)NEQ * (c->d.IM - 2) * (c->d.JM - 2) * (c->d.KM - 2);
+  CK(cudaMemcpyAsync(rhs, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f, double* fx, double* fy, double* fz) {
+  if (!f || !fx || !fy || !fz || IM < 2 || JM < 2 || KM < 2) return CBNS_ERR_ARG;
+  const size_t N = (size_t)IM * JM * KM;
+  double* dbuf = nullptr;
+  CK(cudaMalloc(&dbuf, 4 * N * sizeof(double)));
+  int rc = CBNS_OK;
+  if (cudaMemcpy(dbuf, f, N * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+      launch_gradient_dense((int)IM, (int)JM, (int)KM, dbuf, dbuf + N, dbuf + 2 * N, dbuf + 3 * N, 0) !=
+          cudaSuccess ||
+      cudaMemcpy(fx, dbuf + N, N * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(fy, dbuf + 2 * N, N * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(fz, dbuf + 3 * N, N * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    g_last = cudaGetErrorString(cudaGetLastError());
+    rc = CBNS_ERR_CUDA;
+  }
+  cudaFree(dbuf);
+  return rc;
+}
+
+int cbns_prof_enable(cbns_ctx* c, int on) {
+  if (!c) return CBNS_ERR_ARG;
+  c->prof = on != 0;
+  return CBNS_OK;
+}
+
+int cbns_prof_read(cbns_ctx* c, int id, double* total_ms, unsigned* launches) {
+  if (!c || id < 0 || id >= PK_N) return CBNS_ERR_ARG;
+  RET(sync(c));
+  double tot = 0.0;
+  for (auto& pr : c->ev[id]) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+    tot += ms;
+  }
+  if (total_ms) *total_ms = tot;
+  if (launches) *launches = (unsigned)c->ev[id].size();
+  return CBNS_OK;
+}
+
+int cbns_prof_reset(cbns_ctx* c) {
+  if (!c) return CBNS_ERR_ARG;
+  RET(sync(c));
+  for (auto& v : c->ev) {
+    for (auto& pr : v) {
+      c->ev_pool.push_back(pr.first);
+      c->ev_pool.push_back(pr.second);
+    }
+    v.clear();
+  }
+  return CBNS_OK;
+}
+
+int cbns_launch_count(cbns_ctx* c, unsigned long long* n) {
+  if (!c || !n) return CBNS_ERR_ARG;
+  *n = c->launches;
+  return CBNS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,25 @@
+// bc.cuh - launch interface of the boundary-condition kernels (bc.cu).
+#pragma once
+
+#include "cbns_common.cuh"
+
+namespace cbns {
+
+struct BCArgs {
+  Dims d;
+  double gamma, gam1, gM2, p_inf;
+  unsigned i_begin, i_end;
+  int viscous;
+  double* q;             // the buffer the boundary conditions act on (5 fields)
+  const double* met[10];
+  double* prim[6];       // rho,u,v,w,p,T (viscous runs)
+  StepState* st;
+  int check_done;        // return at once when st->done is set (graph-replayed steps)
+  int sigma;             // inviscid: accumulate boundary-node spectral radii
+};
+
+// interior_prims: also recompute interior primitives (viscous runs), when the
+// primitive arrays do not describe this buffer.  *launches += kernels launched.
+cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int* launches);
+
+}  // namespace cbns

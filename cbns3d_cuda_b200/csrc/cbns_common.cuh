@@ -1,0 +1,72 @@
+// cbns_common.cuh - data layout, run parameters and small device helpers shared
+// by every kernel of the B200 RK3 right-hand-side library.
+//
+// HBM layout (structure of arrays).  Every node field (each conservative
+// variable, each metric, each primitive, each viscous flux component) is one
+// FP64 array over the ghosted box of IM_G x JM_G x KM_G nodes (NG = 2 ghost
+// layers, as include/Block3d_cuda.h:40-49 of the reference).  Node (i,j,k),
+// i in [-2, IM+2), sits at element
+//     LP + (i+2) + PX*((j+2) + JG*(k+2))
+// where LP = 13 leading pad elements make interior node i = 1 (ghosted index 3)
+// start on a 128-byte boundary, and the row pitch PX (a multiple of 16 elements)
+// keeps every row 128-byte aligned.  A conservative state buffer holds its five
+// variables back to back, VOL elements apart (VOL a multiple of 32 elements).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cbns {
+
+constexpr int NEQ = 5;
+constexpr int NG = 2;
+constexpr long LP = 13;
+
+struct Dims {
+  int IM, JM, KM;  // grid points
+  int IG, JG, KG;  // ghosted extents
+  long PX;         // row pitch (elements)
+  long PL;         // plane pitch = PX * JG
+  long VOL;        // one field, padded
+};
+
+__host__ __device__ inline long node_off(const Dims& d, int i, int j, int k) {
+  return LP + (long)(i + NG) + d.PX * ((long)(j + NG) + (long)d.JG * (long)(k + NG));
+}
+
+// Physical parameters after the derivation of src/Block3d.cpp:99-113.
+struct Phys {
+  double gamma, gam1, gam1_inv, gM2, Mach2, p_inf, CFL, Re_inv, Pr_inv, C_T_inf, C_dt_v;
+  double angle_attack;
+  unsigned i_begin, i_end;
+  int viscous, visdiv, precision;
+};
+
+// Device pointers of one context.  Q buffers hold 5 fields each.
+struct Fields {
+  double* met[10];   // xi_x, xi_y, xi_z, eta_x, eta_y, eta_z, zeta_x, zeta_y, zeta_z, Jac
+  double* prim[7];   // rho, u, v, w, p, T, mu (viscous upkeep; on-demand otherwise)
+  double* vflux[12]; // E0..E3, F0..F3, G0..G3 (viscous node fluxes, times J-scaled normals)
+};
+
+// Per-run scalars kept on the device so a whole step can be replayed from a graph.
+struct StepState {
+  unsigned long long sigma_bits;  // max spectral radius (bit pattern of a positive double)
+  double dt;                      // time step of the current step
+  double t_cur;                   // simulated time
+  double t_end;
+  unsigned steps;                 // steps taken
+  int done;                       // time loop finished: kernels return immediately
+  int nan_dt;                     // CFL/max(sigma) was NaN
+  int pad;
+};
+
+// Positive doubles order like their bit patterns; a NaN (either sign) compares
+// above every finite value, so a max over bit patterns propagates NaN.
+__device__ inline void atomic_max_sigma(unsigned long long* a, double s) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(s);
+  if (s != s) b = 0x7ff8000000000000ull;  // canonical NaN, above +inf
+  atomicMax(a, b);
+}
+
+}  // namespace cbns

@@ -1,0 +1,234 @@
+// face_flux.cuh - numerical flux through one grid face: characteristic-wise
+// WENO5-JS reconstruction in the Roe-averaged eigenbasis of the two adjacent
+// nodes, followed by the local Lax-Friedrichs flux.
+//
+// Restates, per face, the arithmetic of the reference's
+//   rec_riemann_{xi,eta,zeta}_kernel  src/rec_riemann_kernel.cu:15-247
+//   calc_eigenvectors_roe             src/calc_eigenvectors_roe.cu:13-152
+//   rec_weno5 / weno5                 src/weno.cu:13-120
+//   lf_flux                           src/lf_flux.cu:13-80
+// with the same basis construction (tangent (0,nz,-ny) unless its norm is
+// below 1e-8), the same WENO5-JS weights (eps = 1e-6 inside beta, before
+// squaring), the same Cartesian wave-speed bound of the LF dissipation, and the
+// same use of the node primitives for the Roe average.  The algebra is
+// reorganised for the GPU (all of it is exact rearrangement, so results agree to
+// rounding):
+//   * the 6 stencil states are projected onto the characteristic fields once;
+//     the low-side stencil uses points 0..4 and the high-side stencil the same
+//     projected values 5..1, instead of projecting 10 states;
+//   * the left eigenvectors are applied through their structure
+//     (w0,w2 = A +- B, w1 = f0 - 2A, w3,w4 = tangential momenta) and the right
+//     eigenvectors likewise, instead of 5x5 matrix products;
+//   * each WENO5 value costs one division (weights scaled by the product of
+//     the squared smoothness indicators) in FP64; the FP32 form uses fast
+//     reciprocals.
+// R is the arithmetic type (double for the plain path, float for the split path).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace cbns {
+
+template <typename R>
+struct FluxConsts {
+  R gamma, gam1, gam1_inv;
+};
+
+template <typename R>
+__device__ __forceinline__ R rcp_(R x) {
+  if constexpr (sizeof(R) == 8) {
+    return 1.0 / x;
+  } else {
+    return __frcp_rn(x);
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ R div_(R a, R b) {
+  if constexpr (sizeof(R) == 8) {
+    return a / b;
+  } else {
+    return __fdividef(a, b);
+  }
+}
+
+// WENO5-JS value at the +1/2 side of c from the stencil a b c d e.
+template <typename R>
+__device__ __forceinline__ R weno5(R a, R b, R c, R d, R e) {
+  const R eps = R(1.0e-6);
+  const R c13 = R(13.0 / 12.0);
+  const R d1 = a - R(2) * b + c, e1 = a - R(4) * b + R(3) * c;
+  const R d2 = b - R(2) * c + d, e2 = b - d;
+  const R d3 = c - R(2) * d + e, e3 = R(3) * c - R(4) * d + e;
+  const R s1 = c13 * d1 * d1 + R(0.25) * e1 * e1 + eps;
+  const R s2 = c13 * d2 * d2 + R(0.25) * e2 * e2 + eps;
+  const R s3 = c13 * d3 * d3 + R(0.25) * e3 * e3 + eps;
+  const R p1 = R(2) * a - R(7) * b + R(11) * c;  // 6 x candidate values
+  const R p2 = -b + R(5) * c + R(2) * d;
+  const R p3 = R(2) * c + R(5) * d - e;
+  if constexpr (sizeof(R) == 8) {
+    const R t1 = s1 * s1, t2 = s2 * s2, t3 = s3 * s3;
+    const R a1 = R(0.1) * (t2 * t3), a2 = R(0.6) * (t1 * t3), a3 = R(0.3) * (t1 * t2);
+    return (a1 * p1 + a2 * p2 + a3 * p3) / (R(6) * (a1 + a2 + a3));
+  } else {
+    const R a1 = __fdividef(R(0.1), s1 * s1);
+    const R a2 = __fdividef(R(0.6), s2 * s2);
+    const R a3 = __fdividef(R(0.3), s3 * s3);
+    return __fdividef(a1 * p1 + a2 * p2 + a3 * p3, R(6) * (a1 + a2 + a3));
+  }
+}
+
+// Flux through the face between stencil points 2 (node a) and 3 (node b).
+// ld(p, n) returns conservative variable n at stencil point p (p = 0..5 are the
+// nodes a-2 .. b+2 along the face normal).  (nx,ny,nz) is the face area vector
+// 0.5*(J grad(xi)|_a + J grad(xi)|_b).  out[0..4] receives the flux.
+template <typename R, typename LD>
+__device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const FluxConsts<R>& C,
+                                          R out[5]) {
+  const R gamma = C.gamma, gam1 = C.gam1, gam1_inv = C.gam1_inv;
+
+  // node primitives at a and b (the reference reads them from the primitive
+  // arrays, which hold exactly these values on every node a face touches)
+  R ra, ua, va, wa, pa, rb, ub, vb, wb, pb, ira, irb;
+  {
+    ra = ld(2, 0);
+    ira = rcp_(ra);
+    ua = ld(2, 1) * ira;
+    va = ld(2, 2) * ira;
+    wa = ld(2, 3) * ira;
+    pa = gam1 * (ld(2, 4) - R(0.5) * ra * (ua * ua + va * va + wa * wa));
+    rb = ld(3, 0);
+    irb = rcp_(rb);
+    ub = ld(3, 1) * irb;
+    vb = ld(3, 2) * irb;
+    wb = ld(3, 3) * irb;
+    pb = gam1 * (ld(3, 4) - R(0.5) * rb * (ub * ub + vb * vb + wb * wb));
+  }
+
+  // orthonormal basis (n, l, m)
+  R lx = R(0), ly = nz, lz = -ny, mx, my, mz;
+  if (ly * ly + lz * lz > R(1.0e-16)) {
+    mx = -ny * ny - nz * nz;
+    my = nx * ny;
+    mz = nx * nz;
+  } else {
+    lx = -nz;
+    ly = R(0);
+    lz = nx;
+    mx = nx * ny;
+    my = -nx * nx - nz * nz;
+    mz = ny * nz;
+  }
+  R ux, uy, uz;  // unit normal
+  {
+    const R in = rsqrt(nx * nx + ny * ny + nz * nz);
+    ux = nx * in;
+    uy = ny * in;
+    uz = nz * in;
+    const R il = rsqrt(lx * lx + ly * ly + lz * lz);
+    lx *= il;
+    ly *= il;
+    lz *= il;
+    const R im = rsqrt(mx * mx + my * my + mz * mz);
+    mx *= im;
+    my *= im;
+    mz *= im;
+  }
+
+  // Roe averages
+  R uu, vv, ww, H, q2, c, qn, ql, qm, K, h;
+  {
+    const R Ha = gamma * pa * ira * gam1_inv + R(0.5) * (ua * ua + va * va + wa * wa);
+    const R Hb = gamma * pb * irb * gam1_inv + R(0.5) * (ub * ub + vb * vb + wb * wb);
+    const R sr = sqrt(rb * ira);
+    const R is = rcp_(R(1) + sr);
+    uu = (ua + sr * ub) * is;
+    vv = (va + sr * vb) * is;
+    ww = (wa + sr * wb) * is;
+    H = (Ha + sr * Hb) * is;
+    q2 = uu * uu + vv * vv + ww * ww;
+    c = sqrt(gam1 * (H - R(0.5) * q2));
+    const R ic = rcp_(c);
+    qn = uu * ux + vv * uy + ww * uz;
+    ql = uu * lx + vv * ly + ww * lz;
+    qm = uu * mx + vv * my + ww * mz;
+    h = R(0.5) * ic;
+    K = gam1 * h * ic;  // (gamma-1)/(2 c^2)
+  }
+
+  // characteristic projection of the 6 stencil states
+  R W[5][6];
+#pragma unroll
+  for (int p = 0; p < 6; ++p) {
+    const R f0 = ld(p, 0), f1 = ld(p, 1), f2 = ld(p, 2), f3 = ld(p, 3), f4 = ld(p, 4);
+    const R A = K * (R(0.5) * q2 * f0 - (uu * f1 + vv * f2 + ww * f3) + f4);
+    const R B = h * (qn * f0 - (ux * f1 + uy * f2 + uz * f3));
+    W[0][p] = A + B;
+    W[1][p] = f0 - R(2) * A;
+    W[2][p] = A - B;
+    W[3][p] = lx * f1 + ly * f2 + lz * f3 - ql * f0;
+    W[4][p] = mx * f1 + my * f2 + mz * f3 - qm * f0;
+  }
+
+  // WENO5 per field: low side from points 0..4, high side from 5..1
+  R wl[5], wh[5];
+#pragma unroll
+  for (int s = 0; s < 5; ++s) {
+    wl[s] = weno5<R>(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4]);
+    wh[s] = weno5<R>(W[s][5], W[s][4], W[s][3], W[s][2], W[s][1]);
+  }
+
+  // back to conservative variables, then primitives, on each side
+  R Lr, Lu, Lv, Lw, Lp, Hr, Hu, Hv, Hw, Hp;
+  {
+    const R hq = R(0.5) * q2;
+    R q[5];
+    auto back = [&](const R* w) {
+      const R s = w[0] + w[2], d = (w[2] - w[0]) * c;
+      q[0] = s + w[1];
+      q[1] = uu * q[0] + ux * d + lx * w[3] + mx * w[4];
+      q[2] = vv * q[0] + uy * d + ly * w[3] + my * w[4];
+      q[3] = ww * q[0] + uz * d + lz * w[3] + mz * w[4];
+      q[4] = H * s + qn * d + hq * w[1] + ql * w[3] + qm * w[4];
+    };
+    back(wl);
+    Lr = q[0];
+    {
+      const R i = rcp_(Lr);
+      Lu = q[1] * i;
+      Lv = q[2] * i;
+      Lw = q[3] * i;
+      Lp = gam1 * (q[4] - R(0.5) * Lr * (Lu * Lu + Lv * Lv + Lw * Lw));
+    }
+    back(wh);
+    Hr = q[0];
+    {
+      const R i = rcp_(Hr);
+      Hu = q[1] * i;
+      Hv = q[2] * i;
+      Hw = q[3] * i;
+      Hp = gam1 * (q[4] - R(0.5) * Hr * (Hu * Hu + Hv * Hv + Hw * Hw));
+    }
+  }
+
+  // local Lax-Friedrichs flux (the reference's lf_flux with R = high side, L = low side)
+  {
+    const R kH = Hu * Hu + Hv * Hv + Hw * Hw, kL = Lu * Lu + Lv * Lv + Lw * Lw;
+    const R cH = sqrt(gamma * Hp * rcp_(Hr)), cL = sqrt(gamma * Lp * rcp_(Lr));
+    const R HH = cH * cH * gam1_inv + R(0.5) * kH, HL = cL * cL * gam1_inv + R(0.5) * kL;
+    const R EH = Hp * gam1_inv + R(0.5) * Hr * kH, EL = Lp * gam1_inv + R(0.5) * Lr * kL;
+    const R qH = Hu * nx + Hv * ny + Hw * nz, qL = Lu * nx + Lv * ny + Lw * nz;
+    const R sx = fmax(fabs(Hu) + cH, fabs(Lu) + cL);
+    const R sy = fmax(fabs(Hv) + cH, fabs(Lv) + cL);
+    const R sz = fmax(fabs(Hw) + cH, fabs(Lw) + cL);
+    const R ws = fabs(sx * nx + sy * ny + sz * nz);
+    const R mL = Lr * qL, mH = Hr * qH;
+    out[0] = R(0.5) * (mL + mH - ws * (Hr - Lr));
+    out[1] = R(0.5) * (mL * Lu + Lp * nx + mH * Hu + Hp * nx - ws * (Hr * Hu - Lr * Lu));
+    out[2] = R(0.5) * (mL * Lv + Lp * ny + mH * Hv + Hp * ny - ws * (Hr * Hv - Lr * Lv));
+    out[3] = R(0.5) * (mL * Lw + Lp * nz + mH * Hw + Hp * nz - ws * (Hr * Hw - Lr * Lw));
+    out[4] = R(0.5) * (mL * HL + mH * HH - ws * (EH - EL));
+  }
+}
+
+}  // namespace cbns

@@ -1,0 +1,245 @@
+// setup.cu - one-time and I/O kernels: metrics (FP64), initial condition,
+// primitive <-> conservative conversion, the AoS <-> SoA transposes that keep the
+// reference's host/checkpoint layout at the boundary, and gathers for getters.
+#include "setup.cuh"
+
+namespace cbns {
+
+namespace {
+
+// 4th-order first derivative along one axis, the stencils of
+// src/gradient_kernel.cu:41-63 (one-sided at the two ends, biased next to
+// them, central inside).  Axes shorter than 5 points, where those stencils
+// index outside the array, use 2nd-order differences.
+__device__ __forceinline__ double dax(const double* f, long s, int g, int n) {
+  if (n < 5) {
+    if (n == 1) return 0.0;
+    if (g == 0) return n >= 3 ? 0.5 * (-3.0 * f[0] + 4.0 * f[s] - f[2 * s]) : f[s] - f[0];
+    if (g == n - 1) return n >= 3 ? 0.5 * (3.0 * f[0] - 4.0 * f[-s] + f[-2 * s]) : f[0] - f[-s];
+    return 0.5 * (f[s] - f[-s]);
+  }
+  if (g == 0)
+    return -25.0 / 12.0 * f[0] + 4.0 * f[s] - 3.0 * f[2 * s] + (4.0 / 3.0) * f[3 * s] - 0.25 * f[4 * s];
+  if (g == 1)
+    return -5.0 / 6.0 * f[0] - 0.25 * f[-s] + 1.5 * f[s] - 0.5 * f[2 * s] + (1.0 / 12.0) * f[3 * s];
+  if (g == n - 2)
+    return (5.0 / 6.0) * f[0] - 1.0 / 12.0 * f[-3 * s] + 0.5 * f[-2 * s] - 1.5 * f[-s] + 0.25 * f[s];
+  if (g == n - 1)
+    return (25.0 / 12.0) * f[0] + 0.25 * f[-4 * s] - 4.0 / 3.0 * f[-3 * s] + 3.0 * f[-2 * s] - 4.0 * f[-s];
+  return (1.0 / 12.0) * f[-2 * s] - 2.0 / 3.0 * f[-s] + (2.0 / 3.0) * f[s] - 1.0 / 12.0 * f[2 * s];
+}
+
+struct Met {
+  double* m[10];
+};
+
+// x_xi .. z_zeta by the stencils above, J by the cofactor determinant and the
+// nine inverse metrics by cofactor / J (src/metrics_kernel.cu:55-70).
+__global__ void metrics_nodes(Dims d, const double* x, const double* y, const double* z, Met M) {
+  const long N = (long)d.IM * d.JM * d.KM;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= N) return;
+  const int i = (int)(e % d.IM);
+  const long r = e / d.IM;
+  const int j = (int)(r % d.JM), k = (int)(r / d.JM);
+  const long sj = d.IM, sk = (long)d.IM * d.JM;
+  const double xx = dax(x + e, 1, i, d.IM), xe = dax(x + e, sj, j, d.JM), xz = dax(x + e, sk, k, d.KM);
+  const double yx = dax(y + e, 1, i, d.IM), ye = dax(y + e, sj, j, d.JM), yz = dax(y + e, sk, k, d.KM);
+  const double zx = dax(z + e, 1, i, d.IM), ze = dax(z + e, sj, j, d.JM), zz = dax(z + e, sk, k, d.KM);
+  const double J = -xe * yx * zz + xe * yz * zx + xx * ye * zz - xx * yz * ze - xz * ye * zx + xz * yx * ze;
+  const long o = node_off(d, i, j, k);
+  M.m[9][o] = J;
+  M.m[0][o] = (ye * zz - yz * ze) / J;
+  M.m[1][o] = (-xe * zz + xz * ze) / J;
+  M.m[2][o] = (xe * yz - xz * ye) / J;
+  M.m[3][o] = (-yx * zz + yz * zx) / J;
+  M.m[4][o] = (xx * zz - xz * zx) / J;
+  M.m[5][o] = (-xx * yz + xz * yx) / J;
+  M.m[6][o] = (-ye * zx + yx * ze) / J;
+  M.m[7][o] = (xe * zx - xx * ze) / J;
+  M.m[8][o] = (-xe * yx + xx * ye) / J;
+}
+
+// Ghost faces, edges and corners take the value of the nearest boundary node
+// (the clamped index), which is what metrics_kernel.cu:72-560 writes.
+__global__ void metrics_ghosts(Dims d, Met M) {
+  const long NGt = (long)d.IG * d.JG * d.KG;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= NGt) return;
+  const int i = (int)(e % d.IG) - NG;
+  const long r = e / d.IG;
+  const int j = (int)(r % d.JG) - NG, k = (int)(r / d.JG) - NG;
+  if (i >= 0 && i < d.IM && j >= 0 && j < d.JM && k >= 0 && k < d.KM) return;
+  const int ci = min(max(i, 0), d.IM - 1), cj = min(max(j, 0), d.JM - 1), ck = min(max(k, 0), d.KM - 1);
+  const long o = node_off(d, i, j, k), c = node_off(d, ci, cj, ck);
+#pragma unroll
+  for (int m = 0; m < 10; ++m) M.m[m][o] = M.m[m][c];
+}
+
+struct Prims {
+  double* p[6];
+};
+
+__device__ __forceinline__ bool ghosted_node(const Dims& d, long e, int& i, int& j, int& k) {
+  if (e >= (long)d.IG * d.JG * d.KG) return false;
+  i = (int)(e % d.IG) - NG;
+  const long r = e / d.IG;
+  j = (int)(r % d.JG) - NG;
+  k = (int)(r / d.JG) - NG;
+  return true;
+}
+
+// src/initial_condition_kernel.cu:13-47: uniform free stream at the angle of attack.
+__global__ void ic_kernel(Dims d, Prims P, double cu, double sv, double p_inf, int viscous) {
+  int i, j, k;
+  if (!ghosted_node(d, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const long o = node_off(d, i, j, k);
+  P.p[0][o] = 1.0;
+  P.p[1][o] = cu;
+  P.p[2][o] = sv;
+  P.p[3][o] = 0.0;
+  P.p[4][o] = p_inf;
+  if (viscous) P.p[5][o] = 1.0;
+}
+
+// src/conservative_kernel.cu:13-48 over the whole ghosted box.
+__global__ void conservative_kernel(Dims d, Prims P, double* q, double gam1) {
+  int i, j, k;
+  if (!ghosted_node(d, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const long o = node_off(d, i, j, k), V = d.VOL;
+  const double r = P.p[0][o], uu = P.p[1][o], vv = P.p[2][o], ww = P.p[3][o], pp = P.p[4][o];
+  q[o] = r;
+  q[V + o] = r * uu;
+  q[2 * V + o] = r * vv;
+  q[3 * V + o] = r * ww;
+  q[4 * V + o] = pp / gam1 + 0.5 * r * (uu * uu + vv * vv + ww * ww);
+}
+
+// src/primitive_kernel.cu:13-51 over the whole ghosted box (with T).
+__global__ void primitive_kernel(Dims d, const double* q, Prims P, double gam1, double gM2) {
+  int i, j, k;
+  if (!ghosted_node(d, blockIdx.x * (long)blockDim.x + threadIdx.x, i, j, k)) return;
+  const long o = node_off(d, i, j, k), V = d.VOL;
+  const double r = q[o], uu = q[V + o] / r, vv = q[2 * V + o] / r, ww = q[3 * V + o] / r;
+  const double pp = gam1 * (q[4 * V + o] - 0.5 * r * (uu * uu + vv * vv + ww * ww));
+  P.p[0][o] = r;
+  P.p[1][o] = uu;
+  P.p[2][o] = vv;
+  P.p[3][o] = ww;
+  P.p[4][o] = pp;
+  P.p[5][o] = gM2 * pp / r;
+}
+
+// dense AoS ghosted (n + 5*(i + IM_G*(j + JM_G*k))) <-> SoA padded
+__global__ void aos_to_soa(Dims d, const double* aos, double* q) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (!ghosted_node(d, e, i, j, k)) return;
+  const long o = node_off(d, i, j, k);
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) q[n * d.VOL + o] = aos[5 * e + n];
+}
+__global__ void soa_to_aos(Dims d, const double* q, double* aos) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (!ghosted_node(d, e, i, j, k)) return;
+  const long o = node_off(d, i, j, k);
+#pragma unroll
+  for (int n = 0; n < NEQ; ++n) aos[5 * e + n] = q[n * d.VOL + o];
+}
+
+// field over the N nodes -> dense IM*JM*KM
+__global__ void gather_nodes(Dims d, const double* f, double* out) {
+  const long N = (long)d.IM * d.JM * d.KM;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= N) return;
+  const int i = (int)(e % d.IM);
+  const long r = e / d.IM;
+  out[e] = f[node_off(d, i, (int)(r % d.JM), (int)(r / d.JM))];
+}
+// field over the ghosted box -> dense IM_G*JM_G*KM_G
+__global__ void gather_ghosted(Dims d, const double* f, double* out) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (!ghosted_node(d, e, i, j, k)) return;
+  out[e] = f[node_off(d, i, j, k)];
+}
+
+// stand-alone gradient of a dense field (src/calc_gradient.cu, gradient_kernel)
+__global__ void gradient_dense(int IM, int JM, int KM, const double* f, double* fx, double* fy, double* fz) {
+  const long N = (long)IM * JM * KM;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= N) return;
+  const int i = (int)(e % IM);
+  const long r = e / IM;
+  const int j = (int)(r % JM), k = (int)(r / JM);
+  fx[e] = dax(f + e, 1, i, IM);
+  fy[e] = dax(f + e, IM, j, JM);
+  fz[e] = dax(f + e, (long)IM * JM, k, KM);
+}
+
+inline unsigned nb(long n) { return (unsigned)((n + 255) / 256); }
+
+}  // namespace
+
+cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, const double* z, double* const met[10],
+                           cudaStream_t s) {
+  Met M;
+  for (int m = 0; m < 10; ++m) M.m[m] = met[m];
+  metrics_nodes<<<nb((long)d.IM * d.JM * d.KM), 256, 0, s>>>(d, x, y, z, M);
+  metrics_ghosts<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ic(const Dims& d, double* const prim[6], double angle_deg, double p_inf, int viscous,
+                      cudaStream_t s) {
+  Prims P;
+  for (int m = 0; m < 6; ++m) P.p[m] = prim[m];
+  const double PI = 3.14159265358979323846;
+  const double AoA = angle_deg * PI / 180.0;
+  ic_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, P, cos(AoA), sin(AoA), p_inf, viscous);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_conservative(const Dims& d, double* const prim[6], double* q, double gam1, cudaStream_t s) {
+  Prims P;
+  for (int m = 0; m < 6; ++m) P.p[m] = prim[m];
+  conservative_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, P, q, gam1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_primitive(const Dims& d, const double* q, double* const prim[6], double gam1, double gM2,
+                             cudaStream_t s) {
+  Prims P;
+  for (int m = 0; m < 6; ++m) P.p[m] = prim[m];
+  primitive_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, q, P, gam1, gM2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_aos_to_soa(const Dims& d, const double* aos, double* q, cudaStream_t s) {
+  aos_to_soa<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, aos, q);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_soa_to_aos(const Dims& d, const double* q, double* aos, cudaStream_t s) {
+  soa_to_aos<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, q, aos);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_nodes(const Dims& d, const double* f, double* out, cudaStream_t s) {
+  gather_nodes<<<nb((long)d.IM * d.JM * d.KM), 256, 0, s>>>(d, f, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_ghosted(const Dims& d, const double* f, double* out, cudaStream_t s) {
+  gather_ghosted<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, f, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gradient_dense(int IM, int JM, int KM, const double* f, double* fx, double* fy, double* fz,
+                                  cudaStream_t s) {
+  gradient_dense<<<nb((long)IM * JM * KM), 256, 0, s>>>(IM, JM, KM, f, fx, fy, fz);
+  return cudaGetLastError();
+}
+
+}  // namespace cbns

@@ -1,0 +1,22 @@
+// setup.cuh - launch interface of the setup and I/O kernels (setup.cu).
+#pragma once
+
+#include "cbns_common.cuh"
+
+namespace cbns {
+
+cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, const double* z, double* const met[10],
+                           cudaStream_t s);
+cudaError_t launch_ic(const Dims& d, double* const prim[6], double angle_deg, double p_inf, int viscous,
+                      cudaStream_t s);
+cudaError_t launch_conservative(const Dims& d, double* const prim[6], double* q, double gam1, cudaStream_t s);
+cudaError_t launch_primitive(const Dims& d, const double* q, double* const prim[6], double gam1, double gM2,
+                             cudaStream_t s);
+cudaError_t launch_aos_to_soa(const Dims& d, const double* aos, double* q, cudaStream_t s);
+cudaError_t launch_soa_to_aos(const Dims& d, const double* q, double* aos, cudaStream_t s);
+cudaError_t launch_gather_nodes(const Dims& d, const double* f, double* out, cudaStream_t s);
+cudaError_t launch_gather_ghosted(const Dims& d, const double* f, double* out, cudaStream_t s);
+cudaError_t launch_gradient_dense(int IM, int JM, int KM, const double* f, double* fx, double* fy, double* fz,
+                                  cudaStream_t s);
+
+}  // namespace cbns

@@ -1,0 +1,343 @@
+// stage.cu - one SSP-RK3 stage in one kernel: inviscid WENO5-char/LF fluxes in
+// all three directions, their differences, the viscous divergence, division by
+// J and the Shu-Osher stage combination, for every interior node.
+//
+// Replaces, for one stage, the reference's
+//   calc_numerical_flux  (src/calc_numerical_flux.cu:15-74; three face kernels
+//                         writing Ep/Fp/Gp to HBM)
+//   viscous_contribution_kernel (src/viscous_contribution_kernel.cu:13-71)
+//   update_rk3 / rk3_kernel     (src/time_integration.cu:15-40,
+//                                src/runge_kutta_kernel.cu:13-80)
+// and, in stage 3 of an inviscid step, the per-node half of calc_dt
+// (src/time_step_kernel.cu:13-96) for interior nodes.
+//
+// Tiling (2.5D).  A CTA of 256 threads owns a TI x TJ = 16 x 15 column of
+// interior nodes and marches it through a chunk of k planes.  Per plane:
+//   ring   : the conservative state of the column on the 6 planes k-2..k+3
+//            (stencil of the k-faces), loaded one new plane per step;
+//   plane  : plane k with a 3-node halo in i and j (stencils of i/j faces);
+//   round A: the 17 x 15 i-faces of plane k  (thread f -> face f, f < 255)
+//   round B: the 16 x 16 j-faces of plane k  (thread f -> face f)
+//   round C: the k+1/2 face of each column   (thread t -> column t, t < 240);
+//            the k-1/2 flux is carried in registers from the previous plane.
+// Every thread computes 3 faces per plane; face fluxes never leave the SM.
+// HBM traffic per node and stage: the stage input (40 B, halos from L2),
+// metrics (80 B), the RK base/partial states (0-80 B) and the output (40 B).
+#include "cbns_common.cuh"
+#include "face_flux.cuh"
+#include "stage.cuh"
+
+namespace cbns {
+
+namespace {
+
+constexpr int TI = 16, TJ = 15, H = 3;
+constexpr int PW = TI + 2 * H;  // 22
+constexpr int PH = TJ + 2 * H;  // 21
+constexpr int NC = TI * TJ;     // 240 columns
+constexpr int NT = 256;         // threads
+constexpr int NFI = (TI + 1) * TJ;  // 255 i-faces
+constexpr int NFJ = TI * (TJ + 1);  // 256 j-faces
+
+template <typename S, typename R>
+struct Smem {
+  S ring[6][NEQ][NC];
+  S plane[NEQ][PH][PW];
+  R fi[NEQ][TJ][TI + 1];
+  R fj[NEQ][TJ + 1][TI];
+};
+
+template <typename R>
+__device__ __forceinline__ void face_normal(const StageArgs& a, long oa, long ob, int dir, R& nx, R& ny,
+                                            R& nz) {
+  const double Ja = __ldg(a.met[9] + oa), Jb = __ldg(a.met[9] + ob);
+  nx = (R)(0.5 * (__ldg(a.met[3 * dir + 0] + oa) * Ja + __ldg(a.met[3 * dir + 0] + ob) * Jb));
+  ny = (R)(0.5 * (__ldg(a.met[3 * dir + 1] + oa) * Ja + __ldg(a.met[3 * dir + 1] + ob) * Jb));
+  nz = (R)(0.5 * (__ldg(a.met[3 * dir + 2] + oa) * Ja + __ldg(a.met[3 * dir + 2] + ob) * Jb));
+}
+
+// 4th-order central derivative of a node field along a stride, at offset o.
+__device__ __forceinline__ double d4(const double* f, long o, long s) {
+  return (1.0 / 12.0) * __ldg(f + o - 2 * s) - (2.0 / 3.0) * __ldg(f + o - s) + (2.0 / 3.0) * __ldg(f + o + s) -
+         (1.0 / 12.0) * __ldg(f + o + 2 * s);
+}
+
+template <typename R, bool VISC, int MODE>
+__global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
+  using S = R;  // shared-memory storage type
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem<S, R>& sm = *reinterpret_cast<Smem<S, R>*>(smem_raw);
+
+  const StepState* st = a.st;
+  if (MODE != 0 && st->done) return;
+  const double dt = (MODE != 0) ? st->dt : 0.0;
+
+  const Dims& d = a.d;
+  const int t = threadIdx.x;
+  const int tile = blockIdx.x;
+  const int ti0 = 1 + TI * (tile % a.ntile_i);
+  const int tj0 = 1 + TJ * (tile / a.ntile_i);
+  const int kb = 1 + a.kchunk * blockIdx.y;
+  const int ke = min(kb + a.kchunk, d.KM - 1);
+  if (kb >= ke) return;
+  const long VOL = d.VOL;
+
+  const FluxConsts<R> C{(R)a.gamma, (R)a.gam1, (R)a.gam1_inv};
+
+  // column owned by this thread
+  const int cx = t % TI, cy = t / TI;
+  const int ci = ti0 + cx, cj = tj0 + cy;
+  const bool col_thread = t < NC;
+  const bool col_valid = col_thread && ci <= d.IM - 2 && cj <= d.JM - 2;
+
+  auto load_ring = [&](int kp) {
+    if (col_thread) {
+      S* dst = &sm.ring[(kp + 6) % 6][0][t];
+      if (ci <= d.IM + 1 && cj <= d.JM + 1) {
+        const long o = node_off(d, ci, cj, kp);
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) dst[n * NC] = (S)__ldg(a.src + n * VOL + o);
+      }
+    }
+  };
+
+  // k-face between planes kk and kk+1 of this thread's column
+  auto k_face = [&](int kk, R out[5]) {
+    const int s0 = (kk - 2 + 6) % 6;
+    auto ld = [&](int p, int n) -> R {
+      int s = s0 + p;
+      s = s >= 6 ? s - 6 : s;
+      return (R)sm.ring[s][n][t];
+    };
+    R nx, ny, nz;
+    face_normal<R>(a, node_off(d, ci, cj, kk), node_off(d, ci, cj, kk + 1), 2, nx, ny, nz);
+    face_flux<R>(ld, nx, ny, nz, C, out);
+  };
+
+  // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
+  for (int kp = kb - 3; kp <= kb + 2; ++kp) load_ring(kp);
+  __syncthreads();
+  R fkm[5] = {0, 0, 0, 0, 0};
+  if (col_valid) k_face(kb - 1, fkm);
+
+  double smax = 0.0;  // running spectral-radius max (stage 3, inviscid)
+  bool snan = false;
+
+  for (int k = kb; k < ke; ++k) {
+    __syncthreads();
+    load_ring(k + 3);
+    // plane k with halo: interior from the ring, halo from global memory
+    {
+      const int sk = k % 6;
+      for (int e = t; e < NC; e += NT) {
+        const int x = e % TI, y = e / TI;
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = sm.ring[sk][n][e];
+      }
+      // halo: 6 columns x TJ rows (i-halo) then 6 rows x TI columns (j-halo)
+      constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;
+      for (int e = t; e < NHI + NHJ; e += NT) {
+        int x, y;
+        if (e < NHI) {
+          const int c6 = e % (2 * H);
+          y = e / (2 * H);
+          x = c6 < H ? c6 - H : TI + (c6 - H);
+        } else {
+          const int e2 = e - NHI;
+          const int r6 = e2 / TI;
+          x = e2 % TI;
+          y = r6 < H ? r6 - H : TJ + (r6 - H);
+        }
+        const int gi = ti0 + x, gj = tj0 + y;
+        if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+          const long o = node_off(d, gi, gj, k);
+#pragma unroll
+          for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = (S)__ldg(a.src + n * VOL + o);
+        }
+      }
+    }
+    __syncthreads();
+
+    // round A: i-faces.  Face fx (0..TI) of row fy lies between tile columns fx-1 and fx.
+    if (t < NFI) {
+      const int fx = t % (TI + 1), fy = t / (TI + 1);
+      const int ga = ti0 + fx - 1, gj = tj0 + fy;
+      if (ga <= d.IM - 2 && gj <= d.JM - 2) {
+        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
+        R nx, ny, nz, f[5];
+        face_normal<R>(a, node_off(d, ga, gj, k), node_off(d, ga + 1, gj, k), 0, nx, ny, nz);
+        face_flux<R>(ld, nx, ny, nz, C, f);
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
+      }
+    }
+    // round B: j-faces.  Face fy (0..TJ) of column fx lies between tile rows fy-1 and fy.
+    if (t < NFJ) {
+      const int fx = t % TI, fy = t / TI;
+      const int gi = ti0 + fx, ga = tj0 + fy - 1;
+      if (gi <= d.IM - 2 && ga <= d.JM - 2) {
+        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
+        R nx, ny, nz, f[5];
+        face_normal<R>(a, node_off(d, gi, ga, k), node_off(d, gi, ga + 1, k), 1, nx, ny, nz);
+        face_flux<R>(ld, nx, ny, nz, C, f);
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
+      }
+    }
+    // round C: the k+1/2 face of this column
+    R fkp[5];
+    if (col_valid) k_face(k, fkp);
+    __syncthreads();
+
+    if (col_valid) {
+      const long o = node_off(d, ci, cj, k);
+      double df[NEQ];
+#pragma unroll
+      for (int n = 0; n < NEQ; ++n)
+        df[n] = (double)(sm.fi[n][cy][cx + 1] - sm.fi[n][cy][cx]) + (double)(sm.fj[n][cy + 1][cx] - sm.fj[n][cy][cx]) +
+                (double)(fkp[n] - fkm[n]);
+      if (VISC) {
+        // viscous divergence; the reference takes the i-derivative at (i,j-1,k-1),
+        // the j-derivative at (i-1,j,k-1), the k-derivative at (i-1,j-1,k)
+        const long sh = a.visdiv == 0 ? 1 : 0;
+        const long oi = o - sh * (d.PX + d.PL), oj = o - sh * (1 + d.PL), ok = o - sh * (1 + d.PX);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+          const double dv = d4(a.vflux[n], oi, 1) + d4(a.vflux[4 + n], oj, d.PX) + d4(a.vflux[8 + n], ok, d.PL);
+          df[n + 1] -= dv;
+        }
+      }
+      const double iJ = 1.0 / __ldg(a.met[9] + o);
+      if (MODE == 0) {
+        const long r = 5L * ((ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * (k - 1)));
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) a.out[r + n] = df[n] * iJ;
+      } else {
+        double q[NEQ];
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) {
+          const double L = dt * (df[n] * iJ);
+          const long e = n * VOL + o;
+          if (MODE == 1) {
+            q[n] = __ldg(a.q0 + e) - L;
+          } else if (MODE == 2) {
+            q[n] = 0.75 * __ldg(a.q0 + e) + 0.25 * (__ldg(a.qp + e) - L);
+          } else {
+            q[n] = (a.q0[e] + 2.0 * (__ldg(a.qp + e) - L)) / 3.0;
+          }
+        }
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) a.out[n * VOL + o] = q[n];
+        if (VISC || a.sigma) {
+          const double r = q[0], ir = 1.0 / r;
+          const double uu = q[1] * ir, vv = q[2] * ir, ww = q[3] * ir;
+          const double pp = a.gam1 * (q[4] - 0.5 * r * (uu * uu + vv * vv + ww * ww));
+          if (VISC) {
+            a.prim[0][o] = r;
+            a.prim[1][o] = uu;
+            a.prim[2][o] = vv;
+            a.prim[3][o] = ww;
+            a.prim[4][o] = pp;
+            a.prim[5][o] = a.gM2 * pp / r;
+          } else {
+            const double cs = sqrt(a.gamma * pp / r);
+            double s = 0.0;
+#pragma unroll
+            for (int dd = 0; dd < 3; ++dd) {
+              const double mx = __ldg(a.met[3 * dd] + o), my = __ldg(a.met[3 * dd + 1] + o),
+                           mz = __ldg(a.met[3 * dd + 2] + o);
+              s += fabs(uu * mx + vv * my + ww * mz) + cs * sqrt(mx * mx + my * my + mz * mz);
+            }
+            if (s != s) snan = true;
+            smax = fmax(smax, s);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) fkm[n] = fkp[n];
+  }
+
+  if (MODE != 0 && !VISC && a.sigma) {
+    // CTA max, one atomic per CTA
+    __shared__ double red[NT / 32];
+    __shared__ int rnan;
+    if (t == 0) rnan = 0;
+    double m = smax;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, s));
+    __syncthreads();
+    if (snan) rnan = 1;
+    if ((t & 31) == 0) red[t >> 5] = m;
+    __syncthreads();
+    if (t == 0) {
+      for (int w = 1; w < NT / 32; ++w) m = fmax(m, red[w]);
+      atomic_max_sigma(&a.st->sigma_bits, rnan ? __longlong_as_double(0x7ff8000000000000ll) : m);
+    }
+  }
+}
+
+template <typename R, bool VISC, int MODE>
+cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
+  const size_t smem = sizeof(Smem<R, R>);
+  dim3 grid(a.ntile_i * a.ntile_j, (a.d.KM - 2 + a.kchunk - 1) / a.kchunk);
+  stage_kernel<R, VISC, MODE><<<grid, NT, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R, bool VISC, int MODE>
+void prepare_t() {
+  cudaFuncSetAttribute(stage_kernel<R, VISC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(Smem<R, R>));
+}
+
+template <typename R, bool VISC>
+void prepare_rv() {
+  prepare_t<R, VISC, 0>();
+  prepare_t<R, VISC, 1>();
+  prepare_t<R, VISC, 2>();
+  prepare_t<R, VISC, 3>();
+}
+
+template <typename R>
+cudaError_t launch_r(const StageArgs& a, int mode, bool visc, cudaStream_t s) {
+  if (visc) {
+    switch (mode) {
+      case 0: return launch_t<R, true, 0>(a, s);
+      case 1: return launch_t<R, true, 1>(a, s);
+      case 2: return launch_t<R, true, 2>(a, s);
+      default: return launch_t<R, true, 3>(a, s);
+    }
+  }
+  switch (mode) {
+    case 0: return launch_t<R, false, 0>(a, s);
+    case 1: return launch_t<R, false, 1>(a, s);
+    case 2: return launch_t<R, false, 2>(a, s);
+    default: return launch_t<R, false, 3>(a, s);
+  }
+}
+
+}  // namespace
+
+// Raise the dynamic shared-memory limit of every instantiation once (outside
+// any stream capture).
+void stage_prepare() {
+  static bool done = false;
+  if (done) return;
+  prepare_rv<double, false>();
+  prepare_rv<double, true>();
+  prepare_rv<float, false>();
+  prepare_rv<float, true>();
+  done = true;
+}
+
+void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j) {
+  *ntile_i = (d.IM - 2 + TI - 1) / TI;
+  *ntile_j = (d.JM - 2 + TJ - 1) / TJ;
+}
+
+cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, cudaStream_t s) {
+  return fp32 ? launch_r<float>(a, mode, visc, s) : launch_r<double>(a, mode, visc, s);
+}
+
+}  // namespace cbns

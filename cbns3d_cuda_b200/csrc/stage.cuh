@@ -1,0 +1,28 @@
+// stage.cuh - launch interface of the fused RK3 stage kernel (stage.cu).
+#pragma once
+
+#include "cbns_common.cuh"
+
+namespace cbns {
+
+struct StageArgs {
+  Dims d;
+  double gamma, gam1, gam1_inv, gM2;
+  const double* src;   // stage input (stencil source), 5 fields
+  const double* q0;    // the reference's Q at the node (RK base)
+  const double* qp;    // the reference's Q_p at the node (stages 2, 3)
+  double* out;         // stage output (5 fields), or the dense RHS array in mode 0
+  const double* met[10];
+  const double* vflux[12];
+  double* prim[6];     // viscous: rho,u,v,w,p,T of the new interior state
+  StepState* st;       // dt, done flag, spectral-radius max
+  int ntile_i, ntile_j, kchunk;
+  int visdiv;          // CBNS_VISDIV_*
+  int sigma;           // accumulate the interior spectral-radius max (inviscid stage 3)
+};
+
+// mode 0: dense RHS output; 1..3: RK stage.  fp32: split-precision flux arithmetic.
+cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, cudaStream_t s);
+void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j);
+
+}  // namespace cbns

@@ -1,0 +1,24 @@
+// step.cuh - launch interface of the time-step bookkeeping kernels (step.cu).
+#pragma once
+
+#include "cbns_common.cuh"
+
+namespace cbns {
+
+struct SigmaArgs {
+  Dims d;
+  double gamma, gam1, C_dt_v;
+  int viscous;
+  const double* q;        // inviscid: primitives recomputed from this buffer
+  const double* prim[6];  // viscous: rho,u,v,w,p,T
+  const double* mu;       // viscous
+  const double* met[10];
+  StepState* st;
+};
+
+// Zero the accumulator and reduce the spectral radius over all grid nodes.
+cudaError_t launch_sigma_nodes(const SigmaArgs& a, cudaStream_t s);
+cudaError_t launch_step_prologue(StepState* st, double CFL, cudaStream_t s);
+cudaError_t launch_set_dt(StepState* st, double dt, cudaStream_t s);
+
+}  // namespace cbns

@@ -1,0 +1,23 @@
+// visc.cuh - launch interface of the viscous node-flux kernel (visc.cu).
+#pragma once
+
+#include "cbns_common.cuh"
+
+namespace cbns {
+
+struct ViscArgs {
+  Dims d;
+  double gamma, Re_inv, C_T_inf, C_dt_v;
+  double qc;                 // -1/(Pr (gamma-1) M^2): heat-flux factor before mu/Re
+  const double* prim[6];     // rho,u,v,w,p,T
+  const double* met[10];
+  double* vflux[12];         // E0..E3, F0..F3, G0..G3
+  double* mu;
+  StepState* st;
+  int check_done;
+  int sigma;                 // accumulate the spectral-radius max over the grid nodes
+};
+
+cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s);
+
+}  // namespace cbns

@@ -1,0 +1,44 @@
+// cbns3d.cpp - command-line entry of the B200 solver (the reference's
+// src/cbns3d.cpp:17-25 with options).  Reads input.txt in the working
+// directory like the reference.
+//   --quiet          no per-step output line
+//   --graph          whole steps replayed from a CUDA graph, dt on the device
+//   --precision P    fp64 (default) | split
+//   --visdiv D       reference (default) | centered
+//   --inviscid / --viscous   override the build-time default
+//   --input FILE     parameter file (default input.txt)
+#include <cstring>
+#include <iostream>
+#include <string>
+
+#include "Block3d.h"
+
+int main(int argc, char** argv) {
+  Block3d::Options o;
+  for (int a = 1; a < argc; ++a) {
+    const std::string s = argv[a];
+    auto next = [&]() -> std::string {
+      if (a + 1 >= argc) {
+        std::cerr << "missing value after " << s << "\n";
+        std::exit(2);
+      }
+      return argv[++a];
+    };
+    if (s == "--quiet") o.quiet = true;
+    else if (s == "--graph") o.graph = true;
+    else if (s == "--inviscid") o.viscous = 0;
+    else if (s == "--viscous") o.viscous = 1;
+    else if (s == "--input") o.input = next();
+    else if (s == "--precision") {
+      const std::string v = next();
+      o.precision = v == "split" ? CBNS_PREC_SPLIT : CBNS_PREC_FP64;
+    } else if (s == "--visdiv") {
+      o.vis_divergence = next() == "centered" ? CBNS_VISDIV_CENTERED : CBNS_VISDIV_REFERENCE;
+    } else {
+      std::cerr << "unknown option " << s << "\n";
+      return 2;
+    }
+  }
+  Block3d block(o);
+  return block.solve();
+}

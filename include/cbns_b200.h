@@ -1,0 +1,158 @@
+/*
+ * cbns_b200.h - C ABI of the B200 (sm_100a) implementation of the cbns3d_cuda
+ * RK3 right-hand-side path.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (CBNS_OK on success); nothing here calls exit() or throws.  The library owns
+ * its device memory (structure-of-arrays, FP64 state), launches on the stream
+ * given by cbns_set_stream (default: the legacy default stream) and keeps the
+ * reference's synchronous contract: each call below returns after its work is
+ * complete on the device unless its comment says otherwise.
+ *
+ * Reference interface each entry point replaces (paths inside the reference
+ * project chenbei102/cbns3d_cuda):
+ *   cbns_create                   copy_block_info   include/copy_block_info.h:9
+ *                                 + allocate_mem    include/allocate_mem.h:9
+ *   cbns_destroy                  free_mem          include/free_mem.h:9
+ *   cbns_calc_metrics             calc_metrics      include/calc_metrics.h:9
+ *   cbns_get_metrics              get_metrics       include/get_metrics.h:9
+ *   cbns_initial_condition        initial_condition include/initial_condition.h:9
+ *   cbns_calc_conservative        calc_conservative include/calc_conservative.h:9
+ *   cbns_set_conservative         set_conservative  include/set_conservative.h:9
+ *   cbns_get_conservative         get_conservative  include/get_conservative.h:9
+ *   cbns_get_primitive            get_primitive     include/get_primitive.h:9
+ *   cbns_calc_primitive           calc_primitive    include/calc_primitive.h:9-10
+ *   cbns_set_bc_calc_primitive    set_bc_calc_primitive include/set_bc_calc_primitive.h:9
+ *   cbns_calc_numerical_flux      calc_numerical_flux   include/calc_numerical_flux.h:9
+ *   cbns_calc_viscous_terms       calc_viscous_terms    include/calc_viscous_terms.h:9
+ *   cbns_calc_viscous_flux_contribution
+ *                                 calc_viscous_flux_contribution
+ *                                                   include/calc_viscous_flux_contribution.h:9
+ *   cbns_update_rk3               update_rk3        include/time_integration.h:9-10
+ *   cbns_calc_dt                  calc_dt           include/calc_dt.h:9
+ *   cbns_calc_gradient            calc_gradient     include/calc_gradient.h:9
+ *   cbns_run                      the time loop of Block3d::solve, src/Block3d.cpp:237-293
+ * The remaining entry points (stream, time, timing, RHS evaluation) have no
+ * single reference counterpart; their comments say what they are for.
+ */
+#ifndef CBNS_B200_H_
+#define CBNS_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define CBNS_OK               0
+#define CBNS_ERR_ARG          1  /* bad argument (null pointer, bad size, bad enum)    */
+#define CBNS_ERR_CUDA         2  /* a CUDA runtime call or kernel launch failed        */
+#define CBNS_ERR_NAN_DT       3  /* the CFL time step is NaN (calc_dt.cu:56-58 throws) */
+#define CBNS_ERR_STATE        4  /* call out of order (e.g. stepping before metrics)   */
+#define CBNS_ERR_UNSUPPORTED  5  /* option not available in this build                 */
+#define CBNS_ERR_NOMEM        6  /* device allocation failed                           */
+#define CBNS_ERR_TOO_LARGE    7  /* size beyond a fixed limit of the entry point       */
+
+/* Which state buffer a call acts on: the reference passes block_data->Q or
+ * block_data->Q_p explicitly (src/Block3d.cpp:249-284). */
+#define CBNS_Q   0
+#define CBNS_QP  1
+
+/* Arithmetic of the inviscid face flux. */
+#define CBNS_PREC_FP64    0  /* plain path, FP64 throughout (parity with the reference) */
+#define CBNS_PREC_SPLIT   1  /* FP32 reconstruction + flux, FP64 state/metrics/reductions */
+#define CBNS_PREC_HYBRID  2  /* SPLIT + learned shock sensor choosing WENO5 or upwind-5 */
+
+/* Where the viscous flux divergence is evaluated. */
+#define CBNS_VISDIV_REFERENCE 0 /* as src/viscous_contribution_kernel.cu:269-288: each
+                                   directional derivative taken at the node shifted by -1
+                                   in both transverse directions                        */
+#define CBNS_VISDIV_CENTERED  1 /* every derivative taken at the node itself           */
+
+/* Run parameters: the fields of Block3dInfo that Block3d::read_input fills
+ * (src/Block3d.cpp:33-138, include/Block3d_cuda.h:32-78) plus build-time
+ * switches of the reference that are run-time options here.  The derived
+ * quantities (Mach^2, gamma*M^2, p_inf = 1/(gamma M^2), Sutherland constant
+ * 110.5/T_inf, C_dt_v, ...) are computed inside cbns_create exactly as
+ * src/Block3d.cpp:99-113 computes them. */
+typedef struct cbns_params {
+  unsigned IM, JM, KM;      /* grid points per direction (each >= 4)              */
+  double   CFL;
+  double   angle_attack;    /* degrees                                             */
+  unsigned i_begin, i_end;  /* j=0 face: wake cut for i < i_begin-1, wall for
+                               i < i_end (unsigned arithmetic, as the reference)   */
+  double   Mach, Re, gamma, Pr, Pr_t, T_inf;
+  int      viscous;         /* 0: INVIS_MODE=ON build; 1: viscous build            */
+  int      precision;       /* CBNS_PREC_*                                         */
+  int      vis_divergence;  /* CBNS_VISDIV_*                                       */
+  int      reserved[5];     /* must be zero                                        */
+} cbns_params;
+
+typedef struct cbns_ctx cbns_ctx;
+
+/* Lifecycle. */
+int cbns_create(const cbns_params* params, cbns_ctx** out);
+int cbns_destroy(cbns_ctx* ctx);
+/* Launch stream for every later call (a cudaStream_t passed as void*). */
+int cbns_set_stream(cbns_ctx* ctx, void* stream);
+const char* cbns_status_string(int status);
+
+/* Setup and I/O.  Host arrays: x,y,z are IM*JM*KM, i fastest (Plot3D order);
+ * Q is the reference's AoS ghosted layout n + 5*(i + IM_G*(j + JM_G*k)) with
+ * IM_G = IM+4 etc. (include/Block3d_cuda.h:100-108), i.e. the checkpoint body. */
+int cbns_calc_metrics(cbns_ctx* ctx, const double* x, const double* y, const double* z);
+int cbns_get_metrics(cbns_ctx* ctx, double* xi_x, double* xi_y, double* xi_z,
+                     double* eta_x, double* eta_y, double* eta_z,
+                     double* zeta_x, double* zeta_y, double* zeta_z, double* Jac);
+int cbns_initial_condition(cbns_ctx* ctx);
+int cbns_calc_conservative(cbns_ctx* ctx, int which);
+int cbns_set_conservative(cbns_ctx* ctx, const double* Q_host);
+int cbns_get_conservative(cbns_ctx* ctx, int which, double* Q_host);
+/* Ghosted primitive arrays (IM_G*JM_G*KM_G each); T may be null. */
+int cbns_get_primitive(cbns_ctx* ctx, double* rho, double* u, double* v, double* w,
+                       double* p, double* T);
+
+/* The RK3 right-hand-side path, one reference entry point each. */
+int cbns_set_bc_calc_primitive(cbns_ctx* ctx, int which);
+int cbns_calc_primitive(cbns_ctx* ctx, int which);
+int cbns_calc_numerical_flux(cbns_ctx* ctx, int which);
+int cbns_calc_viscous_terms(cbns_ctx* ctx);
+int cbns_calc_viscous_flux_contribution(cbns_ctx* ctx);
+int cbns_update_rk3(cbns_ctx* ctx, double dt, unsigned stage);
+int cbns_calc_dt(cbns_ctx* ctx, double* dt);
+
+/* Whole SSP-RK3 steps with the time step kept on the device: per step the CFL
+ * dt is formed from the previous step's spectral-radius maximum, clamped to
+ * t_end - t_cur, and the loop stops once t_cur + 1e-8 > t_end, as the time
+ * loop of src/Block3d.cpp:237-293 does.  Steps are replayed from a CUDA graph.
+ * *steps_done (may be null) receives the steps actually taken. */
+int cbns_run(cbns_ctx* ctx, unsigned nsteps, double t_end, unsigned* steps_done);
+/* Same as cbns_run but returns without synchronising (steps_done unavailable). */
+int cbns_run_async(cbns_ctx* ctx, unsigned nsteps, double t_end);
+int cbns_set_time(cbns_ctx* ctx, double t_cur);
+int cbns_get_time(cbns_ctx* ctx, double* t_cur, double* dt_last);
+
+/* One right-hand-side evaluation for testing: rhs[n + 5*(i + (IM-2)*(j + (JM-2)*k))]
+ * = ((E_{i+1/2}-E_{i-1/2}) + (F..) + (G..) - dfv)/J at interior node (i+1,j+1,k+1),
+ * the quantity rk3_kernel forms (src/runge_kutta_kernel.cu:45-66).  The buffer's
+ * boundary conditions (and viscous terms) must be current.  rhs is a host array. */
+int cbns_eval_rhs(cbns_ctx* ctx, int which, double* rhs_host);
+
+/* The 4th-order gradient of a standalone IM*JM*KM field (test helper of the
+ * reference, src/calc_gradient.cu:17-51).  All arrays are host arrays. */
+int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f,
+                       double* fx, double* fy, double* fz);
+
+/* Per-kernel device timing with CUDA events on the launch stream.  Kernel ids:
+ * 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous node
+ * fluxes, 3 dt/step bookkeeping.  total_ms is the summed event time. */
+int cbns_prof_enable(cbns_ctx* ctx, int on);
+int cbns_prof_read(cbns_ctx* ctx, int kernel_id, double* total_ms, unsigned* launches);
+int cbns_prof_reset(cbns_ctx* ctx);
+/* Number of kernels this context launched since creation (or the last reset). */
+int cbns_launch_count(cbns_ctx* ctx, unsigned long long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CBNS_B200_H_ */

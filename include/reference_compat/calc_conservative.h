@@ -1,0 +1,7 @@
+/* calc_conservative.h - forwarding header with the reference's file name (its include/calc_conservative.h):
+ * host code written against the reference's headers compiles unchanged against
+ * libcbns_b200 when this directory precedes the reference's include directory. */
+#ifndef CBNS_COMPAT_CALC_CONSERVATIVE_H_
+#define CBNS_COMPAT_CALC_CONSERVATIVE_H_
+#include "../block3d_cuda.h"
+#endif

@@ -43,7 +43,7 @@ def golden_cases():
     c.params = dict(c.params, i_begin=1, i_end=20, viscous=True, Re=200.0, T_inf=288.15)
     out["vortex_viscous_wall"] = (c, 10)
 
-    c = cases.case_naca(32, 16, 6)  # free-stream start (is_restart = 1), viscous, wall
+    c = cases.case_naca(32, 16, 6, first=1e-3)  # free-stream start (is_restart = 1), viscous, wall
     out["naca_viscous_freestream"] = (c, 10)
     return out
 
@@ -59,7 +59,8 @@ def run_reference(case, nsteps, workdir: Path):
     dts = []
     for line in r.stdout.splitlines():
         parts = [p.strip() for p in line.split(",")]
-        if len(parts) == 3:
+        # step lines are "n, dt, t"; the mesh-size line "IM, JM, KM" has no decimal point
+        if len(parts) == 3 and any(ch in parts[1] for ch in ".eE"):
             try:
                 int(parts[0])
                 dts.append(float(parts[1]))

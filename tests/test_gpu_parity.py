@@ -125,7 +125,7 @@ def test_steps_wall_and_viscous(graph):
 
 
 def test_steps_naca_freestream_viscous():
-    c = cases.case_naca(48, 24, 6)
+    c = cases.case_naca(48, 24, 6, first=1e-3)
     g, o = pair(c)
     _steps(g, o, 10, graph=True)
     assert max(per_var_rel_linf(g.get_conservative(), o.get_conservative())) <= 1e-10
@@ -134,9 +134,11 @@ def test_steps_naca_freestream_viscous():
 def test_short_dimension_extension():
     """KM = 4: the reference's stencils would index outside the grid; both
     implementations use the 2nd-order extension for the metrics."""
-    c = cases.case_naca(40, 20, 4)
+    c = cases.case_naca(40, 20, 4, first=1e-3)
     g, o = pair(c)
-    assert rel_linf(g.get_metrics(), o.get_metrics()) <= 1e-13
+    # the stretched O-grid's metrics come from differences of nearly equal
+    # coordinates; FMA contraction on the GPU moves them by ~1e-12 relative
+    assert rel_linf(g.get_metrics(), o.get_metrics()) <= 1e-10
     _steps(g, o, 5, graph=True)
     assert max(per_var_rel_linf(g.get_conservative(), o.get_conservative())) <= 1e-10
 

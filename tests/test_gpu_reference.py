@@ -46,23 +46,43 @@ def vtk_fields(path):
 
 
 CASES = {
-    "vortex_c0": (lambda: cases.case_vortex(64, 32, 16), 100, "cbns3d_ref_inv", ["--inviscid"]),
-    "naca_viscous": (lambda: cases.case_naca(64, 32, 6), 50, "cbns3d_ref_visc", ["--viscous"]),
+    "vortex_c0": (lambda: cases.case_vortex(64, 32, 16), 100, "inv"),
+    "naca_viscous": (lambda: cases.case_naca(64, 32, 6, first=1e-3), 50, "visc"),
 }
+# the programs compared with the reference build on identical inputs
+VARIANTS = {
+    "driver": lambda mode: [str(EXE), "--quiet", "--inviscid" if mode == "inv" else "--viscous"],
+    "driver_graph": lambda mode: [str(EXE), "--quiet", "--graph", "--inviscid" if mode == "inv" else "--viscous"],
+    # the reference's own src/Block3d.cpp + src/cbns3d.cpp, unmodified, linked to libcbns_b200
+    "reference_host_dropin": lambda mode: [str(REF / f"cbns3d_dropin_{mode}")],
+}
+_ref_cache = {}
+
+
+def reference_output(name, tmp_root):
+    if name not in _ref_cache:
+        make, n, mode = CASES[name]
+        c = make()
+        d = c.write(tmp_root / f"ref_{name}", nsteps=n, checkpoint_freq=n)
+        out = run([str(REF / f"cbns3d_ref_{mode}")], d)
+        assert "Elapsed Time" in out
+        _ref_cache[name] = (c, d)
+    return _ref_cache[name]
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
-@pytest.mark.parametrize("graph", [False, True])
-def test_driver_matches_reference_build(tmp_path, name, graph):
-    make, n, ref_exe, flags = CASES[name]
-    if not (REF / ref_exe).exists():
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+def test_matches_reference_build(tmp_path_factory, name, variant):
+    make, n, mode = CASES[name]
+    if not (REF / f"cbns3d_ref_{mode}").exists():
         pytest.skip("reference build absent (make -C oracle ref needs the reference sources)")
-    c = make()
-    dref = c.write(tmp_path / "ref", nsteps=n, checkpoint_freq=n)
-    dmine = c.write(tmp_path / "mine", nsteps=n, checkpoint_freq=n)
-    out_ref = run([str(REF / ref_exe)], dref)
-    out_mine = run([str(EXE), "--quiet"] + flags + (["--graph"] if graph else []), dmine)
-    assert "Elapsed Time" in out_ref and "Elapsed Time" in out_mine
+    cmd = VARIANTS[variant](mode)
+    if not Path(cmd[0]).exists():
+        pytest.skip(f"{cmd[0]} not built")
+    c, dref = reference_output(name, tmp_path_factory.getbasetemp())
+    dmine = c.write(tmp_path_factory.mktemp(variant), nsteps=n, checkpoint_freq=n)
+    out_mine = run(cmd, dmine)
+    assert "Elapsed Time" in out_mine
     t_r, Q_r = cases.read_checkpoint(dref / "checkpoint.dat")
     t_m, Q_m = cases.read_checkpoint(dmine / "checkpoint.dat")
     assert abs(t_r - t_m) <= 1e-12 * abs(t_r)

@@ -165,6 +165,11 @@ class Block:
                 self.calc_viscous_terms()
         return t_cur
 
+    def autotune(self) -> int:
+        v = C.c_int()
+        _abi.check(self.lib.cbns_autotune(self.h, C.byref(v)), "cbns_autotune")
+        return v.value
+
     # timing -----------------------------------------------------------------
     def prof_enable(self, on=True):
         _abi.check(self.lib.cbns_prof_enable(self.h, int(on)), "cbns_prof_enable")

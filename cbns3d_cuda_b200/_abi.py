@@ -74,6 +74,7 @@ SIGNATURES = [
     ("cbns_get_time", C.c_int, [_V, _D, _D]),
     ("cbns_eval_rhs", C.c_int, [_V, C.c_int, _D]),
     ("cbns_calc_gradient", C.c_int, [C.c_uint, C.c_uint, C.c_uint, _D, _D, _D, _D]),
+    ("cbns_autotune", C.c_int, [_V, C.POINTER(C.c_int)]),
     ("cbns_prof_enable", C.c_int, [_V, C.c_int]),
     ("cbns_prof_read", C.c_int, [_V, C.c_int, _D, C.POINTER(C.c_uint)]),
     ("cbns_prof_reset", C.c_int, [_V]),

@@ -52,6 +52,7 @@ struct cbns_ctx {
   cudaGraphExec_t gexec = nullptr;
   int g_q = -1, g_p = -1, g_s = -1;
   int ntile_i = 1, ntile_j = 1, kchunk = 1;
+  int stage_variant = 0;  // compiled occupancy variant of the stage kernel (cbns_autotune)
   bool prof = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PK_N];
   std::vector<cudaEvent_t> ev_pool;
@@ -174,9 +175,12 @@ StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const dou
   a.qp = qp;
   a.out = out;
   fill_met(c, a.met);
+  for (int m = 0; m < 10; ++m) a.area[m] = c->f.area[m];
   for (int m = 0; m < 12; ++m) a.vflux[m] = c->f.vflux[m];
   for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
   a.st = c->st;
+  a.q0_is_src = q0 == src;
+  a.qp_is_src = qp == src;
   a.ntile_i = c->ntile_i;
   a.ntile_j = c->ntile_j;
   a.kchunk = c->kchunk;
@@ -187,7 +191,7 @@ StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const dou
 
 int stage_launch(cbns_ctx* c, const StageArgs& a, int mode) {
   Prof p(c, PK_STAGE);
-  CK(launch_stage(a, mode, c->ph.viscous != 0, c->ph.precision != CBNS_PREC_FP64, c->stream));
+  CK(launch_stage(a, mode, c->ph.viscous != 0, c->ph.precision != CBNS_PREC_FP64, c->stage_variant, c->stream));
   c->launches += 1;
   return CBNS_OK;
 }
@@ -352,6 +356,7 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   int rc = CBNS_OK;
   for (int b = 0; b < 3 && rc == CBNS_OK; ++b) rc = dalloc(c, &c->qb[b], (size_t)NEQ * d.VOL);
   for (int m = 0; m < 10 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.met[m], d.VOL);
+  for (int m = 0; m < 10 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.area[m], d.VOL);
   for (int m = 0; m < 7 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.prim[m], d.VOL);
   for (int m = 0; m < 12; ++m) c->f.vflux[m] = nullptr;
   if (p->viscous)
@@ -378,6 +383,7 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   for (void* a : c->allocs) (void)a;
   for (int b = 0; b < 3; ++b) cudaMemsetAsync(c->qb[b], 0, (size_t)NEQ * d.VOL * sizeof(double), c->stream);
   for (int m = 0; m < 10; ++m) cudaMemsetAsync(c->f.met[m], 0, d.VOL * sizeof(double), c->stream);
+  for (int m = 0; m < 10; ++m) cudaMemsetAsync(c->f.area[m], 0, d.VOL * sizeof(double), c->stream);
   for (int m = 0; m < 7; ++m) cudaMemsetAsync(c->f.prim[m], 0, d.VOL * sizeof(double), c->stream);
   if (p->viscous)
     for (int m = 0; m < 12; ++m) cudaMemsetAsync(c->f.vflux[m], 0, d.VOL * sizeof(double), c->stream);
@@ -428,8 +434,8 @@ int cbns_calc_metrics(cbns_ctx* c, const double* x, const double* y, const doubl
   CK(cudaMemcpyAsync(sx, x, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(sx + N, y, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(sx + 2 * N, z, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(launch_metrics(c->d, sx, sx + N, sx + 2 * N, c->f.met, c->stream));
-  c->launches += 2;
+  CK(launch_metrics(c->d, sx, sx + N, sx + 2 * N, c->f.met, c->f.area, c->stream));
+  c->launches += 3;
   RET(sync(c));
   c->have_metrics = true;
   c->sigma_valid = false;
@@ -677,6 +683,39 @@ int cbns_eval_rhs(cbns_ctx* c, int which, double* rhs) {
   const size_t n = (size_t)NEQ * (c->d.IM - 2) * (c->d.JM - 2) * (c->d.KM - 2);
   CK(cudaMemcpyAsync(rhs, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   return sync(c);
+}
+
+int cbns_autotune(cbns_ctx* c, int* chosen) {
+  RET(check_ready(c));
+  const bool fp32 = c->ph.precision != CBNS_PREC_FP64;
+  const int nv = stage_variants(fp32);
+  // time every variant on the current state (RHS-only mode: nothing is updated)
+  const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int v = 0; v < nv; ++v) {
+    c->stage_variant = v;
+    RET(stage_launch(c, a, 0));  // warm-up
+    CK(cudaEventRecord(e0, c->stream));
+    for (int r = 0; r < 3; ++r) RET(stage_launch(c, a, 0));
+    CK(cudaEventRecord(e1, c->stream));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->stage_variant = best;
+  drop_graph(c);
+  if (chosen) *chosen = best;
+  return CBNS_OK;
 }
 
 int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f, double* fx, double* fy, double* fz) {

@@ -45,6 +45,7 @@ struct Phys {
 // Device pointers of one context.  Q buffers hold 5 fields each.
 struct Fields {
   double* met[10];   // xi_x, xi_y, xi_z, eta_x, eta_y, eta_z, zeta_x, zeta_y, zeta_z, Jac
+  double* area[10];  // J*grad(xi) (3), J*grad(eta) (3), J*grad(zeta) (3), 1/J
   double* prim[7];   // rho, u, v, w, p, T, mu (viscous upkeep; on-demand otherwise)
   double* vflux[12]; // E0..E3, F0..F3, G0..G3 (viscous node fluxes, times J-scaled normals)
 };

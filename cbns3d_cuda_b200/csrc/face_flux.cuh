@@ -156,26 +156,61 @@ __device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const 
     K = gam1 * h * ic;  // (gamma-1)/(2 c^2)
   }
 
-  // characteristic projection of the 6 stencil states
-  R W[5][6];
-#pragma unroll
-  for (int p = 0; p < 6; ++p) {
-    const R f0 = ld(p, 0), f1 = ld(p, 1), f2 = ld(p, 2), f3 = ld(p, 3), f4 = ld(p, 4);
-    const R A = K * (R(0.5) * q2 * f0 - (uu * f1 + vv * f2 + ww * f3) + f4);
-    const R B = h * (qn * f0 - (ux * f1 + uy * f2 + uz * f3));
-    W[0][p] = A + B;
-    W[1][p] = f0 - R(2) * A;
-    W[2][p] = A - B;
-    W[3][p] = lx * f1 + ly * f2 + lz * f3 - ql * f0;
-    W[4][p] = mx * f1 + my * f2 + mz * f3 - qm * f0;
-  }
-
-  // WENO5 per field: low side from points 0..4, high side from 5..1
+  // characteristic projection of the 6 stencil states and WENO5 per field
+  // (low side from points 0..4, high side from 5..1).  FP64 projects all five
+  // fields in one pass; FP32 in two (acoustic + entropy fields, which share A
+  // and B, then the shear fields), which keeps at most 18 projected values live.
   R wl[5], wh[5];
+  if constexpr (sizeof(R) == 8) {
+    R W[5][6];
 #pragma unroll
-  for (int s = 0; s < 5; ++s) {
-    wl[s] = weno5<R>(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4]);
-    wh[s] = weno5<R>(W[s][5], W[s][4], W[s][3], W[s][2], W[s][1]);
+    for (int p = 0; p < 6; ++p) {
+      const R f0 = ld(p, 0), f1 = ld(p, 1), f2 = ld(p, 2), f3 = ld(p, 3), f4 = ld(p, 4);
+      const R A = K * (R(0.5) * q2 * f0 - (uu * f1 + vv * f2 + ww * f3) + f4);
+      const R B = h * (qn * f0 - (ux * f1 + uy * f2 + uz * f3));
+      W[0][p] = A + B;
+      W[1][p] = f0 - R(2) * A;
+      W[2][p] = A - B;
+      W[3][p] = lx * f1 + ly * f2 + lz * f3 - ql * f0;
+      W[4][p] = mx * f1 + my * f2 + mz * f3 - qm * f0;
+    }
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+      wl[s] = weno5<R>(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4]);
+      wh[s] = weno5<R>(W[s][5], W[s][4], W[s][3], W[s][2], W[s][1]);
+    }
+  } else {
+    {
+      R W[3][6];
+#pragma unroll
+      for (int p = 0; p < 6; ++p) {
+        const R f0 = ld(p, 0), f1 = ld(p, 1), f2 = ld(p, 2), f3 = ld(p, 3), f4 = ld(p, 4);
+        const R A = K * (R(0.5) * q2 * f0 - (uu * f1 + vv * f2 + ww * f3) + f4);
+        const R B = h * (qn * f0 - (ux * f1 + uy * f2 + uz * f3));
+        W[0][p] = A + B;
+        W[1][p] = f0 - R(2) * A;
+        W[2][p] = A - B;
+      }
+#pragma unroll
+      for (int s = 0; s < 3; ++s) {
+        wl[s] = weno5<R>(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4]);
+        wh[s] = weno5<R>(W[s][5], W[s][4], W[s][3], W[s][2], W[s][1]);
+      }
+    }
+    {
+      R W[2][6];
+#pragma unroll
+      for (int p = 0; p < 6; ++p) {
+        const R f0 = ld(p, 0), f1 = ld(p, 1), f2 = ld(p, 2), f3 = ld(p, 3);
+        W[0][p] = lx * f1 + ly * f2 + lz * f3 - ql * f0;
+        W[1][p] = mx * f1 + my * f2 + mz * f3 - qm * f0;
+      }
+#pragma unroll
+      for (int s = 0; s < 2; ++s) {
+        wl[3 + s] = weno5<R>(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4]);
+        wh[3 + s] = weno5<R>(W[s][5], W[s][4], W[s][3], W[s][2], W[s][1]);
+      }
+    }
   }
 
   // back to conservative variables, then primitives, on each side

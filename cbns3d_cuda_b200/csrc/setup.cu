@@ -76,6 +76,21 @@ __global__ void metrics_ghosts(Dims d, Met M) {
   for (int m = 0; m < 10; ++m) M.m[m][o] = M.m[m][c];
 }
 
+// Node area vectors J*grad(xi), J*grad(eta), J*grad(zeta) and 1/J over the
+// ghosted box: the face normal of the reference is the mean of the two nodes'
+// J*grad(xi) (src/rec_riemann_kernel.cu:44-49), so it is formed once here.
+__global__ void area_kernel(Dims d, Met M, Met A) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= (long)d.IG * d.JG * d.KG) return;
+  const int i = (int)(e % d.IG) - NG;
+  const long r = e / d.IG;
+  const long o = node_off(d, i, (int)(r % d.JG) - NG, (int)(r / d.JG) - NG);
+  const double J = M.m[9][o];
+#pragma unroll
+  for (int m = 0; m < 9; ++m) A.m[m][o] = M.m[m][o] * J;
+  A.m[9][o] = 1.0 / J;
+}
+
 struct Prims {
   double* p[6];
 };
@@ -183,11 +198,15 @@ inline unsigned nb(long n) { return (unsigned)((n + 255) / 256); }
 }  // namespace
 
 cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, const double* z, double* const met[10],
-                           cudaStream_t s) {
-  Met M;
-  for (int m = 0; m < 10; ++m) M.m[m] = met[m];
+                           double* const area[10], cudaStream_t s) {
+  Met M, A;
+  for (int m = 0; m < 10; ++m) {
+    M.m[m] = met[m];
+    A.m[m] = area[m];
+  }
   metrics_nodes<<<nb((long)d.IM * d.JM * d.KM), 256, 0, s>>>(d, x, y, z, M);
   metrics_ghosts<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M);
+  area_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M, A);
   return cudaGetLastError();
 }
 

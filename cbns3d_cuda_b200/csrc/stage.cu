@@ -16,13 +16,17 @@
 //   ring   : the conservative state of the column on the 6 planes k-2..k+3
 //            (stencil of the k-faces), loaded one new plane per step;
 //   plane  : plane k with a 3-node halo in i and j (stencils of i/j faces);
+//   areas  : the node area vectors J*grad(xi) on the i-face nodes and
+//            J*grad(eta) on the j-face nodes of plane k (face normals);
 //   round A: the 17 x 15 i-faces of plane k  (thread f -> face f, f < 255)
 //   round B: the 16 x 16 j-faces of plane k  (thread f -> face f)
 //   round C: the k+1/2 face of each column   (thread t -> column t, t < 240);
-//            the k-1/2 flux is carried in registers from the previous plane.
-// Every thread computes 3 faces per plane; face fluxes never leave the SM.
+//            the k-1/2 flux and the column's J*grad(zeta) are carried in
+//            registers from the previous plane.
+// Every thread computes 3 faces per plane; face fluxes never leave the SM and
+// no global load sits inside a face evaluation.
 // HBM traffic per node and stage: the stage input (40 B, halos from L2),
-// metrics (80 B), the RK base/partial states (0-80 B) and the output (40 B).
+// area vectors and 1/J (80 B), the RK base (0-40 B) and the output (40 B).
 #include "cbns_common.cuh"
 #include "face_flux.cuh"
 #include "stage.cuh"
@@ -38,23 +42,18 @@ constexpr int NC = TI * TJ;     // 240 columns
 constexpr int NT = 256;         // threads
 constexpr int NFI = (TI + 1) * TJ;  // 255 i-faces
 constexpr int NFJ = TI * (TJ + 1);  // 256 j-faces
+constexpr int NSX = (TI + 2) * TJ;  // i-face nodes (i0-1 .. i0+16)
+constexpr int NSY = TI * (TJ + 2);  // j-face nodes (j0-1 .. j0+15)
 
 template <typename S, typename R>
 struct Smem {
   S ring[6][NEQ][NC];
   S plane[NEQ][PH][PW];
+  S sx[3][TJ][TI + 2];  // J*grad(xi) at node (i0-1+c, j0+r)
+  S sy[3][TJ + 2][TI];  // J*grad(eta) at node (i0+c, j0-1+r)
   R fi[NEQ][TJ][TI + 1];
   R fj[NEQ][TJ + 1][TI];
 };
-
-template <typename R>
-__device__ __forceinline__ void face_normal(const StageArgs& a, long oa, long ob, int dir, R& nx, R& ny,
-                                            R& nz) {
-  const double Ja = __ldg(a.met[9] + oa), Jb = __ldg(a.met[9] + ob);
-  nx = (R)(0.5 * (__ldg(a.met[3 * dir + 0] + oa) * Ja + __ldg(a.met[3 * dir + 0] + ob) * Jb));
-  ny = (R)(0.5 * (__ldg(a.met[3 * dir + 1] + oa) * Ja + __ldg(a.met[3 * dir + 1] + ob) * Jb));
-  nz = (R)(0.5 * (__ldg(a.met[3 * dir + 2] + oa) * Ja + __ldg(a.met[3 * dir + 2] + ob) * Jb));
-}
 
 // 4th-order central derivative of a node field along a stride, at offset o.
 __device__ __forceinline__ double d4(const double* f, long o, long s) {
@@ -62,8 +61,11 @@ __device__ __forceinline__ double d4(const double* f, long o, long s) {
          (1.0 / 12.0) * __ldg(f + o + 2 * s);
 }
 
-template <typename R, bool VISC, int MODE>
-__global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
+// NB = CTAs per SM the register budget is cut for: FP64 always 2 (shared
+// memory allows no more); FP32 is built for 2 (128 registers, no spills) and 3
+// (80 registers, a few spills) and cbns_autotune keeps the faster.
+template <typename R, bool VISC, int MODE, int NB>
+__global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
   using S = R;  // shared-memory storage type
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<S, R>& sm = *reinterpret_cast<Smem<S, R>*>(smem_raw);
@@ -81,6 +83,8 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
   const int ke = min(kb + a.kchunk, d.KM - 1);
   if (kb >= ke) return;
   const long VOL = d.VOL;
+  // the ring holds exact stage-input values only when it is stored in FP64
+  constexpr bool kExactRing = sizeof(S) == 8;
 
   const FluxConsts<R> C{(R)a.gamma, (R)a.gam1, (R)a.gam1_inv};
 
@@ -100,30 +104,41 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
       }
     }
   };
+  auto load_zeta = [&](int kp, R z[3]) {
+    const long o = node_off(d, ci, cj, kp);
+#pragma unroll
+    for (int m = 0; m < 3; ++m) z[m] = (R)__ldg(a.area[6 + m] + o);
+  };
 
   // k-face between planes kk and kk+1 of this thread's column
-  auto k_face = [&](int kk, R out[5]) {
+  auto k_face = [&](int kk, const R za[3], const R zb[3], R out[5]) {
     const int s0 = (kk - 2 + 6) % 6;
     auto ld = [&](int p, int n) -> R {
       int s = s0 + p;
       s = s >= 6 ? s - 6 : s;
       return (R)sm.ring[s][n][t];
     };
-    R nx, ny, nz;
-    face_normal<R>(a, node_off(d, ci, cj, kk), node_off(d, ci, cj, kk + 1), 2, nx, ny, nz);
-    face_flux<R>(ld, nx, ny, nz, C, out);
+    face_flux<R>(ld, R(0.5) * (za[0] + zb[0]), R(0.5) * (za[1] + zb[1]), R(0.5) * (za[2] + zb[2]), C, out);
   };
 
   // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
   for (int kp = kb - 3; kp <= kb + 2; ++kp) load_ring(kp);
+  R za[3] = {0, 0, 0}, zb[3] = {0, 0, 0};
+  if (col_valid) {
+    load_zeta(kb - 1, za);
+    load_zeta(kb, zb);
+  }
   __syncthreads();
   R fkm[5] = {0, 0, 0, 0, 0};
-  if (col_valid) k_face(kb - 1, fkm);
+  if (col_valid) k_face(kb - 1, za, zb, fkm);
+#pragma unroll
+  for (int m = 0; m < 3; ++m) za[m] = zb[m];
 
   double smax = 0.0;  // running spectral-radius max (stage 3, inviscid)
   bool snan = false;
 
   for (int k = kb; k < ke; ++k) {
+    if (col_valid) load_zeta(k + 1, zb);  // consumed in round C
     __syncthreads();
     load_ring(k + 3);
     // plane k with halo: interior from the ring, halo from global memory
@@ -155,6 +170,27 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
           for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = (S)__ldg(a.src + n * VOL + o);
         }
       }
+      // area vectors of the face nodes of plane k
+      for (int e = t; e < NSX + NSY; e += NT) {
+        if (e < NSX) {
+          const int c = e % (TI + 2), r = e / (TI + 2);
+          const int gi = ti0 - 1 + c, gj = tj0 + r;
+          if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+            const long o = node_off(d, gi, gj, k);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) sm.sx[m][r][c] = (S)__ldg(a.area[m] + o);
+          }
+        } else {
+          const int e2 = e - NSX;
+          const int c = e2 % TI, r = e2 / TI;
+          const int gi = ti0 + c, gj = tj0 - 1 + r;
+          if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+            const long o = node_off(d, gi, gj, k);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) sm.sy[m][r][c] = (S)__ldg(a.area[3 + m] + o);
+          }
+        }
+      }
     }
     __syncthreads();
 
@@ -164,9 +200,10 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
       const int ga = ti0 + fx - 1, gj = tj0 + fy;
       if (ga <= d.IM - 2 && gj <= d.JM - 2) {
         auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
-        R nx, ny, nz, f[5];
-        face_normal<R>(a, node_off(d, ga, gj, k), node_off(d, ga + 1, gj, k), 0, nx, ny, nz);
-        face_flux<R>(ld, nx, ny, nz, C, f);
+        R f[5];
+        face_flux<R>(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
+                     R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
+                     R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), C, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
       }
@@ -177,16 +214,17 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
       const int gi = ti0 + fx, ga = tj0 + fy - 1;
       if (gi <= d.IM - 2 && ga <= d.JM - 2) {
         auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
-        R nx, ny, nz, f[5];
-        face_normal<R>(a, node_off(d, gi, ga, k), node_off(d, gi, ga + 1, k), 1, nx, ny, nz);
-        face_flux<R>(ld, nx, ny, nz, C, f);
+        R f[5];
+        face_flux<R>(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
+                     R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
+                     R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), C, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
       }
     }
     // round C: the k+1/2 face of this column
     R fkp[5];
-    if (col_valid) k_face(k, fkp);
+    if (col_valid) k_face(k, za, zb, fkp);
     __syncthreads();
 
     if (col_valid) {
@@ -207,23 +245,25 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
           df[n + 1] -= dv;
         }
       }
-      const double iJ = 1.0 / __ldg(a.met[9] + o);
+      const double iJ = __ldg(a.area[9] + o);
       if (MODE == 0) {
         const long r = 5L * ((ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * (k - 1)));
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) a.out[r + n] = df[n] * iJ;
       } else {
+        const int sk = k % 6;
         double q[NEQ];
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) {
           const double L = dt * (df[n] * iJ);
           const long e = n * VOL + o;
+          const double qin = kExactRing ? (double)sm.ring[sk][n][t] : 0.0;
           if (MODE == 1) {
-            q[n] = __ldg(a.q0 + e) - L;
+            q[n] = ((kExactRing && a.q0_is_src) ? qin : __ldg(a.q0 + e)) - L;
           } else if (MODE == 2) {
-            q[n] = 0.75 * __ldg(a.q0 + e) + 0.25 * (__ldg(a.qp + e) - L);
+            q[n] = 0.75 * __ldg(a.q0 + e) + 0.25 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L);
           } else {
-            q[n] = (a.q0[e] + 2.0 * (__ldg(a.qp + e) - L)) / 3.0;
+            q[n] = (a.q0[e] + 2.0 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L)) / 3.0;
           }
         }
 #pragma unroll
@@ -240,12 +280,24 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
             a.prim[4][o] = pp;
             a.prim[5][o] = a.gM2 * pp / r;
           } else {
+            // grad(xi), grad(eta), grad(zeta) = area vectors / J (FP64 in both precisions)
+            double g[9];
+            if (kExactRing) {
+#pragma unroll
+              for (int m = 0; m < 3; ++m) {
+                g[m] = (double)sm.sx[m][cy][cx + 1] * iJ;
+                g[3 + m] = (double)sm.sy[m][cy + 1][cx] * iJ;
+                g[6 + m] = (double)za[m] * iJ;
+              }
+            } else {
+#pragma unroll
+              for (int m = 0; m < 9; ++m) g[m] = __ldg(a.area[m] + o) * iJ;
+            }
             const double cs = sqrt(a.gamma * pp / r);
             double s = 0.0;
 #pragma unroll
             for (int dd = 0; dd < 3; ++dd) {
-              const double mx = __ldg(a.met[3 * dd] + o), my = __ldg(a.met[3 * dd + 1] + o),
-                           mz = __ldg(a.met[3 * dd + 2] + o);
+              const double mx = g[3 * dd], my = g[3 * dd + 1], mz = g[3 * dd + 2];
               s += fabs(uu * mx + vv * my + ww * mz) + cs * sqrt(mx * mx + my * my + mz * mz);
             }
             if (s != s) snan = true;
@@ -256,6 +308,8 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
     }
 #pragma unroll
     for (int n = 0; n < NEQ; ++n) fkm[n] = fkp[n];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) za[m] = zb[m];
   }
 
   if (MODE != 0 && !VISC && a.sigma) {
@@ -277,43 +331,42 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel(const StageArgs a) {
   }
 }
 
-template <typename R, bool VISC, int MODE>
+template <typename R, bool VISC, int MODE, int NB>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
   const size_t smem = sizeof(Smem<R, R>);
   dim3 grid(a.ntile_i * a.ntile_j, (a.d.KM - 2 + a.kchunk - 1) / a.kchunk);
-  stage_kernel<R, VISC, MODE><<<grid, NT, smem, s>>>(a);
+  stage_kernel<R, VISC, MODE, NB><<<grid, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <typename R, bool VISC, int MODE>
-void prepare_t() {
-  cudaFuncSetAttribute(stage_kernel<R, VISC, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(Smem<R, R>));
+template <typename R, int NB>
+void prepare_nb() {
+  const int smem = (int)sizeof(Smem<R, R>);
+  cudaFuncSetAttribute(stage_kernel<R, false, 0, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, false, 1, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, false, 2, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, false, 3, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 0, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 1, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 2, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 3, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
-template <typename R, bool VISC>
-void prepare_rv() {
-  prepare_t<R, VISC, 0>();
-  prepare_t<R, VISC, 1>();
-  prepare_t<R, VISC, 2>();
-  prepare_t<R, VISC, 3>();
-}
-
-template <typename R>
+template <typename R, int NB>
 cudaError_t launch_r(const StageArgs& a, int mode, bool visc, cudaStream_t s) {
   if (visc) {
     switch (mode) {
-      case 0: return launch_t<R, true, 0>(a, s);
-      case 1: return launch_t<R, true, 1>(a, s);
-      case 2: return launch_t<R, true, 2>(a, s);
-      default: return launch_t<R, true, 3>(a, s);
+      case 0: return launch_t<R, true, 0, NB>(a, s);
+      case 1: return launch_t<R, true, 1, NB>(a, s);
+      case 2: return launch_t<R, true, 2, NB>(a, s);
+      default: return launch_t<R, true, 3, NB>(a, s);
     }
   }
   switch (mode) {
-    case 0: return launch_t<R, false, 0>(a, s);
-    case 1: return launch_t<R, false, 1>(a, s);
-    case 2: return launch_t<R, false, 2>(a, s);
-    default: return launch_t<R, false, 3>(a, s);
+    case 0: return launch_t<R, false, 0, NB>(a, s);
+    case 1: return launch_t<R, false, 1, NB>(a, s);
+    case 2: return launch_t<R, false, 2, NB>(a, s);
+    default: return launch_t<R, false, 3, NB>(a, s);
   }
 }
 
@@ -324,10 +377,9 @@ cudaError_t launch_r(const StageArgs& a, int mode, bool visc, cudaStream_t s) {
 void stage_prepare() {
   static bool done = false;
   if (done) return;
-  prepare_rv<double, false>();
-  prepare_rv<double, true>();
-  prepare_rv<float, false>();
-  prepare_rv<float, true>();
+  prepare_nb<double, 2>();
+  prepare_nb<float, 2>();
+  prepare_nb<float, 3>();
   done = true;
 }
 
@@ -336,8 +388,11 @@ void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j) {
   *ntile_j = (d.JM - 2 + TJ - 1) / TJ;
 }
 
-cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, cudaStream_t s) {
-  return fp32 ? launch_r<float>(a, mode, visc, s) : launch_r<double>(a, mode, visc, s);
+int stage_variants(bool fp32) { return fp32 ? 2 : 1; }
+
+cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s) {
+  if (!fp32) return launch_r<double, 2>(a, mode, visc, s);
+  return variant == 1 ? launch_r<float, 3>(a, mode, visc, s) : launch_r<float, 2>(a, mode, visc, s);
 }
 
 }  // namespace cbns

@@ -13,16 +13,20 @@ struct StageArgs {
   const double* qp;    // the reference's Q_p at the node (stages 2, 3)
   double* out;         // stage output (5 fields), or the dense RHS array in mode 0
   const double* met[10];
+  const double* area[10];  // J*grad(xi|eta|zeta) per node, then 1/J
   const double* vflux[12];
   double* prim[6];     // viscous: rho,u,v,w,p,T of the new interior state
   StepState* st;       // dt, done flag, spectral-radius max
+  int q0_is_src, qp_is_src;  // RK operands that equal the stage input (read from the ring)
   int ntile_i, ntile_j, kchunk;
   int visdiv;          // CBNS_VISDIV_*
   int sigma;           // accumulate the interior spectral-radius max (inviscid stage 3)
 };
 
 // mode 0: dense RHS output; 1..3: RK stage.  fp32: split-precision flux arithmetic.
-cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, cudaStream_t s);
+// variant: a compiled occupancy variant, 0 .. stage_variants(fp32)-1.
+cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s);
+int stage_variants(bool fp32);
 void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j);
 
 }  // namespace cbns

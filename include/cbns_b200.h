@@ -159,6 +159,11 @@ int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f,
 int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM, const double* f,
                                double* fx, double* fy, double* fz);
 
+/* Pick, by timing on the current state, the fastest compiled variant of the
+ * stage kernel for this context's precision (the state is not modified);
+ * *chosen (may be null) receives the variant index.  Later steps use it. */
+int cbns_autotune(cbns_ctx* ctx, int* chosen);
+
 /* Per-kernel device timing with CUDA events on the launch stream.  Kernel ids:
  * 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous node
  * fluxes, 3 dt/step bookkeeping.  total_ms is the summed event time. */

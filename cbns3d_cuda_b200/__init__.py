@@ -165,6 +165,34 @@ class Block:
                 self.calc_viscous_terms()
         return t_cur
 
+    # hybrid flux (precision PREC_HYBRID) -------------------------------------
+    def sensor_load(self, params: np.ndarray, tau: float):
+        """Install the sensor network (CBNS_SENSOR_NPARAM floats) and its threshold."""
+        p = np.ascontiguousarray(params, dtype=np.float32).reshape(-1)
+        if p.size != 1601:
+            raise ValueError(f"sensor parameters: expected 1601 values, got {p.size}")
+        _abi.check(self.lib.cbns_sensor_load(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), float(tau)),
+                   "cbns_sensor_load")
+
+    def sensor_audit(self, stride: int = 97, bound: float = 1.0e-2):
+        _abi.check(self.lib.cbns_sensor_audit(self.h, int(stride), float(bound)), "cbns_sensor_audit")
+
+    def sensor_stats(self) -> dict:
+        s = _abi.SensorStats()
+        _abi.check(self.lib.cbns_sensor_stats_get(self.h, C.byref(s)), "cbns_sensor_stats_get")
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def sensor_mask(self) -> tuple[np.ndarray, bool]:
+        """(decisions of the latest sensor evaluation, 1 = WENO5; audit forced WENO5)."""
+        n = self.sensor_stats()["faces_per_step"]
+        m = np.empty(n, dtype=np.uint8)
+        f = C.c_int()
+        _abi.check(self.lib.cbns_sensor_mask_get(self.h, m.ctypes.data, n, C.byref(f)), "cbns_sensor_mask_get")
+        return m, bool(f.value)
+
+    def sensor_stats_reset(self):
+        _abi.check(self.lib.cbns_sensor_stats_reset(self.h), "cbns_sensor_stats_reset")
+
     def autotune(self) -> int:
         v = C.c_int()
         _abi.check(self.lib.cbns_autotune(self.h, C.byref(v)), "cbns_autotune")

@@ -46,6 +46,16 @@ class Params(C.Structure):
     ]
 
 
+class SensorStats(C.Structure):
+    """cbns_sensor_stats: counters of the hybrid flux's sensor and audit."""
+
+    _fields_ = [
+        ("weno_faces", C.c_ulonglong), ("audit_faces", C.c_ulonglong),
+        ("audit_fail_steps", C.c_uint), ("audit_max", C.c_float),
+        ("sensor_fail", C.c_int), ("faces_per_step", C.c_ulonglong),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point
 _D = C.POINTER(C.c_double)
 _V = C.c_void_p
@@ -75,6 +85,16 @@ SIGNATURES = [
     ("cbns_eval_rhs", C.c_int, [_V, C.c_int, _D]),
     ("cbns_calc_gradient", C.c_int, [C.c_uint, C.c_uint, C.c_uint, _D, _D, _D, _D]),
     ("cbns_autotune", C.c_int, [_V, C.POINTER(C.c_int)]),
+    ("cbns_sensor_sample", C.c_int,
+     [_V, C.c_int, C.c_uint, C.c_uint, _V, _V, _V, _V, C.c_uint, C.POINTER(C.c_uint)]),
+    ("cbns_mlp_grad", C.c_int, [_V, _V, _V, C.c_uint, C.c_float, _V, _V, _V]),
+    ("cbns_mlp_adam", C.c_int, [_V, _V, _V, _V, C.c_uint, C.c_float, _V]),
+    ("cbns_mlp_predict", C.c_int, [_V, _V, C.c_uint, _V, C.c_int, _V, _V]),
+    ("cbns_sensor_load", C.c_int, [_V, C.POINTER(C.c_float), C.c_float]),
+    ("cbns_sensor_audit", C.c_int, [_V, C.c_uint, C.c_float]),
+    ("cbns_sensor_stats_get", C.c_int, [_V, C.POINTER(SensorStats)]),
+    ("cbns_sensor_stats_reset", C.c_int, [_V]),
+    ("cbns_sensor_mask_get", C.c_int, [_V, _V, C.c_ulonglong, C.POINTER(C.c_int)]),
     ("cbns_prof_enable", C.c_int, [_V, C.c_int]),
     ("cbns_prof_read", C.c_int, [_V, C.c_int, _D, C.POINTER(C.c_uint)]),
     ("cbns_prof_reset", C.c_int, [_V]),

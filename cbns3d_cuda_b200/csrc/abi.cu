@@ -25,14 +25,19 @@
 #include "stage.cuh"
 #include "step.cuh"
 #include "visc.cuh"
+#include "sensor_kernels.cuh"
 
 using namespace cbns;
+
+namespace cbns {
+cudaError_t launch_mlp_predict_tc(const float* P, const float* X, unsigned n, float* out, int* fail, cudaStream_t s);
+}
 
 namespace cbns {
 void stage_prepare();
 }
 
-enum { PK_STAGE = 0, PK_BC = 1, PK_VISC = 2, PK_STEP = 3, PK_N = 4 };
+enum { PK_STAGE = 0, PK_BC = 1, PK_VISC = 2, PK_STEP = 3, PK_SENSOR = 4, PK_N = 5 };
 
 struct cbns_ctx {
   cbns_params prm;
@@ -45,6 +50,7 @@ struct cbns_ctx {
   double* staging = nullptr;
   size_t staging_elems = 0;
   StepState* st = nullptr;
+  unsigned* counter = nullptr;  // device counter for face sampling
   bool have_metrics = false, sigma_valid = false;
   int prims_of = -1;     // physical buffer whose interior primitives the arrays hold
   int pending_src = -1;  // buffer given to calc_numerical_flux, consumed by update_rk3
@@ -53,6 +59,14 @@ struct cbns_ctx {
   int g_q = -1, g_p = -1, g_s = -1;
   int ntile_i = 1, ntile_j = 1, kchunk = 1;
   int stage_variant = 0;  // compiled occupancy variant of the stage kernel (cbns_autotune)
+  // hybrid flux: the learned sensor's parameters and per-face decisions
+  float* sensor_params = nullptr;  // device, CBNS_SENSOR_NPARAM floats
+  unsigned char* mask = nullptr;   // device, one byte per face
+  long nfaces = 0;
+  float sensor_tau = 0.5f;
+  unsigned audit_stride = 97;
+  float audit_bound = 1.0e-2f;
+  bool sensor_loaded = false;
   bool prof = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[PK_N];
   std::vector<cudaEvent_t> ev_pool;
@@ -186,6 +200,7 @@ StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const dou
   a.kchunk = c->kchunk;
   a.visdiv = c->ph.visdiv;
   a.sigma = sigma;
+  a.mask = c->ph.precision == CBNS_PREC_HYBRID ? c->mask : nullptr;
   return a;
 }
 
@@ -256,6 +271,42 @@ void drop_graph(cbns_ctx* c) {
   c->graph = nullptr;
 }
 
+// The hybrid flux's decisions for the state q: the sensor network on every
+// face (tensor cores), then the audit of a rotating sample of its linear-flux
+// faces against WENO5 (which forces WENO5 for the step on a violation).
+int sensor_launch(cbns_ctx* c, const double* q, bool check_done) {
+  Prof p(c, PK_SENSOR);
+  MaskArgs m;
+  m.d = c->d;
+  m.gamma = (float)c->ph.gamma;
+  m.gam1 = (float)c->ph.gam1;
+  m.q = q;
+  for (int k = 0; k < 10; ++k) m.area[k] = c->f.area[k];
+  m.params = c->sensor_params;
+  m.tau = c->sensor_tau;
+  m.mask = c->mask;
+  m.st = c->st;
+  m.check_done = check_done;
+  CK(launch_sensor_mask(m, c->stream));
+  AuditArgs a;
+  a.d = c->d;
+  a.gamma = (float)c->ph.gamma;
+  a.gam1 = (float)c->ph.gam1;
+  a.gam1_inv = (float)c->ph.gam1_inv;
+  a.q = q;
+  for (int k = 0; k < 10; ++k) a.area[k] = c->f.area[k];
+  a.mask = c->mask;
+  a.stride = c->audit_stride;
+  a.bound = c->audit_bound;
+  a.st = c->st;
+  a.check_done = check_done;
+  CK(launch_sensor_audit(a, c->stream));
+  c->launches += 2;
+  return CBNS_OK;
+}
+
+bool hybrid(const cbns_ctx* c) { return c->ph.precision == CBNS_PREC_HYBRID; }
+
 // One SSP-RK3 step on the fixed buffer roles P0 = Q, P1 = spare, P2 = Q_p.
 int enqueue_step(cbns_ctx* c) {
   const bool visc = c->ph.viscous != 0;
@@ -267,6 +318,7 @@ int enqueue_step(cbns_ctx* c) {
     CK(launch_step_prologue(c->st, c->ph.CFL, c->stream));
     c->launches += 1;
   }
+  if (hybrid(c)) RET(sensor_launch(c, P0, true));
   struct S {
     const double *src, *q0, *qp;
     double* out;
@@ -284,6 +336,10 @@ int check_ready(cbns_ctx* c) {
   if (!c) return CBNS_ERR_ARG;
   if (!c->have_metrics) {
     g_last = "metrics have not been computed (cbns_calc_metrics)";
+    return CBNS_ERR_STATE;
+  }
+  if (hybrid(c) && !c->sensor_loaded) {
+    g_last = "the hybrid flux needs the sensor network (cbns_sensor_load)";
     return CBNS_ERR_STATE;
   }
   return CBNS_OK;
@@ -316,7 +372,6 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   if (p->vis_divergence != CBNS_VISDIV_REFERENCE && p->vis_divergence != CBNS_VISDIV_CENTERED) return CBNS_ERR_ARG;
   for (int r : p->reserved)
     if (r != 0) return CBNS_ERR_ARG;
-  if (p->precision == CBNS_PREC_HYBRID) return CBNS_ERR_UNSUPPORTED;
   const double ng = ((double)p->IM + 4) * ((double)p->JM + 4) * ((double)p->KM + 4);
   if (ng * 5 > 2.0e9) return CBNS_ERR_TOO_LARGE;
 
@@ -364,6 +419,17 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   const long NGt = (long)d.IG * d.JG * d.KG;
   c->staging_elems = (size_t)std::max(5 * NGt, 10L * d.IM * d.JM * d.KM);
   if (rc == CBNS_OK) rc = dalloc(c, &c->staging, c->staging_elems);
+  c->nfaces = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2) + (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2) +
+              (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 1);
+  if (rc == CBNS_OK && p->precision == CBNS_PREC_HYBRID) {
+    double* tmp = nullptr;
+    rc = dalloc(c, &tmp, (size_t)(c->nfaces + 7) / 8);
+    c->mask = reinterpret_cast<unsigned char*>(tmp);
+    if (rc == CBNS_OK) {
+      rc = dalloc(c, &tmp, (CBNS_SENSOR_NPARAM + 1) / 2);
+      c->sensor_params = reinterpret_cast<float*>(tmp);
+    }
+  }
   if (rc == CBNS_OK) {
     void* s = nullptr;
     if (cudaMalloc(&s, sizeof(StepState)) != cudaSuccess) rc = CBNS_ERR_NOMEM;
@@ -371,6 +437,14 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
       c->allocs.push_back(s);
       c->st = static_cast<StepState*>(s);
       cudaMemset(s, 0, sizeof(StepState));
+    }
+  }
+  if (rc == CBNS_OK) {
+    void* s = nullptr;
+    if (cudaMalloc(&s, 256) != cudaSuccess) rc = CBNS_ERR_NOMEM;
+    else {
+      c->allocs.push_back(s);
+      c->counter = static_cast<unsigned*>(s);
     }
   }
   if (rc == CBNS_OK && cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) rc = CBNS_ERR_CUDA;
@@ -569,6 +643,10 @@ int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
     CK(launch_set_dt(c->st, dt, c->stream));
     c->launches += 1;
   }
+  if (hybrid(c) && stage == 1) {
+    CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
+    RET(sensor_launch(c, c->qb[src], false));
+  }
   const StageArgs a = stage_args(c, c->qb[src], c->qb[c->lq], c->qb[c->lp], c->qb[out], false);
   RET(stage_launch(c, a, (int)stage));
   if (swap) {
@@ -678,10 +756,129 @@ int cbns_run_async(cbns_ctx* c, unsigned nsteps, double t_end) { return run_impl
 int cbns_eval_rhs(cbns_ctx* c, int which, double* rhs) {
   RET(check_ready(c));
   if (!rhs || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
+  if (hybrid(c)) {
+    CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
+    RET(sensor_launch(c, buf(c, which), false));
+  }
   const StageArgs a = stage_args(c, buf(c, which), nullptr, nullptr, c->staging, false);
   RET(stage_launch(c, a, 0));
   const size_t n = (size_t)NEQ * (c->d.IM - 2) * (c->d.JM - 2) * (c->d.KM - 2);
   CK(cudaMemcpyAsync(rhs, c->staging, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int cbns_sensor_sample(cbns_ctx* c, int which, unsigned stride, unsigned offset, float* feat, unsigned char* label,
+                       float* dev, unsigned* index, unsigned capacity, unsigned* count) {
+  RET(check_ready(c));
+  if ((which != CBNS_Q && which != CBNS_QP) || stride == 0 || offset >= stride || !feat || !label || !count)
+    return CBNS_ERR_ARG;
+  SampleArgs a;
+  a.d = c->d;
+  a.gamma = (float)c->ph.gamma;
+  a.gam1 = (float)c->ph.gam1;
+  a.q = buf(c, which);
+  for (int m = 0; m < 10; ++m) a.area[m] = c->f.area[m];
+  a.stride = stride;
+  a.offset = offset;
+  a.feat = feat;
+  a.label = label;
+  a.dev = dev;
+  a.index = index;
+  a.capacity = capacity;
+  a.count = c->counter;
+  CK(cudaMemsetAsync(c->counter, 0, sizeof(unsigned), c->stream));
+  CK(launch_sample_faces(a, c->stream));
+  c->launches += 1;
+  CK(cudaMemcpyAsync(count, c->counter, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  return sync(c);
+}
+
+int cbns_mlp_grad(const float* P, const float* X, const unsigned char* Y, unsigned n, float pos_w, float* G,
+                  float* loss, void* stream) {
+  if (!P || !G || !loss || (n && (!X || !Y))) return CBNS_ERR_ARG;
+  CK(launch_mlp_grad(P, X, Y, n, pos_w, G, loss, static_cast<cudaStream_t>(stream)));
+  return CBNS_OK;
+}
+
+int cbns_mlp_adam(float* P, const float* G, float* M, float* V, unsigned step, float lr, void* stream) {
+  if (!P || !G || !M || !V || step == 0) return CBNS_ERR_ARG;
+  CK(launch_adam(P, G, M, V, step, lr, static_cast<cudaStream_t>(stream)));
+  return CBNS_OK;
+}
+
+int cbns_mlp_predict(const float* P, const float* X, unsigned n, float* out, int use_tc, int* status, void* stream) {
+  if (!P || !out || (n && !X)) return CBNS_ERR_ARG;
+  if (use_tc) {
+    if (!status) return CBNS_ERR_ARG;
+    CK(launch_mlp_predict_tc(P, X, n, out, status, static_cast<cudaStream_t>(stream)));
+  } else {
+    CK(launch_mlp_predict(P, X, n, out, static_cast<cudaStream_t>(stream)));
+  }
+  return CBNS_OK;
+}
+
+int cbns_sensor_load(cbns_ctx* c, const float* params, float tau) {
+  if (!c || !params) return CBNS_ERR_ARG;
+  if (!hybrid(c)) {
+    g_last = "cbns_sensor_load needs a context of precision CBNS_PREC_HYBRID";
+    return CBNS_ERR_STATE;
+  }
+  if (!(tau > 0.f && tau < 1.f)) return CBNS_ERR_ARG;
+  for (int k = 0; k < CBNS_SENSOR_NPARAM; ++k)
+    if (!std::isfinite(params[k])) return CBNS_ERR_ARG;
+  CK(cudaMemcpyAsync(c->sensor_params, params, CBNS_SENSOR_NPARAM * sizeof(float), cudaMemcpyHostToDevice,
+                     c->stream));
+  c->sensor_tau = tau;
+  c->sensor_loaded = true;
+  drop_graph(c);
+  return sync(c);
+}
+
+int cbns_sensor_audit(cbns_ctx* c, unsigned stride, float bound) {
+  if (!c || stride == 0 || !(bound > 0.f)) return CBNS_ERR_ARG;
+  c->audit_stride = stride;
+  c->audit_bound = bound;
+  drop_graph(c);
+  return CBNS_OK;
+}
+
+int cbns_sensor_stats_get(cbns_ctx* c, cbns_sensor_stats* out) {
+  if (!c || !out) return CBNS_ERR_ARG;
+  StepState h;
+  CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  RET(sync(c));
+  out->weno_faces = h.weno_faces;
+  out->audit_faces = h.audit_faces;
+  out->audit_fail_steps = h.audit_fail_steps;
+  out->audit_max = h.audit_max;
+  out->sensor_fail = h.sensor_fail;
+  out->faces_per_step = (unsigned long long)c->nfaces;
+  return CBNS_OK;
+}
+
+int cbns_sensor_mask_get(cbns_ctx* c, unsigned char* mask, unsigned long long n, int* forced) {
+  if (!c || !mask) return CBNS_ERR_ARG;
+  if (!hybrid(c)) return CBNS_ERR_STATE;
+  if (n < (unsigned long long)c->nfaces) return CBNS_ERR_ARG;
+  CK(cudaMemcpyAsync(mask, c->mask, (size_t)c->nfaces, cudaMemcpyDeviceToHost, c->stream));
+  int f = 0;
+  CK(cudaMemcpyAsync(&f, &c->st->force_weno, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  RET(sync(c));
+  if (forced) *forced = f;
+  return CBNS_OK;
+}
+
+int cbns_sensor_stats_reset(cbns_ctx* c) {
+  if (!c) return CBNS_ERR_ARG;
+  StepState h;
+  CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  RET(sync(c));
+  h.weno_faces = 0;
+  h.audit_faces = 0;
+  h.audit_fail_steps = 0;
+  h.audit_max = 0.f;
+  h.sensor_fail = 0;
+  CK(cudaMemcpyAsync(c->st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   return sync(c);
 }
 

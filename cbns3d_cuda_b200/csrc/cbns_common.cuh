@@ -59,7 +59,12 @@ struct StepState {
   unsigned steps;                 // steps taken
   int done;                       // time loop finished: kernels return immediately
   int nan_dt;                     // CFL/max(sigma) was NaN
-  int pad;
+  int force_weno;                 // hybrid: the audit rejected this step's sensor decisions
+  unsigned audit_fail_steps;      // hybrid: steps whose sensor decisions the audit rejected
+  unsigned long long weno_faces;  // hybrid: faces sent to WENO5 (summed over steps)
+  unsigned long long audit_faces; // hybrid: faces the audit re-evaluated
+  float audit_max;                // hybrid: largest relative flux difference the audit saw
+  int sensor_fail;                // hybrid: a tensor-core wait timed out
 };
 
 // Positive doubles order like their bit patterns; a NaN (either sign) compares

@@ -78,6 +78,30 @@ __device__ __forceinline__ R weno5(R a, R b, R c, R d, R e) {
   }
 }
 
+// Local Lax-Friedrichs flux from the two reconstructed states (the reference's
+// lf_flux with R = the high side H, L = the low side): the component-wise
+// Cartesian wave-speed bound, flux = (F_L + F_H - ws (U_H - U_L)) / 2.
+template <typename R>
+__device__ __forceinline__ void lf_flux_prims(R Lr, R Lu, R Lv, R Lw, R Lp, R Hr, R Hu, R Hv, R Hw, R Hp, R nx,
+                                              R ny, R nz, const FluxConsts<R>& C, R out[5]) {
+  const R gamma = C.gamma, gam1_inv = C.gam1_inv;
+  const R kH = Hu * Hu + Hv * Hv + Hw * Hw, kL = Lu * Lu + Lv * Lv + Lw * Lw;
+  const R cH = sqrt(gamma * Hp * rcp_(Hr)), cL = sqrt(gamma * Lp * rcp_(Lr));
+  const R HH = cH * cH * gam1_inv + R(0.5) * kH, HL = cL * cL * gam1_inv + R(0.5) * kL;
+  const R EH = Hp * gam1_inv + R(0.5) * Hr * kH, EL = Lp * gam1_inv + R(0.5) * Lr * kL;
+  const R qH = Hu * nx + Hv * ny + Hw * nz, qL = Lu * nx + Lv * ny + Lw * nz;
+  const R sx = fmax(fabs(Hu) + cH, fabs(Lu) + cL);
+  const R sy = fmax(fabs(Hv) + cH, fabs(Lv) + cL);
+  const R sz = fmax(fabs(Hw) + cH, fabs(Lw) + cL);
+  const R ws = fabs(sx * nx + sy * ny + sz * nz);
+  const R mL = Lr * qL, mH = Hr * qH;
+  out[0] = R(0.5) * (mL + mH - ws * (Hr - Lr));
+  out[1] = R(0.5) * (mL * Lu + Lp * nx + mH * Hu + Hp * nx - ws * (Hr * Hu - Lr * Lu));
+  out[2] = R(0.5) * (mL * Lv + Lp * ny + mH * Hv + Hp * ny - ws * (Hr * Hv - Lr * Lv));
+  out[3] = R(0.5) * (mL * Lw + Lp * nz + mH * Hw + Hp * nz - ws * (Hr * Hw - Lr * Lw));
+  out[4] = R(0.5) * (mL * HL + mH * HH - ws * (EH - EL));
+}
+
 // Flux through the face between stencil points 2 (node a) and 3 (node b).
 // ld(p, n) returns conservative variable n at stencil point p (p = 0..5 are the
 // nodes a-2 .. b+2 along the face normal).  (nx,ny,nz) is the face area vector
@@ -246,24 +270,34 @@ __device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const 
     }
   }
 
-  // local Lax-Friedrichs flux (the reference's lf_flux with R = high side, L = low side)
-  {
-    const R kH = Hu * Hu + Hv * Hv + Hw * Hw, kL = Lu * Lu + Lv * Lv + Lw * Lw;
-    const R cH = sqrt(gamma * Hp * rcp_(Hr)), cL = sqrt(gamma * Lp * rcp_(Lr));
-    const R HH = cH * cH * gam1_inv + R(0.5) * kH, HL = cL * cL * gam1_inv + R(0.5) * kL;
-    const R EH = Hp * gam1_inv + R(0.5) * Hr * kH, EL = Lp * gam1_inv + R(0.5) * Lr * kL;
-    const R qH = Hu * nx + Hv * ny + Hw * nz, qL = Lu * nx + Lv * ny + Lw * nz;
-    const R sx = fmax(fabs(Hu) + cH, fabs(Lu) + cL);
-    const R sy = fmax(fabs(Hv) + cH, fabs(Lv) + cL);
-    const R sz = fmax(fabs(Hw) + cH, fabs(Lw) + cL);
-    const R ws = fabs(sx * nx + sy * ny + sz * nz);
-    const R mL = Lr * qL, mH = Hr * qH;
-    out[0] = R(0.5) * (mL + mH - ws * (Hr - Lr));
-    out[1] = R(0.5) * (mL * Lu + Lp * nx + mH * Hu + Hp * nx - ws * (Hr * Hu - Lr * Lu));
-    out[2] = R(0.5) * (mL * Lv + Lp * ny + mH * Hv + Hp * ny - ws * (Hr * Hv - Lr * Lv));
-    out[3] = R(0.5) * (mL * Lw + Lp * nz + mH * Hw + Hp * nz - ws * (Hr * Hw - Lr * Lw));
-    out[4] = R(0.5) * (mL * HL + mH * HH - ws * (EH - EL));
+  lf_flux_prims<R>(Lr, Lu, Lv, Lw, Lp, Hr, Hu, Hv, Hw, Hp, nx, ny, nz, C, out);
+}
+
+// Flux through the same face with the linear upwind-biased 5th-order
+// reconstruction of each conservative variable (the WENO5 candidate values
+// combined with the ideal weights 0.1/0.6/0.3: (2a - 13b + 47c + 27d - 3e)/60).
+// With ideal weights the characteristic projection cancels (it is linear and
+// the same for every stencil point), so this equals characteristic WENO5
+// wherever the nonlinear weights sit at their linear values -- the faces the
+// learned sensor sends here.  Same Lax-Friedrichs flux as face_flux.
+template <typename R, typename LD>
+__device__ __forceinline__ void face_flux_linear(const LD& ld, R nx, R ny, R nz, const FluxConsts<R>& C,
+                                                 R out[5]) {
+  const R k60 = R(1.0 / 60.0);
+  R ql[5], qh[5];
+#pragma unroll
+  for (int n = 0; n < 5; ++n) {
+    const R f0 = ld(0, n), f1 = ld(1, n), f2 = ld(2, n), f3 = ld(3, n), f4 = ld(4, n), f5 = ld(5, n);
+    ql[n] = (R(2) * f0 - R(13) * f1 + R(47) * f2 + R(27) * f3 - R(3) * f4) * k60;
+    qh[n] = (R(2) * f5 - R(13) * f4 + R(47) * f3 + R(27) * f2 - R(3) * f1) * k60;
   }
+  const R gam1 = C.gam1;
+  const R iL = rcp_(ql[0]), iH = rcp_(qh[0]);
+  const R Lu = ql[1] * iL, Lv = ql[2] * iL, Lw = ql[3] * iL;
+  const R Hu = qh[1] * iH, Hv = qh[2] * iH, Hw = qh[3] * iH;
+  const R Lp = gam1 * (ql[4] - R(0.5) * ql[0] * (Lu * Lu + Lv * Lv + Lw * Lw));
+  const R Hp = gam1 * (qh[4] - R(0.5) * qh[0] * (Hu * Hu + Hv * Hv + Hw * Hw));
+  lf_flux_prims<R>(ql[0], Lu, Lv, Lw, Lp, qh[0], Hu, Hv, Hw, Hp, nx, ny, nz, C, out);
 }
 
 }  // namespace cbns

@@ -1,0 +1,319 @@
+// sensor.cu - training side of the learned shock sensor: face sampling with
+// features and WENO-weight labels from a solver state, the network's loss and
+// gradient over a batch (forward and backward by hand), the Adam update, and
+// an FP32 forward pass.  See sensor.cuh for the features, label and layout.
+#include "face_flux.cuh"
+#include "sensor.cuh"
+#include "sensor_kernels.cuh"
+
+namespace cbns {
+
+namespace {
+
+// ---------------------------------------------------------------- sampling
+__global__ void sample_faces_kernel(const SampleArgs a) {
+  const Dims& d = a.d;
+  const long ni = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
+  const long nj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
+  const long nk = (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 1);
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= ni + nj + nk || (e % a.stride) != a.offset) return;
+  int dir, i, j, k;
+  if (e < ni) {  // face between (i, j+1, k+1) and (i+1, j+1, k+1)
+    dir = 0;
+    i = (int)(e % (d.IM - 1));
+    j = 1 + (int)((e / (d.IM - 1)) % (d.JM - 2));
+    k = 1 + (int)(e / ((long)(d.IM - 1) * (d.JM - 2)));
+  } else if (e < ni + nj) {
+    const long r = e - ni;
+    dir = 1;
+    i = 1 + (int)(r % (d.IM - 2));
+    j = (int)((r / (d.IM - 2)) % (d.JM - 1));
+    k = 1 + (int)(r / ((long)(d.IM - 2) * (d.JM - 1)));
+  } else {
+    const long r = e - ni - nj;
+    dir = 2;
+    i = 1 + (int)(r % (d.IM - 2));
+    j = 1 + (int)((r / (d.IM - 2)) % (d.JM - 2));
+    k = (int)(r / ((long)(d.IM - 2) * (d.JM - 2)));
+  }
+  const long sd = dir == 0 ? 1 : (dir == 1 ? d.PX : d.PL);
+  const long oa = node_off(d, i, j, k), ob = oa + sd;
+  const double* q = a.q;
+  const long V = d.VOL;
+  auto ld = [&](int p, int n) -> float { return (float)q[n * V + oa + (p - 2) * sd]; };
+  const float nx = (float)(0.5 * (a.area[3 * dir][oa] + a.area[3 * dir][ob]));
+  const float ny = (float)(0.5 * (a.area[3 * dir + 1][oa] + a.area[3 * dir + 1][ob]));
+  const float nz = (float)(0.5 * (a.area[3 * dir + 2][oa] + a.area[3 * dir + 2][ob]));
+  const float in = rsqrtf(nx * nx + ny * ny + nz * nz);
+  float f[SN_IN];
+  face_features(ld, nx * in, ny * in, nz * in, a.gamma, a.gam1, f);
+  const float dev = face_weno_deviation(ld, nx, ny, nz, a.gamma, a.gam1);
+  const unsigned slot = atomicAdd(a.count, 1u);
+  if (slot >= a.capacity) return;
+#pragma unroll
+  for (int m = 0; m < SN_IN; ++m) a.feat[(long)slot * SN_IN + m] = f[m];
+  a.label[slot] = dev > SN_DEV_THRESHOLD ? 1 : 0;
+  if (a.dev) a.dev[slot] = dev;
+  if (a.index) a.index[slot] = (unsigned)e;
+}
+
+// ---------------------------------------------------------------- loss and gradient
+constexpr int TILE = 128, GT = 256, HP = SN_H + 1;
+
+struct GradSmem {
+  float x[TILE][16];
+  float h1[TILE][HP], h2[TILE][HP], g2[TILE][HP], g1[TILE][HP];
+  float dz[TILE];
+  float W2[SN_H][SN_H];
+  float w3[SN_H];
+};
+
+// Binary cross-entropy with positive-class weight, averaged over n samples:
+// loss = -(1/n) sum w_i [y_i log p_i + (1 - y_i) log(1 - p_i)], p = sigmoid(z).
+// Each CTA takes tiles of 128 samples: forward into shared memory, backward by
+// the chain rule, per-thread partial sums of the weight gradients in registers,
+// one atomic add per parameter per CTA at the end.
+__global__ void __launch_bounds__(GT) mlp_grad_kernel(const float* __restrict__ P, const float* __restrict__ X,
+                                                      const unsigned char* __restrict__ Y, unsigned n, float pos_w,
+                                                      float inv_n, float* G, float* loss) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  GradSmem& s = *reinterpret_cast<GradSmem*>(raw);
+  const int t = threadIdx.x;
+  const int c = t & 31, rb = t >> 5;  // column and first row of this thread's outputs
+  for (int e = t; e < SN_H * SN_H; e += GT) s.W2[e / SN_H][e % SN_H] = P[SP_W2 + e];
+  if (t < SN_H) s.w3[t] = P[SP_W3 + t];
+  float w1[SN_IN], w2[SN_H];
+#pragma unroll
+  for (int k = 0; k < SN_IN; ++k) w1[k] = P[SP_W1 + c * SN_IN + k];
+#pragma unroll
+  for (int k = 0; k < SN_H; ++k) w2[k] = P[SP_W2 + c * SN_H + k];
+  const float b1 = P[SP_B1 + c], b2 = P[SP_B2 + c], b3 = P[SP_B3];
+  // owned gradient entries
+  float gW2[4] = {0, 0, 0, 0}, gW1[2] = {0, 0}, gvec = 0.f, lsum = 0.f;
+  __syncthreads();
+  const unsigned ntiles = (n + TILE - 1) / TILE;
+  for (unsigned tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const unsigned base = tile * TILE;
+    for (int e = t; e < TILE * 16; e += GT) {
+      const int r = e >> 4, k = e & 15;
+      const unsigned sidx = base + r;
+      s.x[r][k] = (k < SN_IN && sidx < n) ? X[(size_t)sidx * SN_IN + k] : 0.f;
+    }
+    __syncthreads();
+    for (int r = rb; r < TILE; r += 8) {
+      float h = b1;
+#pragma unroll
+      for (int k = 0; k < SN_IN; ++k) h += s.x[r][k] * w1[k];
+      s.h1[r][c] = fmaxf(h, 0.f);
+    }
+    __syncthreads();
+    for (int r = rb; r < TILE; r += 8) {
+      float h = b2;
+#pragma unroll
+      for (int k = 0; k < SN_H; ++k) h += s.h1[r][k] * w2[k];
+      s.h2[r][c] = fmaxf(h, 0.f);
+    }
+    __syncthreads();
+    if (t < TILE) {
+      const unsigned sidx = base + t;
+      float dz = 0.f;
+      if (sidx < n) {
+        float z = b3;
+#pragma unroll
+        for (int k = 0; k < SN_H; ++k) z += s.h2[t][k] * s.w3[k];
+        const float y = Y[sidx] ? 1.f : 0.f;
+        const float w = Y[sidx] ? pos_w : 1.f;
+        const float p = 1.f / (1.f + __expf(-z));
+        // log(sigmoid(z)) and log(1 - sigmoid(z)) in a form that does not overflow
+        const float lp = -log1pf(__expf(-fabsf(z))) + fminf(z, 0.f);
+        const float lq = lp - z;
+        lsum += -w * (y * lp + (1.f - y) * lq) * inv_n;
+        dz = w * (p - y) * inv_n;
+      }
+      s.dz[t] = dz;
+    }
+    __syncthreads();
+    for (int r = rb; r < TILE; r += 8) s.g2[r][c] = s.h2[r][c] > 0.f ? s.dz[r] * s.w3[c] : 0.f;
+    __syncthreads();
+    // dW2[cc][k] = sum_r g2[r][cc] h1[r][k]
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = t + GT * q, cc = e / SN_H, k = e % SN_H;
+      float acc = 0.f;
+      for (int r = 0; r < TILE; ++r) acc += s.g2[r][cc] * s.h1[r][k];
+      gW2[q] += acc;
+    }
+    // per-column vectors: db1 (t<32, after g1), db2 (32..63), dw3 (64..95), db3 (96)
+    if (t >= 32 && t < 64) {
+      float acc = 0.f;
+      for (int r = 0; r < TILE; ++r) acc += s.g2[r][t - 32];
+      gvec += acc;
+    } else if (t >= 64 && t < 96) {
+      float acc = 0.f;
+      for (int r = 0; r < TILE; ++r) acc += s.dz[r] * s.h2[r][t - 64];
+      gvec += acc;
+    } else if (t == 96) {
+      float acc = 0.f;
+      for (int r = 0; r < TILE; ++r) acc += s.dz[r];
+      gvec += acc;
+    }
+    // g1[r][k] = (sum_c g2[r][c] W2[c][k]) * relu'(h1)
+    for (int r = rb; r < TILE; r += 8) {
+      float acc = 0.f;
+#pragma unroll
+      for (int cc = 0; cc < SN_H; ++cc) acc += s.g2[r][cc] * s.W2[cc][c];
+      s.g1[r][c] = s.h1[r][c] > 0.f ? acc : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      const int e = t + GT * q;
+      if (e < SN_H * SN_IN) {
+        const int cc = e / SN_IN, k = e % SN_IN;
+        float acc = 0.f;
+        for (int r = 0; r < TILE; ++r) acc += s.g1[r][cc] * s.x[r][k];
+        gW1[q] += acc;
+      }
+    }
+    if (t < 32) {
+      float acc = 0.f;
+      for (int r = 0; r < TILE; ++r) acc += s.g1[r][t];
+      gvec += acc;
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) atomicAdd(&G[SP_W2 + t + GT * q], gW2[q]);
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    if (t + GT * q < SN_H * SN_IN) atomicAdd(&G[SP_W1 + t + GT * q], gW1[q]);
+  if (t < 32) atomicAdd(&G[SP_B1 + t], gvec);
+  else if (t < 64) atomicAdd(&G[SP_B2 + t - 32], gvec);
+  else if (t < 96) atomicAdd(&G[SP_W3 + t - 64], gvec);
+  else if (t == 96) atomicAdd(&G[SP_B3], gvec);
+  if (t < TILE) {
+    float l = lsum;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((t & 31) == 0) atomicAdd(loss, l);
+  }
+}
+
+// ---------------------------------------------------------------- audit
+__global__ void __launch_bounds__(128) sensor_audit_kernel(const AuditArgs a) {
+  if (a.check_done && a.st->done) return;
+  const Dims& d = a.d;
+  const long nf = total_faces(d);
+  const unsigned off = a.st->steps % a.stride;
+  const long e = (blockIdx.x * (long)blockDim.x + threadIdx.x) * a.stride + off;
+  float err = 0.f;
+  bool audited = false;
+  int dir, i, j, k;
+  if (e < nf && a.mask[e] == 0 && decode_face(d, e, dir, i, j, k)) {
+    const long sd = dir == 0 ? 1 : (dir == 1 ? d.PX : d.PL);
+    const long oa = node_off(d, i, j, k), ob = oa + sd;
+    auto ld = [&](int p, int n) -> float { return (float)__ldg(a.q + n * d.VOL + oa + (p - 2) * sd); };
+    const float nx = (float)(0.5 * (__ldg(a.area[3 * dir] + oa) + __ldg(a.area[3 * dir] + ob)));
+    const float ny = (float)(0.5 * (__ldg(a.area[3 * dir + 1] + oa) + __ldg(a.area[3 * dir + 1] + ob)));
+    const float nz = (float)(0.5 * (__ldg(a.area[3 * dir + 2] + oa) + __ldg(a.area[3 * dir + 2] + ob)));
+    const FluxConsts<float> C{a.gamma, a.gam1, a.gam1_inv};
+    float fw[5], fl[5];
+    face_flux<float>(ld, nx, ny, nz, C, fw);
+    face_flux_linear<float>(ld, nx, ny, nz, C, fl);
+    float num = 0.f, den = 0.f;
+#pragma unroll
+    for (int n = 0; n < 5; ++n) {
+      num = fmaxf(num, fabsf(fw[n] - fl[n]));
+      den = fmaxf(den, fabsf(fw[n]));
+    }
+    err = num / (den + 1.0e-20f);
+    if (!(err == err)) err = 3.0e38f;
+    audited = true;
+  }
+  const unsigned full = 0xffffffffu;
+  const unsigned n_aud = __popc(__ballot_sync(full, audited));
+  float m = err;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(full, m, o));
+  if ((threadIdx.x & 31) == 0 && n_aud) {
+    atomicAdd(&a.st->audit_faces, (unsigned long long)n_aud);
+    atomicMax(reinterpret_cast<int*>(&a.st->audit_max), __float_as_int(m));  // m >= 0: int order = float order
+    if (m > a.bound && atomicExch(&a.st->force_weno, 1) == 0) atomicAdd(&a.st->audit_fail_steps, 1u);
+  }
+}
+
+__global__ void adam_kernel(float* P, const float* G, float* M, float* V, float lr, float c1, float c2) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= SP_N) return;
+  const float g = G[e];
+  const float m = 0.9f * M[e] + 0.1f * g;
+  const float v = 0.999f * V[e] + 0.001f * g * g;
+  M[e] = m;
+  V[e] = v;
+  P[e] -= lr * (m * c1) / (sqrtf(v * c2) + 1.0e-8f);
+}
+
+__global__ void mlp_predict_kernel(const float* __restrict__ P, const float* __restrict__ X, unsigned n,
+                                   float* __restrict__ out) {
+  __shared__ float sp[SP_N];
+  for (int e = threadIdx.x; e < SP_N; e += blockDim.x) sp[e] = P[e];
+  __syncthreads();
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float x[SN_IN];
+#pragma unroll
+  for (int k = 0; k < SN_IN; ++k) x[k] = X[(size_t)i * SN_IN + k];
+  out[i] = 1.f / (1.f + __expf(-mlp_forward(sp, x)));
+}
+
+}  // namespace
+
+cudaError_t launch_sample_faces(const SampleArgs& a, cudaStream_t s) {
+  const Dims& d = a.d;
+  const long n = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2) + (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2) +
+                 (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 1);
+  sample_faces_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sensor_audit(const AuditArgs& a, cudaStream_t s) {
+  const long nf = (long)(a.d.IM - 1) * (a.d.JM - 2) * (a.d.KM - 2) + (long)(a.d.IM - 2) * (a.d.JM - 1) * (a.d.KM - 2) +
+                  (long)(a.d.IM - 2) * (a.d.JM - 2) * (a.d.KM - 1);
+  const long n = (nf + a.stride - 1) / a.stride;
+  sensor_audit_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_grad(const float* P, const float* X, const unsigned char* Y, unsigned n, float pos_w, float* G,
+                            float* loss, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(G, 0, SP_N * sizeof(float), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(loss, 0, sizeof(float), s);
+  if (e != cudaSuccess) return e;
+  if (n == 0) return cudaSuccess;
+  static bool attr = false;
+  if (!attr) {
+    e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GradSmem));
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  const unsigned ntiles = (n + TILE - 1) / TILE;
+  const unsigned grid = ntiles < 296u ? ntiles : 296u;
+  mlp_grad_kernel<<<grid, GT, sizeof(GradSmem), s>>>(P, X, Y, n, pos_w, 1.0f / (float)n, G, loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float* P, const float* G, float* M, float* V, unsigned step, float lr, cudaStream_t s) {
+  const float c1 = 1.0f / (1.0f - powf(0.9f, (float)step));
+  const float c2 = 1.0f / (1.0f - powf(0.999f, (float)step));
+  adam_kernel<<<(SP_N + 255) / 256, 256, 0, s>>>(P, G, M, V, lr, c1, c2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mlp_predict(const float* P, const float* X, unsigned n, float* out, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  mlp_predict_kernel<<<(n + 255) / 256, 256, 0, s>>>(P, X, n, out);
+  return cudaGetLastError();
+}
+
+}  // namespace cbns

@@ -64,7 +64,8 @@ __device__ __forceinline__ double d4(const double* f, long o, long s) {
 // NB = CTAs per SM the register budget is cut for: FP64 always 2 (shared
 // memory allows no more); FP32 is built for 2 (128 registers, no spills) and 3
 // (80 registers, a few spills) and cbns_autotune keeps the faster.
-template <typename R, bool VISC, int MODE, int NB>
+// HYB: hybrid flux (learned-sensor decision per face, see the flux lambda).
+template <typename R, bool VISC, int MODE, int NB, bool HYB>
 __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
   using S = R;  // shared-memory storage type
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -87,6 +88,21 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
   constexpr bool kExactRing = sizeof(S) == 8;
 
   const FluxConsts<R> C{(R)a.gamma, (R)a.gam1, (R)a.gam1_inv};
+
+  // Face flux.  The hybrid kernel reads the sensor's decision byte of the face
+  // (global face index e: i-faces, j-faces, k-faces in the reference's
+  // Ep/Fp/Gp order): 1 = characteristic WENO5, 0 = linear upwind-5; when the
+  // audit has set force_weno the whole step uses WENO5.
+  const bool all_weno = !HYB || st->force_weno;
+  const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
+  const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
+  auto flux = [&](const auto& ld, R nx, R ny, R nz, long e, R out[5]) {
+    if (HYB && !all_weno && __ldg(a.mask + e) == 0) {
+      face_flux_linear<R>(ld, nx, ny, nz, C, out);
+    } else {
+      face_flux<R>(ld, nx, ny, nz, C, out);
+    }
+  };
 
   // column owned by this thread
   const int cx = t % TI, cy = t / TI;
@@ -118,7 +134,8 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
       s = s >= 6 ? s - 6 : s;
       return (R)sm.ring[s][n][t];
     };
-    face_flux<R>(ld, R(0.5) * (za[0] + zb[0]), R(0.5) * (za[1] + zb[1]), R(0.5) * (za[2] + zb[2]), C, out);
+    const long e = nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * kk);
+    flux(ld, R(0.5) * (za[0] + zb[0]), R(0.5) * (za[1] + zb[1]), R(0.5) * (za[2] + zb[2]), e, out);
   };
 
   // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
@@ -201,9 +218,10 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
       if (ga <= d.IM - 2 && gj <= d.JM - 2) {
         auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
         R f[5];
-        face_flux<R>(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
-                     R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
-                     R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), C, f);
+        const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
+        flux(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
+             R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
+             R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), e, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
       }
@@ -215,9 +233,10 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
       if (gi <= d.IM - 2 && ga <= d.JM - 2) {
         auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
         R f[5];
-        face_flux<R>(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
-                     R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
-                     R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), C, f);
+        const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
+        flux(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
+             R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
+             R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), e, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
       }
@@ -331,42 +350,42 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
   }
 }
 
-template <typename R, bool VISC, int MODE, int NB>
+template <typename R, bool VISC, int MODE, int NB, bool HYB>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
   const size_t smem = sizeof(Smem<R, R>);
   dim3 grid(a.ntile_i * a.ntile_j, (a.d.KM - 2 + a.kchunk - 1) / a.kchunk);
-  stage_kernel<R, VISC, MODE, NB><<<grid, NT, smem, s>>>(a);
+  stage_kernel<R, VISC, MODE, NB, HYB><<<grid, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <typename R, int NB>
+template <typename R, int NB, bool HYB>
 void prepare_nb() {
   const int smem = (int)sizeof(Smem<R, R>);
-  cudaFuncSetAttribute(stage_kernel<R, false, 0, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, false, 1, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, false, 2, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, false, 3, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 0, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 1, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 2, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 3, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, false, 0, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, false, 1, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, false, 2, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, false, 3, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 0, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 1, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 2, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaFuncSetAttribute(stage_kernel<R, true, 3, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 
-template <typename R, int NB>
+template <typename R, int NB, bool HYB>
 cudaError_t launch_r(const StageArgs& a, int mode, bool visc, cudaStream_t s) {
   if (visc) {
     switch (mode) {
-      case 0: return launch_t<R, true, 0, NB>(a, s);
-      case 1: return launch_t<R, true, 1, NB>(a, s);
-      case 2: return launch_t<R, true, 2, NB>(a, s);
-      default: return launch_t<R, true, 3, NB>(a, s);
+      case 0: return launch_t<R, true, 0, NB, HYB>(a, s);
+      case 1: return launch_t<R, true, 1, NB, HYB>(a, s);
+      case 2: return launch_t<R, true, 2, NB, HYB>(a, s);
+      default: return launch_t<R, true, 3, NB, HYB>(a, s);
     }
   }
   switch (mode) {
-    case 0: return launch_t<R, false, 0, NB>(a, s);
-    case 1: return launch_t<R, false, 1, NB>(a, s);
-    case 2: return launch_t<R, false, 2, NB>(a, s);
-    default: return launch_t<R, false, 3, NB>(a, s);
+    case 0: return launch_t<R, false, 0, NB, HYB>(a, s);
+    case 1: return launch_t<R, false, 1, NB, HYB>(a, s);
+    case 2: return launch_t<R, false, 2, NB, HYB>(a, s);
+    default: return launch_t<R, false, 3, NB, HYB>(a, s);
   }
 }
 
@@ -377,9 +396,11 @@ cudaError_t launch_r(const StageArgs& a, int mode, bool visc, cudaStream_t s) {
 void stage_prepare() {
   static bool done = false;
   if (done) return;
-  prepare_nb<double, 2>();
-  prepare_nb<float, 2>();
-  prepare_nb<float, 3>();
+  prepare_nb<double, 2, false>();
+  prepare_nb<float, 2, false>();
+  prepare_nb<float, 3, false>();
+  prepare_nb<float, 2, true>();
+  prepare_nb<float, 3, true>();
   done = true;
 }
 
@@ -391,8 +412,9 @@ void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j) {
 int stage_variants(bool fp32) { return fp32 ? 2 : 1; }
 
 cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s) {
-  if (!fp32) return launch_r<double, 2>(a, mode, visc, s);
-  return variant == 1 ? launch_r<float, 3>(a, mode, visc, s) : launch_r<float, 2>(a, mode, visc, s);
+  if (!fp32) return launch_r<double, 2, false>(a, mode, visc, s);
+  if (a.mask) return variant == 1 ? launch_r<float, 3, true>(a, mode, visc, s) : launch_r<float, 2, true>(a, mode, visc, s);
+  return variant == 1 ? launch_r<float, 3, false>(a, mode, visc, s) : launch_r<float, 2, false>(a, mode, visc, s);
 }
 
 }  // namespace cbns

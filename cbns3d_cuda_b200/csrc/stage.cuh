@@ -17,6 +17,7 @@ struct StageArgs {
   const double* vflux[12];
   double* prim[6];     // viscous: rho,u,v,w,p,T of the new interior state
   StepState* st;       // dt, done flag, spectral-radius max
+  const unsigned char* mask;  // hybrid: per-face sensor decision (null: plain flux everywhere)
   int q0_is_src, qp_is_src;  // RK operands that equal the stage input (read from the ring)
   int ntile_i, ntile_j, kchunk;
   int visdiv;          // CBNS_VISDIV_*

@@ -85,6 +85,7 @@ __global__ void step_prologue(StepState* st, double CFL) {
   st->dt = dt;
   st->t_cur = t_cur + dt;
   st->sigma_bits = 0ull;  // stage 3 of this step accumulates the next maximum
+  st->force_weno = 0;     // the hybrid's audit decides afresh for every step
   st->steps += 1;
 }
 

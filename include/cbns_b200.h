@@ -159,6 +159,76 @@ int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f,
 int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM, const double* f,
                                double* fx, double* fy, double* fz);
 
+/* Learned shock sensor (no counterpart in the reference).  A network of
+ * CBNS_SENSOR_NIN inputs, two hidden layers of CBNS_SENSOR_NHID ReLU units and
+ * one sigmoid output estimates, per grid face, the probability that the face
+ * needs the full characteristic WENO5 flux.  Parameters are a float vector of
+ * CBNS_SENSOR_NPARAM values: W1[32][15] b1[32] W2[32][32] b2[32] w3[32] b3.
+ * Features of a face: the jumps of density, pressure and normal velocity
+ * across its 5-point stencil, divided by the face's mean density, pressure and
+ * sound speed.  Label: 1 when the WENO5 nonlinear weights of the face's
+ * characteristic reconstruction depart from the linear weights by more than
+ * 0.05.  Pointers marked _dev are device pointers; stream is a cudaStream_t. */
+#define CBNS_SENSOR_NIN    15
+#define CBNS_SENSOR_NHID   32
+#define CBNS_SENSOR_NPARAM 1601
+/* Features, labels (and, where the pointers are not null, the weight
+ * deviation and the global face index) of the faces whose global index i
+ * satisfies i % stride == offset, from the given state buffer.  Global face
+ * index: i-faces, then j-faces, then k-faces, each in the order of the
+ * reference's Ep/Fp/Gp arrays (include/Block3d_cuda.h:110-123).  Samples are
+ * written in no particular order; at most capacity faces are written and
+ * *count gets the number sampled (which may exceed capacity). */
+int cbns_sensor_sample(cbns_ctx* ctx, int which, unsigned stride, unsigned offset, float* feat_dev,
+                       unsigned char* label_dev, float* dev_dev, unsigned* index_dev, unsigned capacity,
+                       unsigned* count);
+/* Mean weighted binary cross-entropy over n samples (positive class weight
+ * pos_weight) and its gradient with respect to every parameter. */
+int cbns_mlp_grad(const float* params_dev, const float* x_dev, const unsigned char* y_dev, unsigned n,
+                  float pos_weight, float* grad_dev, float* loss_dev, void* stream);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) at step number step >= 1. */
+int cbns_mlp_adam(float* params_dev, const float* grad_dev, float* m_dev, float* v_dev, unsigned step,
+                  float lr, void* stream);
+/* Probabilities for n feature vectors: FP32 on the CUDA cores, or BF16 on the
+ * tcgen05 tensor cores (use_tensor_cores != 0; *status_dev is set non-zero if
+ * a tensor-core wait timed out). */
+int cbns_mlp_predict(const float* params_dev, const float* x_dev, unsigned n, float* out_dev,
+                     int use_tensor_cores, int* status_dev, void* stream);
+
+/* The hybrid flux (CBNS_PREC_HYBRID).  Every time step the network is
+ * evaluated on every face of the step's starting state on the tensor cores;
+ * faces with probability >= tau take the characteristic WENO5 flux, the others
+ * the linear upwind-5 flux (same Lax-Friedrichs splitting, component-wise).
+ * The decisions hold for the three stages of the step.  An audit recomputes,
+ * on the linear faces with (global face index % audit_stride) equal to
+ * (step % audit_stride), both fluxes; a relative difference above audit_bound
+ * on any of them makes the whole step take WENO5 everywhere.  A context of
+ * precision HYBRID refuses to step (CBNS_ERR_STATE) until cbns_sensor_load.
+ * params_host: CBNS_SENSOR_NPARAM floats in host memory. */
+int cbns_sensor_load(cbns_ctx* ctx, const float* params_host, float tau);
+/* audit_stride >= 1 (1 audits every linear face every step); audit_bound > 0
+ * (relative to the face's largest flux component).  Defaults 97 and 1e-2. */
+int cbns_sensor_audit(cbns_ctx* ctx, unsigned audit_stride, float audit_bound);
+/* Counters since the last cbns_sensor_stats_reset: faces sent to WENO5 by the
+ * network (summed over steps), faces audited, steps whose decisions the audit
+ * rejected, the largest relative difference the audit saw, and a non-zero
+ * sensor_fail when a tensor-core wait timed out (the step then took WENO5). */
+typedef struct cbns_sensor_stats {
+  unsigned long long weno_faces;
+  unsigned long long audit_faces;
+  unsigned audit_fail_steps;
+  float audit_max;
+  int sensor_fail;
+  unsigned long long faces_per_step;
+} cbns_sensor_stats;
+int cbns_sensor_stats_get(cbns_ctx* ctx, cbns_sensor_stats* stats);
+/* The decisions of the latest sensor evaluation (one byte per face in global
+ * face index order, 1 = WENO5) copied to mask_host, which holds n >=
+ * faces_per_step bytes; *forced (may be null) = 1 when the audit (or a
+ * tensor-core timeout) made that step take WENO5 everywhere. */
+int cbns_sensor_mask_get(cbns_ctx* ctx, unsigned char* mask_host, unsigned long long n, int* forced);
+int cbns_sensor_stats_reset(cbns_ctx* ctx);
+
 /* Pick, by timing on the current state, the fastest compiled variant of the
  * stage kernel for this context's precision (the state is not modified);
  * *chosen (may be null) receives the variant index.  Later steps use it. */
@@ -166,7 +236,8 @@ int cbns_autotune(cbns_ctx* ctx, int* chosen);
 
 /* Per-kernel device timing with CUDA events on the launch stream.  Kernel ids:
  * 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous node
- * fluxes, 3 dt/step bookkeeping.  total_ms is the summed event time. */
+ * fluxes, 3 dt/step bookkeeping, 4 hybrid sensor and audit.  total_ms is the
+ * summed event time. */
 int cbns_prof_enable(cbns_ctx* ctx, int on);
 int cbns_prof_read(cbns_ctx* ctx, int kernel_id, double* total_ms, unsigned* launches);
 int cbns_prof_reset(cbns_ctx* ctx);

@@ -245,6 +245,7 @@ struct Oracle {
   std::vector<double> tau[6];    // xx, yy, zz, xy, xz, yz
   std::vector<double> qf[3];
   std::vector<double> Ev, Fv, Gv, dfv, Ep, Fp, Gp, dtn;
+  std::vector<unsigned char> hmask;  // hybrid flux decisions (1 = WENO5); empty = WENO5 everywhere
   bool have_metrics = false;
 
   explicit Oracle(const cbns_params& p) : P(p), D(derive(p)) {
@@ -484,6 +485,32 @@ struct Oracle {
   // ---------------------------------------------------------------------------
   // One face of rec_riemann_{xi,eta,zeta}_kernel (src/rec_riemann_kernel.cu:15-247):
   // nodes a (low) and b (high) along direction with stride sd, metric arrays mx,my,mz.
+  // Linear upwind-5 face flux of the hybrid scheme (no counterpart in the
+  // reference): each conservative component reconstructed with the WENO5
+  // optimal weights frozen, (2a - 13b + 47c + 27d - 3e) / 60 on both sides,
+  // then the same Lax-Friedrichs flux as the WENO5 face.
+  void face_linear(const std::vector<double>& Q, long ta, long sd, int mdir, double* out) const {
+    const long tb = ta + sd;
+    const double Ja = met[9][ta], Jb = met[9][tb];
+    const double nx = 0.5 * (met[3 * mdir + 0][ta] * Ja + met[3 * mdir + 0][tb] * Jb);
+    const double ny = 0.5 * (met[3 * mdir + 1][ta] * Ja + met[3 * mdir + 1][tb] * Jb);
+    const double nz = 0.5 * (met[3 * mdir + 2][ta] * Ja + met[3 * mdir + 2][tb] * Jb);
+    double ql[5], qh[5];
+    for (int n = 0; n < 5; ++n) {
+      const double f0 = Q[5 * (ta - 2 * sd) + n], f1 = Q[5 * (ta - sd) + n], f2 = Q[5 * ta + n];
+      const double f3 = Q[5 * tb + n], f4 = Q[5 * (tb + sd) + n], f5 = Q[5 * (tb + 2 * sd) + n];
+      ql[n] = (2.0 * f0 - 13.0 * f1 + 47.0 * f2 + 27.0 * f3 - 3.0 * f4) / 60.0;
+      qh[n] = (2.0 * f5 - 13.0 * f4 + 47.0 * f3 + 27.0 * f2 - 3.0 * f1) / 60.0;
+    }
+    lf_flux(to_prim(qh, D.gam1), to_prim(ql, D.gam1), nx, ny, nz, P.gamma, D.gam1, out);
+  }
+
+  // Face flux under the hybrid mask (empty mask: WENO5 everywhere).
+  void face_h(const std::vector<double>& Q, long e, long ta, long sd, int mdir, double* out) const {
+    if (!hmask.empty() && hmask[e] == 0) face_linear(Q, ta, sd, mdir, out);
+    else face(Q, ta, sd, mdir, out);
+  }
+
   void face(const std::vector<double>& Q, long ta, long sd, int mdir, double* out) const {
     const long tb = ta + sd;
     const double Ja = met[9][ta], Jb = met[9][tb];
@@ -504,24 +531,33 @@ struct Oracle {
   }
 
   // calc_numerical_flux: src/calc_numerical_flux.cu:15-74.
+  // With a hybrid mask set, faces whose mask byte is 0 take face_linear;
+  // mask index: i-faces, then j-faces, then k-faces, each in Ep/Fp/Gp order.
   void calc_numerical_flux(int which) {
     const auto& Q = buf(which);
     const long sI = 1, sJ = IG, sK = IG * JG;
+    const long ni = (IM - 1) * (JM - 2) * (KM - 2), nj = (IM - 2) * (JM - 1) * (KM - 2);
 #pragma omp parallel for schedule(dynamic, 1)
     for (long k = 0; k < KM - 2; ++k)
       for (long j = 0; j < JM - 2; ++j)
-        for (long i = 0; i < IM - 1; ++i)
-          face(Q, g(i, j + 1, k + 1), sI, 0, &Ep[NEQ * (i + (IM - 1) * (j + (JM - 2) * k))]);
+        for (long i = 0; i < IM - 1; ++i) {
+          const long e = i + (IM - 1) * (j + (JM - 2) * k);
+          face_h(Q, e, g(i, j + 1, k + 1), sI, 0, &Ep[NEQ * e]);
+        }
 #pragma omp parallel for schedule(dynamic, 1)
     for (long k = 0; k < KM - 2; ++k)
       for (long j = 0; j < JM - 1; ++j)
-        for (long i = 0; i < IM - 2; ++i)
-          face(Q, g(i + 1, j, k + 1), sJ, 1, &Fp[NEQ * (i + (IM - 2) * (j + (JM - 1) * k))]);
+        for (long i = 0; i < IM - 2; ++i) {
+          const long e = i + (IM - 2) * (j + (JM - 1) * k);
+          face_h(Q, ni + e, g(i + 1, j, k + 1), sJ, 1, &Fp[NEQ * e]);
+        }
 #pragma omp parallel for schedule(dynamic, 1)
     for (long k = 0; k < KM - 1; ++k)
       for (long j = 0; j < JM - 2; ++j)
-        for (long i = 0; i < IM - 2; ++i)
-          face(Q, g(i + 1, j + 1, k), sK, 2, &Gp[NEQ * (i + (IM - 2) * (j + (JM - 2) * k))]);
+        for (long i = 0; i < IM - 2; ++i) {
+          const long e = i + (IM - 2) * (j + (JM - 2) * k);
+          face_h(Q, ni + nj + e, g(i + 1, j + 1, k), sK, 2, &Gp[NEQ * e]);
+        }
   }
 
   // Flux difference + viscous contribution over J at interior node (i,j,k),
@@ -788,6 +824,78 @@ void orc_eval_rhs(void* h, int which, double* rhs) {
     for (long j = 1; j <= J2; ++j)
       for (long i = 1; i <= I2; ++i) o->df_at(i, j, k, &rhs[5 * ((i - 1) + I2 * ((j - 1) + J2 * (k - 1)))]);
 }
+// Hybrid flux decisions for the following flux evaluations: n bytes in global
+// face index order (1 = WENO5, 0 = linear upwind-5); n = 0 clears the mask.
+void orc_set_face_mask(void* h, const unsigned char* mask, long n) {
+  auto* o = static_cast<Oracle*>(h);
+  if (n <= 0 || !mask) o->hmask.clear();
+  else o->hmask.assign(mask, mask + n);
+}
+
+// Sensor features and WENO-weight deviation of every grid face, in the order
+// i-faces, j-faces, k-faces (each i fastest), for the learned shock sensor
+// (no counterpart in the reference).  Restates the definitions of the
+// library's sensor.cuh in FP64: 15 normalised jumps of density, pressure and
+// normal velocity; deviation = max |w_k - d_k| of the characteristic WENO5
+// weights (basis and Roe average of the flux) on both sides of all 5 fields.
+void orc_sensor_faces(void* h, int which, float* feat, float* dev) {
+  auto* o = static_cast<Oracle*>(h);
+  const auto& Q = o->buf(which);
+  const long IM = o->IM, JM = o->JM, KM = o->KM;
+  const long ni = (IM - 1) * (JM - 2) * (KM - 2), nj = (IM - 2) * (JM - 1) * (KM - 2), nk = (IM - 2) * (JM - 2) * (KM - 1);
+  const double gam1 = o->D.gam1, gamma = o->P.gamma;
+#pragma omp parallel for schedule(static)
+  for (long e = 0; e < ni + nj + nk; ++e) {
+    int dir;
+    long i, j, k;
+    if (e < ni) { dir = 0; i = e % (IM - 1); j = 1 + (e / (IM - 1)) % (JM - 2); k = 1 + e / ((IM - 1) * (JM - 2)); }
+    else if (e < ni + nj) { const long r = e - ni; dir = 1; i = 1 + r % (IM - 2); j = (r / (IM - 2)) % (JM - 1); k = 1 + r / ((IM - 2) * (JM - 1)); }
+    else { const long r = e - ni - nj; dir = 2; i = 1 + r % (IM - 2); j = 1 + (r / (IM - 2)) % (JM - 2); k = r / ((IM - 2) * (JM - 2)); }
+    const long sd = dir == 0 ? 1 : (dir == 1 ? o->IG : o->IG * o->JG);
+    const long ta = o->g(i, j, k), tb = ta + sd;
+    const double Ja = o->met[9][ta], Jb = o->met[9][tb];
+    const double nx = 0.5 * (o->met[3 * dir][ta] * Ja + o->met[3 * dir][tb] * Jb);
+    const double ny = 0.5 * (o->met[3 * dir + 1][ta] * Ja + o->met[3 * dir + 1][tb] * Jb);
+    const double nz = 0.5 * (o->met[3 * dir + 2][ta] * Ja + o->met[3 * dir + 2][tb] * Jb);
+    const double nn = std::sqrt(nx * nx + ny * ny + nz * nz);
+    double r[6], pr[6], un[6];
+    for (int q = 0; q < 6; ++q) {
+      const Prim s = to_prim(&Q[5 * (ta + (q - 2) * sd)], gam1);
+      r[q] = s.r; pr[q] = s.p; un[q] = (s.u * nx + s.v * ny + s.w * nz) / nn;
+    }
+    const double rb = 0.5 * (r[2] + r[3]), pb = 0.5 * (pr[2] + pr[3]), cb = std::sqrt(gamma * pb / rb);
+    for (int m = 0; m < 5; ++m) {
+      feat[15 * e + m] = (float)((r[m + 1] - r[m]) / rb);
+      feat[15 * e + 5 + m] = (float)((pr[m + 1] - pr[m]) / pb);
+      feat[15 * e + 10 + m] = (float)((un[m + 1] - un[m]) / cb);
+    }
+    const Prim a = to_prim(&Q[5 * ta], gam1), b = to_prim(&Q[5 * tb], gam1);
+    double R[5][5], L[5][5];
+    roe_eigen(a, b, nx, ny, nz, gamma, gam1, R, L);
+    double W[5][6];
+    for (int q = 0; q < 6; ++q)
+      for (int s = 0; s < 5; ++s) {
+        double acc = 0.0;
+        for (int n = 0; n < 5; ++n) acc += L[s][n] * Q[5 * (ta + (q - 2) * sd) + n];
+        W[s][q] = acc;
+      }
+    auto wdev = [](double A, double B, double Cc, double Dd, double E) {
+      const double eps = 1.0e-6;
+      const double s1 = (13.0 / 12.0) * (A - 2 * B + Cc) * (A - 2 * B + Cc) + 0.25 * (A - 4 * B + 3 * Cc) * (A - 4 * B + 3 * Cc) + eps;
+      const double s2 = (13.0 / 12.0) * (B - 2 * Cc + Dd) * (B - 2 * Cc + Dd) + 0.25 * (B - Dd) * (B - Dd) + eps;
+      const double s3 = (13.0 / 12.0) * (Cc - 2 * Dd + E) * (Cc - 2 * Dd + E) + 0.25 * (3 * Cc - 4 * Dd + E) * (3 * Cc - 4 * Dd + E) + eps;
+      const double a1 = 0.1 / (s1 * s1), a2 = 0.6 / (s2 * s2), a3 = 0.3 / (s3 * s3), t = a1 + a2 + a3;
+      return std::max(std::max(std::abs(a1 / t - 0.1), std::abs(a2 / t - 0.6)), std::abs(a3 / t - 0.3));
+    };
+    double dv = 0.0;
+    for (int s = 0; s < 5; ++s) {
+      dv = std::max(dv, wdev(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4]));
+      dv = std::max(dv, wdev(W[s][5], W[s][4], W[s][3], W[s][2], W[s][1]));
+    }
+    dev[e] = (float)dv;
+  }
+}
+
 // calc_gradient (src/calc_gradient.cu:17-51): gradient of an unghosted field.
 void orc_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f, double* fx, double* fy,
                        double* fz) {

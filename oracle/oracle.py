@@ -60,6 +60,8 @@ def load():
         "orc_solve": (C.c_int, [V, C.c_uint, C.c_double, D, C.POINTER(C.c_uint)]),
         "orc_eval_rhs": (None, [V, C.c_int, D]),
         "orc_calc_gradient": (None, [C.c_uint, C.c_uint, C.c_uint, D, D, D, D]),
+        "orc_sensor_faces": (None, [V, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "orc_set_face_mask": (None, [V, C.c_void_p, C.c_long]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -176,6 +178,25 @@ class OracleBlock:
         out = np.empty(NEQ * (self.IM - 2) * (self.JM - 2) * (self.KM - 2))
         self.lib.orc_eval_rhs(self.h, which, _p(out))
         return out
+
+    def set_face_mask(self, mask=None):
+        """Hybrid decisions (uint8 per face, 1 = WENO5) for later flux
+        evaluations; None restores WENO5 everywhere."""
+        if mask is None:
+            self.lib.orc_set_face_mask(self.h, None, 0)
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        self.lib.orc_set_face_mask(self.h, m.ctypes.data, m.size)
+
+    def sensor_faces(self, which=0):
+        """(features n x 15, deviation n) of every face, i-, j-, then k-faces."""
+        IM, JM, KM = self.IM, self.JM, self.KM
+        n = (IM - 1) * (JM - 2) * (KM - 2) + (IM - 2) * (JM - 1) * (KM - 2) + (IM - 2) * (JM - 2) * (KM - 1)
+        f = np.empty((n, 15), dtype=np.float32)
+        d = np.empty(n, dtype=np.float32)
+        self.lib.orc_sensor_faces(self.h, which, f.ctypes.data_as(C.POINTER(C.c_float)),
+                                  d.ctypes.data_as(C.POINTER(C.c_float)))
+        return f, d
 
     def init_like_reference(self, x, y, z, Q0=None):
         """calc_metrics, the start state and the first boundary pass of

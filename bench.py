@@ -1,21 +1,24 @@
 #!/usr/bin/env python
 """Throughput of the RK3 right-hand-side path: cell-updates per second.
 
-One step = one full SSP-RK3 step (three fused stage kernels, boundary
-conditions, device-side CFL dt) of one block of synthetic input.  Default
-workload: the shock-vortex case of 256 x 256 x 128 nodes (inviscid; inputs
-larger than L2, so no flush is needed).  A cell-update is one interior node
-advanced one step; N_upd = (IM-2)(JM-2)(KM-2).
+One step = one full SSP-RK3 step (sensor + audit for the hybrid, three fused
+stage kernels, boundary conditions, device-side CFL dt) of one block of
+synthetic input.  Default workload: the shock-vortex case of 256 x 256 x 128
+nodes (inviscid; inputs larger than L2, so no flush is needed), W + K = 103
+steps from the initial state.  A cell-update is one interior node advanced one
+step; N_upd = (IM-2)(JM-2)(KM-2).
 
-  value   device-resident throughput of the split-precision path (FP32 flux
-          arithmetic, FP64 state/metrics/reductions), timed with CUDA events on
-          the launch stream; its density L2 error against the FP64 path after
-          the same steps is reported and must stay <= 1e-5.
-  paths   the same for the plain FP64 path (parity with the reference).
-  e2e     the reference-style host-driven solve through the C ABI
-          (block3d_cuda call sequence: dt read back every step, dt passed per
-          stage), with the state uploaded from pinned host memory before and
-          downloaded after the K steps inside the timed region.
+  value   device-resident throughput of the learned-sensor hybrid (per face
+          WENO5-characteristic or linear upwind-5 flux in FP32, FP64 state,
+          metrics and reductions), timed with CUDA events on the launch stream;
+          its density L2 error against the plain FP64 path after the same steps
+          is reported beside it and must stay <= 1e-5.
+  paths   the same for the plain FP64 path (parity with the reference) and the
+          split-precision path without the sensor (all faces WENO5 in FP32).
+  e2e     the reference-style host-driven solve of the hybrid through the C
+          ABI (block3d_cuda call sequence: dt read back every step, dt passed
+          per stage), with the state uploaded from pinned host memory before
+          and downloaded after the K steps inside the timed region.
   roofline  HBM roofline of the dominant kernel (the fused stage kernel).
   cpu_baseline  the FP64 CPU oracle (OpenMP, all host cores) on a bounded sample.
 
@@ -51,13 +54,14 @@ ALG_BYTES_PER_UPDATE = 560.0
 def args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="shock_vortex", choices=["shock_vortex", "blast", "vortex"])
     ap.add_argument("--size", default=None, help="IMxJMxKM (default: the case's config size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--sensor", default=str(ROOT / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz"))
     return ap.parse_args()
 
 
@@ -119,14 +123,26 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+SENSOR = None  # (params, tau) of the trained sensor network
+
+
+def load_sensor(path):
+    global SENSOR
+    w = np.load(path)
+    SENSOR = (w["params"].astype(np.float32), float(w["tau"]))
+    return SENSOR
+
+
 def init_block(case, precision):
-    from cbns3d_cuda_b200 import CBNS_Q, Block, make_params
+    from cbns3d_cuda_b200 import CBNS_Q, PREC_HYBRID, Block, make_params
     p = dict(case.params)
     p["precision"] = precision
     b = Block(make_params(*case.shape, **p))
     b.calc_metrics(case.x, case.y, case.z)
     b.set_conservative(case.Q0)
     b.set_bc_calc_primitive(CBNS_Q)
+    if precision == PREC_HYBRID:
+        b.sensor_load(*SENSOR)
     return b
 
 
@@ -143,52 +159,53 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def device_pass(case, precision, K, W, torch, dist):
-    """W untimed steps, then K timed steps with per-kernel events; returns
-    (ms, block, per-kernel stats, launches)."""
+def device_pass(case, precision, K, W, torch, dist, clocks=None):
+    """W untimed steps, K steps replayed from the CUDA graph and timed with
+    events on the launch stream (optionally with clock sampling), the state
+    read back, then K more steps with events around every kernel for the
+    per-kernel breakdown.  Returns a dict."""
+    from cbns3d_cuda_b200 import PREC_HYBRID
     b = init_block(case, precision)
     stream = torch.cuda.Stream()  # a real stream: the legacy default stream cannot be graph-captured
     b.set_stream(stream.cuda_stream)
-    b.torch_stream = stream
-    b.variant = b.autotune()
+    out = {"variant": b.autotune()}
     b.set_time(0.0)
     b.run(W)
-    b.prof_enable(True)
-    b.prof_reset()
+    if precision == PREC_HYBRID:
+        b.sensor_stats_reset()
     l0 = b.launch_count()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if clocks:
+        clocks.__enter__()
     e0.record(stream)
     b.run_async(K)
     e1.record(stream)
     torch.cuda.synchronize()
+    if clocks:
+        clocks.__exit__(None, None, None)
     if dist:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    launches = b.launch_count() - l0
-    kern = {kid: b.prof_read(kid) for kid in range(4)}
+    out["ms"] = e0.elapsed_time(e1)
+    out["launches"] = b.launch_count() - l0
+    IM, JM, KM = case.shape
+    out["rho"] = b.get_conservative().reshape(KM + 4, JM + 4, IM + 4, 5)[2:-2, 2:-2, 2:-2, 0].copy()
+    out["stats"] = b.sensor_stats() if precision == PREC_HYBRID else None
+    b.prof_enable(True)
+    b.prof_reset()
+    b.run(K)
+    out["kern"] = {kid: b.prof_read(kid) for kid in range(5)}
     b.prof_enable(False)
-    return ms, b, kern, launches
-
-
-def graph_pass(b, K, torch):
-    """The same steps replayed from the CUDA graph (no per-kernel events)."""
-    stream = b.torch_stream
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    b.run_async(K)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    return e0.elapsed_time(e1)
+    b.close()
+    return out
 
 
 def e2e_pass(case, K, torch):
-    """Host-driven solve through the C ABI with host buffers (pinned)."""
-    from cbns3d_cuda_b200 import CBNS_Q, PREC_SPLIT, _abi
-    b = init_block(case, PREC_SPLIT)
+    """Host-driven solve of the hybrid through the C ABI with host buffers (pinned)."""
+    from cbns3d_cuda_b200 import CBNS_Q, PREC_HYBRID, _abi
+    b = init_block(case, PREC_HYBRID)
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
     n = case.Q0.size
@@ -251,29 +268,33 @@ def run_ours(a):
         dist = dist_mod
     else:
         torch.cuda.set_device(0)
-    from cbns3d_cuda_b200 import PREC_FP64, PREC_SPLIT
+    from cbns3d_cuda_b200 import PREC_FP64, PREC_HYBRID, PREC_SPLIT
+    load_sensor(a.sensor)
     size = tuple(int(v) for v in a.size.split("x")) if a.size else None
     case, wl = make_case(a.case, size)
     K, W = a.steps, a.warmup
     N = n_updates(case)
-
-    # plain FP64 path
-    ms64, b64, kern64, _ = device_pass(case, PREC_FP64, K, W, torch, dist)
-    q64 = b64.get_conservative()
-    # split-precision path (headline), clocks sampled during its timed region
-    with Clocks(local) as clk:
-        ms32, b32, kern32, launches = device_pass(case, PREC_SPLIT, K, W, torch, dist)
-    clocks = clk.summary()
-    q32 = b32.get_conservative()
-    variant32 = b32.variant
     IM, JM, KM = case.shape
-    r64 = q64.reshape(KM + 4, JM + 4, IM + 4, 5)[2:-2, 2:-2, 2:-2, 0]
-    r32 = q32.reshape(KM + 4, JM + 4, IM + 4, 5)[2:-2, 2:-2, 2:-2, 0]
-    rho_l2 = float(np.sqrt(np.mean((r32 - r64) ** 2) / np.mean(r64 ** 2)))
-    rho_linf = float(np.max(np.abs(r32 - r64)) / np.max(np.abs(r64)))
-    gms32 = graph_pass(b32, K, torch)
-    b64.close()
-    b32.close()
+
+    # plain FP64 path, the split path without the sensor, then the
+    # learned-sensor hybrid (headline) with clocks sampled during its timed region
+    p64 = device_pass(case, PREC_FP64, K, W, torch, dist)
+    p32 = device_pass(case, PREC_SPLIT, K, W, torch, dist)
+    clk = Clocks(local)
+    ph = device_pass(case, PREC_HYBRID, K, W, torch, dist, clocks=clk)
+    clocks = clk.summary()
+    r64, r32, rh = p64["rho"], p32["rho"], ph["rho"]
+    ms64, ms32, msh = p64["ms"], p32["ms"], ph["ms"]
+    kern64, kern32, kernh = p64["kern"], p32["kern"], ph["kern"]
+    stats, launches = ph["stats"], ph["launches"]
+    variant32, varianth = p32["variant"], ph["variant"]
+
+    def err(r):
+        return (float(np.sqrt(np.mean((r - r64) ** 2) / np.mean(r64 ** 2))),
+                float(np.max(np.abs(r - r64)) / np.max(np.abs(r64))))
+
+    l2_32, linf_32 = err(r32)
+    l2_h, linf_h = err(rh)
 
     def reduce_max(x):
         if not dist:
@@ -282,8 +303,9 @@ def run_ours(a):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    ms32, ms64, gms32 = reduce_max(ms32), reduce_max(ms64), reduce_max(gms32)
-    value = world * N * K / (ms32 / 1e3)
+    ms32, ms64, msh = reduce_max(ms32), reduce_max(ms64), reduce_max(msh)
+    value = world * N * K / (msh / 1e3)
+    value32 = world * N * K / (ms32 / 1e3)
     value64 = world * N * K / (ms64 / 1e3)
 
     e2e = None
@@ -293,39 +315,55 @@ def run_ours(a):
         e2e = {"value": world * N * K / (ems / 1e3), "unit": "cell-updates/s", **eb}
 
     peak, peak_kind = measured_peaks()
-    st_ms, st_n = kern32[0]
+    # the per-kernel events come from a second run of K steps (same work per step)
+    st_ms, st_n = kernh[0]
     alg_per_launch = ALG_BYTES_PER_UPDATE / 3.0 * N
     achieved = alg_per_launch / (st_ms / st_n / 1e3) / 1e9 if st_n else None
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         t = json.loads(tf.read_text())
-        if "stage_bytes_per_update" in t:
-            traffic = t["stage_bytes_per_update"] / 3.0 * N
-    st64_ms, st64_n = kern64[0]
+        if "hybrid_stage_bytes_per_update" in t:
+            traffic = t["hybrid_stage_bytes_per_update"] / 3.0 * N
+
+    def kern_ms(k):
+        return {name: {"ms_per_step": k[i][0] / K, "launches_per_step": k[i][1] / K}
+                for i, name in enumerate(["stage", "bc", "viscous", "dt", "sensor+audit"]) if k[i][1]}
+
+    weno_frac = stats["weno_faces"] / (K * stats["faces_per_step"]) if stats["faces_per_step"] else None
     if rank == 0:
         cpu = None if a.no_cpu_baseline else cpu_baseline(case)
         line = {
             "metric": "cell-updates/s: learned-hybrid FP32 vs plain FP64 WENO5, same B200, rho-L2<=1e-5",
             "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": K, "warmup": W,
-            "ms_per_step": ms32 / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": msh / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 flux / f64 state", "data": "synthetic",
-            "config": {"workload": wl, "path": "split precision (FP32 WENO5-char/LF flux, FP64 state, metrics, dt)",
+            "config": {"workload": wl,
+                       "path": "learned-sensor hybrid: per face WENO5-char or linear upwind-5 flux (FP32), "
+                               "FP64 state, metrics, dt; sensor MLP on tcgen05 (BF16) every step, audit on a "
+                               "rotating 1/97 sample of the linear faces",
                        "grid": list(case.shape), "cell_updates_per_step": N, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (3 state buffers + 10 metric arrays)",
-                       "learned_sensor": "not built: value is the split path without the sensor"},
-            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "stage_kernel_ms": st64_ms / max(st64_n, 1)},
-                      "split": {"value": value, "ms_per_step": ms32 / K, "rho_l2_vs_fp64": rho_l2,
-                                "rho_linf_vs_fp64": rho_linf, "graph_replay_value": world * N * K / (gms32 / 1e3),
-                                "stage_variant": variant32},
-                      "split_over_fp64": value / value64},
+                       "sensor": {"weights": os.path.relpath(a.sensor, ROOT), "tau": SENSOR[1]}},
+            "rho_l2_vs_fp64": l2_h, "rho_linf_vs_fp64": linf_h,
+            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "kernels": kern_ms(kern64)},
+                      "split": {"value": value32, "ms_per_step": ms32 / K, "rho_l2_vs_fp64": l2_32,
+                                "rho_linf_vs_fp64": linf_32, "stage_variant": variant32,
+                                "kernels": kern_ms(kern32)},
+                      "hybrid": {"value": value, "ms_per_step": msh / K, "rho_l2_vs_fp64": l2_h,
+                                 "rho_linf_vs_fp64": linf_h, "weno_face_fraction": weno_frac,
+                                 "audit_rejected_steps": stats["audit_fail_steps"],
+                                 "audit_faces": stats["audit_faces"], "audit_max_rel_diff": stats["audit_max"],
+                                 "sensor_timeouts": stats["sensor_fail"], "stage_variant": varianth,
+                                 "kernels": kern_ms(kernh)},
+                      "hybrid_over_fp64": value / value64, "hybrid_over_split": value / value32},
             "e2e": e2e,
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "kernel": "stage_kernel (fused WENO5-char/LF sweeps + RK3 update)",
+                         "kernel": "stage_kernel, hybrid (fused WENO5-char or linear/LF sweeps + RK3 update)",
                          "alg_bytes_per_launch": alg_per_launch, "peak_kind": peak_kind,
-                         "note": "FP64 and FP32 pipe bound, not HBM bound: ~13 kFLOP per cell-update"},
+                         "note": "FP32 pipe and latency bound, not HBM bound"},
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

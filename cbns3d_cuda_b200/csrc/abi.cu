@@ -338,6 +338,12 @@ int check_ready(cbns_ctx* c) {
     g_last = "metrics have not been computed (cbns_calc_metrics)";
     return CBNS_ERR_STATE;
   }
+  return CBNS_OK;
+}
+
+// check_ready plus, for the flux evaluations of a hybrid context, the sensor.
+int check_flux_ready(cbns_ctx* c) {
+  RET(check_ready(c));
   if (hybrid(c) && !c->sensor_loaded) {
     g_last = "the hybrid flux needs the sensor network (cbns_sensor_load)";
     return CBNS_ERR_STATE;
@@ -609,7 +615,7 @@ int cbns_set_bc_calc_primitive(cbns_ctx* c, int which) {
 }
 
 int cbns_calc_numerical_flux(cbns_ctx* c, int which) {
-  RET(check_ready(c));
+  RET(check_flux_ready(c));
   if (which != CBNS_Q && which != CBNS_QP) return CBNS_ERR_ARG;
   // the fluxes are formed inside the stage kernel launched by cbns_update_rk3
   c->pending_src = which;
@@ -630,7 +636,7 @@ int cbns_calc_viscous_terms(cbns_ctx* c) {
 }
 
 int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
-  RET(check_ready(c));
+  RET(check_flux_ready(c));
   if (stage < 1 || stage > 3) return CBNS_ERR_ARG;
   const int src_l = c->pending_src >= 0 ? c->pending_src : (stage == 1 ? CBNS_Q : CBNS_QP);
   c->pending_src = -1;
@@ -690,7 +696,7 @@ int cbns_get_time(cbns_ctx* c, double* t_cur, double* dt_last) {
 }
 
 static int run_impl(cbns_ctx* c, unsigned nsteps, double t_end, bool wait, unsigned* steps_done) {
-  RET(check_ready(c));
+  RET(check_flux_ready(c));
   {
     StepState h;
     CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -754,7 +760,7 @@ int cbns_run(cbns_ctx* c, unsigned nsteps, double t_end, unsigned* steps_done) {
 int cbns_run_async(cbns_ctx* c, unsigned nsteps, double t_end) { return run_impl(c, nsteps, t_end, false, nullptr); }
 
 int cbns_eval_rhs(cbns_ctx* c, int which, double* rhs) {
-  RET(check_ready(c));
+  RET(check_flux_ready(c));
   if (!rhs || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
   if (hybrid(c)) {
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
@@ -883,10 +889,15 @@ int cbns_sensor_stats_reset(cbns_ctx* c) {
 }
 
 int cbns_autotune(cbns_ctx* c, int* chosen) {
-  RET(check_ready(c));
+  RET(check_flux_ready(c));
   const bool fp32 = c->ph.precision != CBNS_PREC_FP64;
   const int nv = stage_variants(fp32);
-  // time every variant on the current state (RHS-only mode: nothing is updated)
+  // time every variant on the current state (RHS-only mode: nothing is updated);
+  // the hybrid kernel is timed on the sensor's decisions for this state
+  if (hybrid(c)) {
+    CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
+    RET(sensor_launch(c, c->qb[c->lq], false));
+  }
   const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));

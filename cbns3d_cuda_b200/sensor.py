@@ -78,8 +78,9 @@ def predict(params, X, tensor_cores=False):
     return out
 
 
-def train(X, Y, epochs=3, batch=16384, lr=3e-3, pos_weight=None, seed=0, params=None, log=None):
-    """Adam on the weighted cross-entropy; returns (params tensor, loss history)."""
+def train(X, Y, epochs=3, batch=16384, lr=3e-3, pos_weight=None, seed=0, params=None, log=None, cosine=False):
+    """Adam on the weighted cross-entropy; returns (params tensor, loss history).
+    cosine: decay the learning rate to 0 over the run (half a cosine)."""
     import torch
     lib = _abi.load()
     n = X.shape[0]
@@ -95,6 +96,7 @@ def train(X, Y, epochs=3, batch=16384, lr=3e-3, pos_weight=None, seed=0, params=
     gen.manual_seed(seed)
     step = 0
     hist = []
+    total = epochs * ((n + batch - 1) // batch)
     for ep in range(epochs):
         perm = torch.randperm(n, device="cuda", generator=gen)
         tot = 0.0
@@ -105,8 +107,10 @@ def train(X, Y, epochs=3, batch=16384, lr=3e-3, pos_weight=None, seed=0, params=
             yb = Y[idx].contiguous()
             _abi.check(lib.cbns_mlp_grad(_ptr(P), _ptr(xb), _ptr(yb), xb.shape[0], float(pos_weight), _ptr(G),
                                          _ptr(L), None), "cbns_mlp_grad")
+            lr_now = lr * 0.5 * (1.0 + np.cos(np.pi * step / total)) if cosine else lr
             step += 1
-            _abi.check(lib.cbns_mlp_adam(_ptr(P), _ptr(G), _ptr(M), _ptr(V), step, float(lr), None), "cbns_mlp_adam")
+            _abi.check(lib.cbns_mlp_adam(_ptr(P), _ptr(G), _ptr(M), _ptr(V), step, float(lr_now), None),
+                       "cbns_mlp_adam")
             if nb % 16 == 0:
                 tot += float(L.item())
             nb += 1

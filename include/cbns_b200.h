@@ -166,7 +166,7 @@ int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM, const doub
  * CBNS_SENSOR_NPARAM values: W1[32][15] b1[32] W2[32][32] b2[32] w3[32] b3.
  * Features of a face: the jumps of density, pressure and normal velocity
  * across its 5-point stencil, divided by the face's mean density, pressure and
- * sound speed.  Label: 1 when the WENO5 nonlinear weights of the face's
+ * sound speed, each compressed as asinh(f / 0.01) / asinh(100).  Label: 1 when the WENO5 nonlinear weights of the face's
  * characteristic reconstruction depart from the linear weights by more than
  * 0.05.  Pointers marked _dev are device pointers; stream is a cudaStream_t. */
 #define CBNS_SENSOR_NIN    15

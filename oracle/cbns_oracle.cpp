@@ -835,10 +835,12 @@ void orc_set_face_mask(void* h, const unsigned char* mask, long n) {
 // Sensor features and WENO-weight deviation of every grid face, in the order
 // i-faces, j-faces, k-faces (each i fastest), for the learned shock sensor
 // (no counterpart in the reference).  Restates the definitions of the
-// library's sensor.cuh in FP64: 15 normalised jumps of density, pressure and
+// library's sensor.cuh in FP64: 15 normalised (then asinh-compressed) jumps of density, pressure and
 // normal velocity; deviation = max |w_k - d_k| of the characteristic WENO5
 // weights (basis and Roe average of the flux) on both sides of all 5 fields.
 void orc_sensor_faces(void* h, int which, float* feat, float* dev) {
+  // each jump compressed as asinh(f / 0.01) / asinh(100)
+  auto compress = [](double f) { return std::asinh(f / 0.01) / std::asinh(100.0); };
   auto* o = static_cast<Oracle*>(h);
   const auto& Q = o->buf(which);
   const long IM = o->IM, JM = o->JM, KM = o->KM;
@@ -865,9 +867,9 @@ void orc_sensor_faces(void* h, int which, float* feat, float* dev) {
     }
     const double rb = 0.5 * (r[2] + r[3]), pb = 0.5 * (pr[2] + pr[3]), cb = std::sqrt(gamma * pb / rb);
     for (int m = 0; m < 5; ++m) {
-      feat[15 * e + m] = (float)((r[m + 1] - r[m]) / rb);
-      feat[15 * e + 5 + m] = (float)((pr[m + 1] - pr[m]) / pb);
-      feat[15 * e + 10 + m] = (float)((un[m + 1] - un[m]) / cb);
+      feat[15 * e + m] = (float)compress((r[m + 1] - r[m]) / rb);
+      feat[15 * e + 5 + m] = (float)compress((pr[m + 1] - pr[m]) / pb);
+      feat[15 * e + 10 + m] = (float)compress((un[m + 1] - un[m]) / cb);
     }
     const Prim a = to_prim(&Q[5 * ta], gam1), b = to_prim(&Q[5 * tb], gam1);
     double R[5][5], L[5][5];

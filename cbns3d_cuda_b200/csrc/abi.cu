@@ -37,7 +37,7 @@ namespace cbns {
 void stage_prepare();
 }
 
-enum { PK_STAGE = 0, PK_BC = 1, PK_VISC = 2, PK_STEP = 3, PK_SENSOR = 4, PK_N = 5 };
+enum { PK_STAGE = 0, PK_BC = 1, PK_VISC = 2, PK_STEP = 3, PK_SENSOR = 4, PK_AUDIT = 5, PK_N = 6 };
 
 struct cbns_ctx {
   cbns_params prm;
@@ -61,7 +61,8 @@ struct cbns_ctx {
   int stage_variant = 0;  // compiled occupancy variant of the stage kernel (cbns_autotune)
   // hybrid flux: the learned sensor's parameters and per-face decisions
   float* sensor_params = nullptr;  // device, CBNS_SENSOR_NPARAM floats
-  unsigned char* mask = nullptr;   // device, one byte per face
+  unsigned char* mask = nullptr;   // device, one byte per face: the decisions the fluxes use
+  unsigned char* mask_raw = nullptr;  // device: the network's decisions before widening
   long nfaces = 0;
   float sensor_tau = 0.5f;
   unsigned audit_stride = 97;
@@ -275,7 +276,6 @@ void drop_graph(cbns_ctx* c) {
 // face (tensor cores), then the audit of a rotating sample of its linear-flux
 // faces against WENO5 (which forces WENO5 for the step on a violation).
 int sensor_launch(cbns_ctx* c, const double* q, bool check_done) {
-  Prof p(c, PK_SENSOR);
   MaskArgs m;
   m.d = c->d;
   m.gamma = (float)c->ph.gamma;
@@ -284,10 +284,26 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done) {
   for (int k = 0; k < 10; ++k) m.area[k] = c->f.area[k];
   m.params = c->sensor_params;
   m.tau = c->sensor_tau;
-  m.mask = c->mask;
+  m.mask = c->mask_raw;
   m.st = c->st;
   m.check_done = check_done;
-  CK(launch_sensor_mask(m, c->stream));
+  {
+    Prof p(c, PK_SENSOR);
+    CK(launch_sensor_mask(m, c->stream));
+    // widening in i, j, k: raw -> mask -> raw -> mask
+    unsigned char* bufs[4] = {c->mask_raw, c->mask, c->mask_raw, c->mask};
+    for (int dim = 0; dim < 3; ++dim) {
+      DilateArgs w;
+      w.d = c->d;
+      w.in = bufs[dim];
+      w.out = bufs[dim + 1];
+      w.dim = dim;
+      w.st = c->st;
+      w.count = dim == 2;
+      w.check_done = check_done;
+      CK(launch_sensor_dilate(w, c->stream));
+    }
+  }
   AuditArgs a;
   a.d = c->d;
   a.gamma = (float)c->ph.gamma;
@@ -300,8 +316,11 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done) {
   a.bound = c->audit_bound;
   a.st = c->st;
   a.check_done = check_done;
-  CK(launch_sensor_audit(a, c->stream));
-  c->launches += 2;
+  {
+    Prof p(c, PK_AUDIT);
+    CK(launch_sensor_audit(a, c->stream));
+  }
+  c->launches += 6;  // two sensor sweeps, three widening passes and the audit
   return CBNS_OK;
 }
 
@@ -427,10 +446,16 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   if (rc == CBNS_OK) rc = dalloc(c, &c->staging, c->staging_elems);
   c->nfaces = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2) + (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2) +
               (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 1);
+  if (rc == CBNS_OK && p->precision == CBNS_PREC_HYBRID && c->nfaces >= (1L << 31)) {
+    g_last = "the hybrid flux indexes faces with 32-bit integers: grid too large";
+    rc = CBNS_ERR_TOO_LARGE;
+  }
   if (rc == CBNS_OK && p->precision == CBNS_PREC_HYBRID) {
     double* tmp = nullptr;
     rc = dalloc(c, &tmp, (size_t)(c->nfaces + 7) / 8);
     c->mask = reinterpret_cast<unsigned char*>(tmp);
+    if (rc == CBNS_OK) rc = dalloc(c, &tmp, (size_t)(c->nfaces + 7) / 8);
+    c->mask_raw = reinterpret_cast<unsigned char*>(tmp);
     if (rc == CBNS_OK) {
       rc = dalloc(c, &tmp, (CBNS_SENSOR_NPARAM + 1) / 2);
       c->sensor_params = reinterpret_cast<float*>(tmp);

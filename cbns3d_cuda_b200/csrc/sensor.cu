@@ -42,13 +42,16 @@ __global__ void sample_faces_kernel(const SampleArgs a) {
   const double* q = a.q;
   const long V = d.VOL;
   auto ld = [&](int p, int n) -> float { return (float)q[n * V + oa + (p - 2) * sd]; };
-  const float nx = (float)(0.5 * (a.area[3 * dir][oa] + a.area[3 * dir][ob]));
-  const float ny = (float)(0.5 * (a.area[3 * dir + 1][oa] + a.area[3 * dir + 1][ob]));
-  const float nz = (float)(0.5 * (a.area[3 * dir + 2][oa] + a.area[3 * dir + 2][ob]));
-  const float in = rsqrtf(nx * nx + ny * ny + nz * nz);
+  // the same FP32 arithmetic as the per-step sensor sweep, so that inference
+  // sees exactly the features the network was trained on
+  const float A[3] = {(float)a.area[3 * dir][oa], (float)a.area[3 * dir + 1][oa], (float)a.area[3 * dir + 2][oa]};
+  const float B[3] = {(float)a.area[3 * dir][ob], (float)a.area[3 * dir + 1][ob], (float)a.area[3 * dir + 2][ob]};
+  float ux, uy, uz;
+  face_unit_normal(A, B, ux, uy, uz);
   float f[SN_IN];
-  face_features(ld, nx * in, ny * in, nz * in, a.gamma, a.gam1, f);
-  const float dev = face_weno_deviation(ld, nx, ny, nz, a.gamma, a.gam1);
+  face_features(ld, ux, uy, uz, a.gamma, a.gam1, f);
+  const float dev = face_weno_deviation(ld, 0.5f * (A[0] + B[0]), 0.5f * (A[1] + B[1]), 0.5f * (A[2] + B[2]),
+                                        a.gamma, a.gam1);
   const unsigned slot = atomicAdd(a.count, 1u);
   if (slot >= a.capacity) return;
 #pragma unroll
@@ -200,13 +203,61 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float* __restrict__ 
   }
 }
 
+// ---------------------------------------------------------------- widening
+// Grid: x over the faces of a line along i, y over groups of DL lines along
+// j, z over (direction, k); no index division per face.
+constexpr int DL = 16;
+__global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) {
+  if (a.check_done && a.st->done) return;
+  const Dims& d = a.d;
+  const int IM = d.IM, JM = d.JM, KM = d.KM;
+  const int dir = blockIdx.z / (KM - 1), x2 = blockIdx.z % (KM - 1);
+  const int x0 = blockIdx.x * blockDim.x + threadIdx.x;
+  // extents (n0, n1, n2) and first index of this direction's faces
+  const int n0 = dir == 0 ? IM - 1 : IM - 2, n1 = dir == 1 ? JM - 1 : JM - 2, n2 = dir == 2 ? KM - 1 : KM - 2;
+  const int first = dir == 0 ? 0 : (dir == 1 ? (IM - 1) * (JM - 2) * (KM - 2)
+                                             : (IM - 1) * (JM - 2) * (KM - 2) + (IM - 2) * (JM - 1) * (KM - 2));
+  if (x2 >= n2) return;  // uniform per CTA
+  const bool valid = x0 < n0;
+  const int w = a.dim == dir ? SN_DILATE_ALONG : SN_DILATE_ACROSS;
+  const int len = a.dim == 0 ? n0 : (a.dim == 1 ? n1 : n2);
+  const int stride = a.dim == 0 ? 1 : (a.dim == 1 ? n0 : n0 * n1);
+  unsigned cnt = 0;
+  const unsigned char* __restrict__ in = a.in;
+  unsigned char* __restrict__ out = a.out;
+  const int y0 = blockIdx.y * DL, y1 = min(n1, y0 + DL);
+  if (valid) {
+    // all lines' loads are independent: let them be in flight together
+#pragma unroll 4
+    for (int x1 = y0; x1 < y1; ++x1) {
+      const int e = first + x0 + n0 * (x1 + n1 * x2);
+      const int pos = a.dim == 0 ? x0 : (a.dim == 1 ? x1 : x2);
+      unsigned char dec = 0;
+#pragma unroll
+      for (int o = -2; o <= 2; ++o) {
+        const int p = pos + o;
+        if (o >= -w && o <= w && p >= 0 && p < len) dec |= __ldg(in + e + o * stride);
+      }
+      out[e] = dec;
+      cnt += dec;
+    }
+  }
+  if (a.count) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&a.st->weno_faces, (unsigned long long)cnt);
+  }
+}
+
 // ---------------------------------------------------------------- audit
 __global__ void __launch_bounds__(128) sensor_audit_kernel(const AuditArgs a) {
   if (a.check_done && a.st->done) return;
   const Dims& d = a.d;
   const long nf = total_faces(d);
+  // runs of 128 consecutive faces (coalesced loads): run r is audited when
+  // r % stride == steps % stride
   const unsigned off = a.st->steps % a.stride;
-  const long e = (blockIdx.x * (long)blockDim.x + threadIdx.x) * a.stride + off;
+  const long e = ((long)blockIdx.x * a.stride + off) * 128 + threadIdx.x;
   float err = 0.f;
   bool audited = false;
   int dir, i, j, k;
@@ -280,8 +331,15 @@ cudaError_t launch_sample_faces(const SampleArgs& a, cudaStream_t s) {
 cudaError_t launch_sensor_audit(const AuditArgs& a, cudaStream_t s) {
   const long nf = (long)(a.d.IM - 1) * (a.d.JM - 2) * (a.d.KM - 2) + (long)(a.d.IM - 2) * (a.d.JM - 1) * (a.d.KM - 2) +
                   (long)(a.d.IM - 2) * (a.d.JM - 2) * (a.d.KM - 1);
-  const long n = (nf + a.stride - 1) / a.stride;
-  sensor_audit_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a);
+  const long runs = (nf + 127) / 128;
+  sensor_audit_kernel<<<(unsigned)((runs + a.stride - 1) / a.stride), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sensor_dilate(const DilateArgs& a, cudaStream_t s) {
+  const dim3 grid((unsigned)((a.d.IM - 1 + 127) / 128), (unsigned)((a.d.JM - 1 + DL - 1) / DL),
+                  (unsigned)(3 * (a.d.KM - 1)));
+  sensor_dilate_kernel<<<grid, 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -9,10 +9,16 @@
 //   f[10 + m] = (un_{m+1}  - un_m)  / c_bar          un = velocity . unit normal
 // with rho_bar, p_bar the means over a and b and c_bar = sqrt(gamma p_bar / rho_bar):
 // normalised density, pressure and normal-velocity jumps of the 5-point stencil,
-// each then compressed as asinh(f / s) / asinh(1 / s) with s = SN_FEAT_SCALE:
-// linear below s, logarithmic above, 1 at f = 1.  The jumps that matter span
-// 1e-4 .. 1; on that range the compression lets a 32-unit ReLU network
+// each then compressed as sign(f) log2(1 + |f| / s) with s = SN_FEAT_SCALE:
+// linear below s, logarithmic above (6.66 at |f| = 1).  The jumps that matter
+// span 1e-4 .. 1; on that range the compression lets a 32-unit ReLU network
 // separate the faces far better than the raw jumps do.
+//
+// Flat stencils.  A face whose compressed features sum (in absolute value) to
+// less than SN_FLAT (every jump below ~3e-5) takes the linear flux without
+// the network: its density, pressure and normal velocity are constant to
+// within FP32 noise of the state, where the trained network decides linear
+// as well.
 //
 // Label.  The characteristic WENO5 of the face (same basis as the flux) gives
 // nonlinear weights w_k on both sides for the 5 fields; the deviation is
@@ -34,9 +40,85 @@ constexpr int SN_IN = 15, SN_H = 32;
 constexpr int SP_W1 = 0, SP_B1 = 480, SP_W2 = 512, SP_B2 = 1536, SP_W3 = 1568, SP_B3 = 1600, SP_N = 1601;
 constexpr float SN_DEV_THRESHOLD = 0.05f;
 constexpr float SN_FEAT_SCALE = 0.01f;
-constexpr float SN_FEAT_NORM = 0.18873828f;  // 1 / asinh(1 / SN_FEAT_SCALE) = 1 / asinh(100)
+constexpr float SN_FLAT = 0.0045f;  // sum of |features| below which a stencil is flat
 
-__device__ __forceinline__ float feat_compress(float x) { return asinhf(x * (1.0f / SN_FEAT_SCALE)) * SN_FEAT_NORM; }
+// log2 on the special-function unit; the arguments here are >= 1
+__device__ __forceinline__ float lg2_approx(float v) {
+  float r;
+  asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+
+// Compressed feature of a raw difference dlt whose normalised jump is dlt * n,
+// with g = n / SN_FEAT_SCALE: sign(dlt) log2(1 + |dlt| g).
+__device__ __forceinline__ float feat_of(float dlt, float g) {
+  return copysignf(lg2_approx(__fmaf_rn(fabsf(dlt), g, 1.0f)), dlt);
+}
+
+// Primitives of one node from its conservative state, as the features use them.
+struct NodePrim {
+  float r, p, u, v, w;
+};
+
+// The feature arithmetic is written with explicit round-to-nearest operations
+// (no contraction left to the compiler), so that the per-step sensor and the
+// training sampler, which reach a face's stencil in different ways, compute
+// bit-identical features.
+__device__ __forceinline__ NodePrim node_prim(float q0, float q1, float q2, float q3, float q4, float gam1) {
+  NodePrim s;
+  const float ir = __frcp_rn(q0);
+  s.r = q0;
+  s.u = __fmul_rn(q1, ir);
+  s.v = __fmul_rn(q2, ir);
+  s.w = __fmul_rn(q3, ir);
+  const float k = __fmaf_rn(s.w, s.w, __fmaf_rn(s.v, s.v, __fmul_rn(s.u, s.u)));
+  s.p = __fmul_rn(gam1, __fsub_rn(q4, __fmul_rn(__fmul_rn(0.5f, q0), k)));
+  return s;
+}
+
+// Unit face normal from the area vectors of the face's two nodes (FP32 copies).
+__device__ __forceinline__ void face_unit_normal(const float a[3], const float b[3], float& x, float& y, float& z) {
+  x = __fmul_rn(0.5f, __fadd_rn(a[0], b[0]));
+  y = __fmul_rn(0.5f, __fadd_rn(a[1], b[1]));
+  z = __fmul_rn(0.5f, __fadd_rn(a[2], b[2]));
+  const float in = rsqrtf(__fmaf_rn(z, z, __fmaf_rn(y, y, __fmul_rn(x, x))));
+  x = __fmul_rn(x, in);
+  y = __fmul_rn(y, in);
+  z = __fmul_rn(z, in);
+}
+
+// The 15 features of a face from the primitives of its 6 stencil nodes
+// (P(q) returns the NodePrim of point q) and the unit face normal.
+template <typename PF>
+__device__ __forceinline__ void features_of(const PF& P, float ux, float uy, float uz, float gamma, float f[SN_IN]) {
+  float r[6], p[6], un[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    const NodePrim s = P(q);
+    r[q] = s.r;
+    p[q] = s.p;
+    un[q] = __fmaf_rn(s.w, uz, __fmaf_rn(s.v, uy, __fmul_rn(s.u, ux)));
+  }
+  const float rb = __fmul_rn(0.5f, __fadd_rn(r[2], r[3])), pb = __fmul_rn(0.5f, __fadd_rn(p[2], p[3]));
+  const float irb = __frcp_rn(rb), ipb = __frcp_rn(pb);
+  const float icb = rsqrtf(__fmul_rn(__fmul_rn(gamma, pb), irb));
+  const float gr = __fmul_rn(irb, 1.0f / SN_FEAT_SCALE), gp = __fmul_rn(ipb, 1.0f / SN_FEAT_SCALE);
+  const float gu = __fmul_rn(icb, 1.0f / SN_FEAT_SCALE);
+#pragma unroll
+  for (int m = 0; m < 5; ++m) {
+    f[m] = feat_of(__fsub_rn(r[m + 1], r[m]), gr);
+    f[5 + m] = feat_of(__fsub_rn(p[m + 1], p[m]), gp);
+    f[10 + m] = feat_of(__fsub_rn(un[m + 1], un[m]), gu);
+  }
+}
+
+// Sum of |features| (NaN if any feature is NaN): the flat-stencil test
+__device__ __forceinline__ float feature_l1(const float f[SN_IN]) {
+  float a = 0.f;
+#pragma unroll
+  for (int m = 0; m < SN_IN; ++m) a = __fadd_rn(a, fabsf(f[m]));
+  return a;
+}
 
 // Global face index e -> direction and the low node (i, j, k) of the face:
 // i-faces, then j-faces, then k-faces, each in the order of the reference's
@@ -73,27 +155,13 @@ __device__ __forceinline__ long total_faces(const Dims& d) {
          (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 1);
 }
 
+// Features of a face from a stencil loader: ld(p, n) = conservative variable n
+// at stencil point p.
 template <typename LD>
 __device__ __forceinline__ void face_features(const LD& ld, float ux, float uy, float uz, float gamma, float gam1,
                                               float f[SN_IN]) {
-  float r[6], p[6], un[6];
-#pragma unroll
-  for (int q = 0; q < 6; ++q) {
-    const float rr = ld(q, 0), ir = 1.0f / rr;
-    const float u = ld(q, 1) * ir, v = ld(q, 2) * ir, w = ld(q, 3) * ir;
-    r[q] = rr;
-    p[q] = gam1 * (ld(q, 4) - 0.5f * rr * (u * u + v * v + w * w));
-    un[q] = u * ux + v * uy + w * uz;
-  }
-  const float rb = 0.5f * (r[2] + r[3]), pb = 0.5f * (p[2] + p[3]);
-  const float cb = sqrtf(gamma * pb / rb);
-  const float irb = 1.0f / rb, ipb = 1.0f / pb, icb = 1.0f / cb;
-#pragma unroll
-  for (int m = 0; m < 5; ++m) {
-    f[m] = feat_compress((r[m + 1] - r[m]) * irb);
-    f[5 + m] = feat_compress((p[m + 1] - p[m]) * ipb);
-    f[10 + m] = feat_compress((un[m + 1] - un[m]) * icb);
-  }
+  auto P = [&](int q) { return node_prim(ld(q, 0), ld(q, 1), ld(q, 2), ld(q, 3), ld(q, 4), gam1); };
+  features_of(P, ux, uy, uz, gamma, f);
 }
 
 // max |w_k - d_k| of the WENO5-JS weights of one scalar stencil a..e

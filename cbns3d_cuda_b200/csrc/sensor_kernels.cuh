@@ -34,9 +34,30 @@ struct MaskArgs {
   int check_done;
 };
 
-// Audit of the decisions: on the faces with e % stride == steps % stride that
-// the sensor sent to the linear flux, recompute the WENO5 flux; a relative
-// difference above bound sets st->force_weno for the step.
+// Widening of the decisions: a face takes WENO5 when the sensor chose WENO5
+// for a face of the same direction within SN_DILATE_ALONG faces along its own
+// grid line or SN_DILATE_ACROSS faces in the two other index directions.  A
+// discontinuity moves less than a cell per time step (CFL <= 1): along a line
+// it reaches at most one more node of the 6-node stencils near it, and a
+// curved front (a blast) reaches grid lines next to those it crossed at the
+// step's start, so those faces stay on WENO5 for the step's three stages.
+// Three separable passes (one per index direction); the last one counts the
+// WENO5 faces.
+constexpr int SN_DILATE_ALONG = 2, SN_DILATE_ACROSS = 1;
+struct DilateArgs {
+  Dims d;
+  const unsigned char* in;
+  unsigned char* out;
+  int dim;                 // index direction of this pass: 0 = i, 1 = j, 2 = k
+  StepState* st;           // WENO5 faces are counted when count != 0
+  int count;
+  int check_done;
+};
+
+// Audit of the decisions: on the runs of 128 consecutive faces with
+// (e / 128) % stride == steps % stride, the faces the sensor sent to the linear
+// flux are recomputed with WENO5; a relative difference above bound sets
+// st->force_weno for the step.
 struct AuditArgs {
   Dims d;
   float gamma, gam1, gam1_inv;
@@ -52,6 +73,7 @@ struct AuditArgs {
 cudaError_t launch_sample_faces(const SampleArgs& a, cudaStream_t s);
 cudaError_t launch_sensor_mask(const MaskArgs& a, cudaStream_t s);
 cudaError_t launch_sensor_audit(const AuditArgs& a, cudaStream_t s);
+cudaError_t launch_sensor_dilate(const DilateArgs& a, cudaStream_t s);
 cudaError_t launch_mlp_grad(const float* P, const float* X, const unsigned char* Y, unsigned n, float pos_w, float* G,
                             float* loss, cudaStream_t s);
 cudaError_t launch_adam(float* P, const float* G, float* M, float* V, unsigned step, float lr, cudaStream_t s);

@@ -43,63 +43,280 @@ __global__ void __launch_bounds__(128) mlp_predict_tc_kernel(const float* __rest
   }
 }
 
-// One 128-face tile per round: each thread forms the features of one face from
-// global memory, the tile goes through the network on the tensor cores, and the
-// thread writes its face's decision.
-__global__ void __launch_bounds__(128) sensor_mask_kernel(const MaskArgs a) {
+// Per-step decisions of the hybrid flux, in directional sweeps.  A work item
+// is up to SW_CH tiles of 128 faces:
+//   i-faces: 128 consecutive faces of SW_CH grid rows (j, k); each row's node
+//            primitives (i0-2 .. i0+130) are staged in shared memory, the
+//            next row's loads in flight while the current row is classified;
+//   j-faces: a segment of 128 i-columns at one k, SW_CH consecutive faces
+//            along j; every thread keeps its column's 6-node window of
+//            primitives in registers and loads one node ahead per face;
+//   k-faces: the same along k at one j.
+// So each node's primitives are formed once per direction, and a tile's
+// loads are coalesced along i.  A tile whose faces all have flat stencils is
+// decided linear at once; any other tile goes through the network on the
+// tensor cores and each thread writes the decision byte of its face.
+constexpr int SW_T = 128;  // faces per tile = threads per CTA
+constexpr int SW_CH = 30;  // tiles per work item (a multiple of the 6-face window rotation)
+
+struct RowSmem {
+  float pr[5][SW_T + 8];  // r, p, u, v, w of nodes i0-2 .. i0+130
+  float ax[3][SW_T + 4];  // J grad(xi) of nodes i0 .. i0+128
+};
+
+// The window sweeps stream each column's nodes through a per-thread ring of
+// SW_D slots filled by asynchronous copies (cp.async), SW_D faces ahead: slot
+// u % SW_D holds the 5 state values of node f0+3+u and the area vector of
+// node f0+1+u for face f0+u.
+constexpr int SW_D = 4;
+struct WinSmem {
+  double v[SW_D][8][SW_T];
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(tc::smem_u32(smem)), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_ring() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(SW_D - 1) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+struct SweepCtx {
+  tc::Smem* s;
+  unsigned phase;
+  float zcut;
+  unsigned char* mask;
+};
+
+// Decision of the thread's face e (when valid) from its features f; false if
+// a tensor-core wait timed out.  Called by all threads of the CTA.
+__device__ __forceinline__ bool classify(SweepCtx& c, int t, const float f[SN_IN], bool valid, long e) {
+  unsigned char dec = 0;
+  const bool flat = feature_l1(f) < SN_FLAT;  // false for NaN features
+  if (!__syncthreads_and(!valid || flat)) {
+    tc::put_features(*c.s, t, f);
+    float z = 0.f;
+    if (!tc::run_tile(*c.s, t, c.phase, &z)) return false;
+    // non-finite features (e.g. a non-physical state) fall back to WENO5
+    dec = (!flat && (z >= c.zcut || !(z == z))) ? 1 : 0;
+  }
+  if (valid) c.mask[e] = dec;
+  return true;
+}
+
+// KIND 0: the i-face rows; KIND 1: the j- and k-face window sweeps (two
+// launches, so that each path gets its own register allocation).
+template <int KIND>
+__global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(const MaskArgs a) {
   if (a.check_done && a.st->done) return;
   extern __shared__ unsigned char raw[];
-  tc::Smem& s = *reinterpret_cast<tc::Smem*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
+  tc::Smem& s = *reinterpret_cast<tc::Smem*>(base);
+  RowSmem& rs = *reinterpret_cast<RowSmem*>(base + sizeof(tc::Smem));
+  WinSmem& ws = *reinterpret_cast<WinSmem*>(base + sizeof(tc::Smem));
   const int t = threadIdx.x;
   if (t < 32) tc::tmem_alloc(&s.tmem, tc::TMEM_COLS);
   if (t == 0) tc::mbar_init(&s.bar);
-  tc::load_weights(s, a.params, t, 128);
+  tc::load_weights(s, a.params, t, SW_T);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
+
   const Dims& d = a.d;
-  const long nf = total_faces(d);
-  const long ntiles = (nf + 127) / 128;
-  // p >= tau  <=>  logit >= log(tau / (1 - tau))
-  const float zcut = logf(a.tau / (1.f - a.tau));
-  unsigned phase = 0;
-  unsigned nweno = 0;
-  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long e = tile * 128 + t;
-    int dir, i, j, k;
-    float f[SN_IN];
-    if (decode_face(d, e, dir, i, j, k)) {
-      const long sd = dir == 0 ? 1 : (dir == 1 ? d.PX : d.PL);
-      const long oa = node_off(d, i, j, k), ob = oa + sd;
-      auto ld = [&](int p, int n) -> float { return (float)__ldg(a.q + n * d.VOL + oa + (p - 2) * sd); };
-      const float nx = (float)(0.5 * (__ldg(a.area[3 * dir] + oa) + __ldg(a.area[3 * dir] + ob)));
-      const float ny = (float)(0.5 * (__ldg(a.area[3 * dir + 1] + oa) + __ldg(a.area[3 * dir + 1] + ob)));
-      const float nz = (float)(0.5 * (__ldg(a.area[3 * dir + 2] + oa) + __ldg(a.area[3 * dir + 2] + ob)));
-      const float in = rsqrtf(nx * nx + ny * ny + nz * nz);
-      face_features(ld, nx * in, ny * in, nz * in, a.gamma, a.gam1, f);
-    } else {
+  const int IM = d.IM, JM = d.JM, KM = d.KM;
+  const long VOL = d.VOL;
+  const long nfi = (long)(IM - 1) * (JM - 2) * (KM - 2);
+  const long nfj = (long)(IM - 2) * (JM - 1) * (KM - 2);
+  const int nseg0 = (IM - 1 + SW_T - 1) / SW_T, nseg = (IM - 2 + SW_T - 1) / SW_T;
+  const int rows = (JM - 2) * (KM - 2);
+  const long n0 = (long)nseg0 * ((rows + SW_CH - 1) / SW_CH);
+  const long n1 = (long)nseg * (KM - 2) * ((JM - 1 + SW_CH - 1) / SW_CH);
+  const long n2 = (long)nseg * (JM - 2) * ((KM - 1 + SW_CH - 1) / SW_CH);
+  const float gamma = a.gamma, gam1 = a.gam1;
+  SweepCtx cx{&s, 0u, logf(a.tau / (1.f - a.tau)), a.mask};  // p >= tau  <=>  logit >= zcut
+  bool ok = true;
+
+  auto load_q = [&](const double* p, double q[5]) {
 #pragma unroll
-      for (int m = 0; m < SN_IN; ++m) f[m] = 0.f;
-    }
-    tc::put_features(s, t, f);
-    float z = 0.f;
-    if (!tc::run_tile(s, t, phase, &z)) {
-      if (t == 0) {  // decisions incomplete: the step takes WENO5 everywhere
-        atomicExch(&a.st->sensor_fail, 1);
-        atomicExch(&a.st->force_weno, 1);
+    for (int n = 0; n < 5; ++n) q[n] = __ldg(p + n * VOL);
+  };
+  auto prim_of = [&](const double q[5]) {
+    return node_prim((float)q[0], (float)q[1], (float)q[2], (float)q[3], (float)q[4], gam1);
+  };
+
+  const long it0 = KIND == 0 ? 0 : n0, it1 = KIND == 0 ? n0 : n0 + n1 + n2;
+  for (long item = it0 + blockIdx.x; ok && item < it1; item += gridDim.x) {
+    float f[SN_IN];
+    if (KIND == 0) {  // i-faces, row by row
+      const int seg = (int)(item % nseg0), rc = (int)(item / nseg0);
+      const int i0 = seg * SW_T;
+      const int r0 = rc * SW_CH, r1 = min(rows, (rc + 1) * SW_CH);
+      // this thread's share of a row: node x = t (and x = SW_T + t for t < 5)
+      // and the area vector of node x = t (and x = SW_T for t = 0); the next
+      // row's share is loaded while the current row goes through the network
+      double q0[5], q1[5], a0[3], a1[3];
+      auto fetch = [&](int r) {
+        const int j = 1 + r % (JM - 2), k = 1 + r / (JM - 2);
+        const int ia = i0 - 2 + t, ib = i0 - 2 + SW_T + t;
+        if (ia <= IM + 1) load_q(a.q + node_off(d, ia, j, k), q0);
+        if (t < 5 && ib <= IM + 1) load_q(a.q + node_off(d, ib, j, k), q1);
+        if (i0 + t <= IM + 1) {
+          const long o = node_off(d, i0 + t, j, k);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) a0[m] = __ldg(a.area[m] + o);
+        }
+        if (t == 0 && i0 + SW_T <= IM + 1) {
+          const long o = node_off(d, i0 + SW_T, j, k);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) a1[m] = __ldg(a.area[m] + o);
+        }
+      };
+      auto put = [&](int x, const double q[5]) {
+        const NodePrim p = prim_of(q);
+        rs.pr[0][x] = p.r;
+        rs.pr[1][x] = p.p;
+        rs.pr[2][x] = p.u;
+        rs.pr[3][x] = p.v;
+        rs.pr[4][x] = p.w;
+      };
+      fetch(r0);
+      for (int r = r0; ok && r < r1; ++r) {
+        const int j = 1 + r % (JM - 2), k = 1 + r / (JM - 2);
+        __syncthreads();  // the previous row's staging is no longer read
+        if (i0 - 2 + t <= IM + 1) put(t, q0);
+        if (t < 5 && i0 - 2 + SW_T + t <= IM + 1) put(SW_T + t, q1);
+        if (i0 + t <= IM + 1) {
+#pragma unroll
+          for (int m = 0; m < 3; ++m) rs.ax[m][t] = (float)a0[m];
+        }
+        if (t == 0 && i0 + SW_T <= IM + 1) {
+#pragma unroll
+          for (int m = 0; m < 3; ++m) rs.ax[m][SW_T] = (float)a1[m];
+        }
+        if (r + 1 < r1) fetch(r + 1);
+        __syncthreads();
+        const int i = i0 + t;
+        const bool valid = i <= IM - 2;
+        if (valid) {
+          const float A[3] = {rs.ax[0][t], rs.ax[1][t], rs.ax[2][t]};
+          const float B[3] = {rs.ax[0][t + 1], rs.ax[1][t + 1], rs.ax[2][t + 1]};
+          float nx, ny, nz;
+          face_unit_normal(A, B, nx, ny, nz);
+          auto P = [&](int q) {
+            NodePrim p;
+            p.r = rs.pr[0][t + q];
+            p.p = rs.pr[1][t + q];
+            p.u = rs.pr[2][t + q];
+            p.v = rs.pr[3][t + q];
+            p.w = rs.pr[4][t + q];
+            return p;
+          };
+          features_of(P, nx, ny, nz, gamma, f);
+        } else {
+#pragma unroll
+          for (int m = 0; m < SN_IN; ++m) f[m] = 0.f;
+        }
+        ok = classify(cx, t, f, valid, i + (long)(IM - 1) * ((j - 1) + (long)(JM - 2) * (k - 1)));
       }
-      break;
-    }
-    if (e < nf) {
-      // non-finite features (e.g. a non-physical state) fall back to WENO5
-      const unsigned char dec = (z >= zcut || !(z == z)) ? 1 : 0;
-      a.mask[e] = dec;
-      nweno += dec;
+    } else {  // j- or k-faces: a window sweep along the direction
+      const bool dj = item < n0 + n1;
+      const long it = dj ? item - n0 : item - n0 - n1;
+      const int seg = (int)(it % nseg);
+      const long r2 = it / nseg;
+      // dj: c = k (1..KM-2), faces along j; else c = j (1..JM-2), faces along k
+      const int cdim = dj ? KM - 2 : JM - 2;
+      const int c = 1 + (int)(r2 % cdim), ch = (int)(r2 / cdim);
+      const int nface = dj ? JM - 1 : KM - 1;
+      const int f0 = ch * SW_CH, f1 = min(nface, f0 + SW_CH);
+      const int i = 1 + seg * SW_T + t;
+      const bool valid = i <= IM - 2;
+      const long sd = dj ? d.PX : d.PL;
+      const int am = dj ? 3 : 6;  // J grad(eta) or J grad(zeta)
+      // offset of the sweep's position 0 for this column; face fc has global
+      // index e0 + fc * es
+      const long obase = dj ? node_off(d, valid ? i : 1, 0, c) : node_off(d, valid ? i : 1, c, 0);
+      const long e0 = dj ? nfi + (i - 1) + (long)(IM - 2) * (JM - 1) * (c - 1) : nfi + nfj + (i - 1) + (long)(IM - 2) * (c - 1);
+      const long es = dj ? (long)(IM - 2) : (long)(IM - 2) * (JM - 2);
+      NodePrim W0, W1, W2, W3, W4, W5;
+      float Aa[3], Ab[3];
+      // step u (face f0+u) consumes node f0+3+u and the area vector of node f0+1+u
+      auto issue = [&](int u) {
+        if (valid && f0 + u < f1) {
+          const int slot = u % SW_D;
+          const long on = obase + (long)(f0 + 3 + u) * sd, oa = obase + (long)(f0 + 1 + u) * sd;
+#pragma unroll
+          for (int n = 0; n < 5; ++n) cp_async8(&ws.v[slot][n][t], a.q + n * VOL + on);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) cp_async8(&ws.v[slot][5 + m][t], a.area[am + m] + oa);
+        }
+        cp_async_commit();  // one group per step, empty or not
+      };
+#pragma unroll
+      for (int u = 0; u < SW_D; ++u) issue(u);
+      if (valid) {
+        double qq[5];
+        load_q(a.q + obase + (long)(f0 - 2) * sd, qq);
+        W0 = prim_of(qq);
+        load_q(a.q + obase + (long)(f0 - 1) * sd, qq);
+        W1 = prim_of(qq);
+        load_q(a.q + obase + (long)f0 * sd, qq);
+        W2 = prim_of(qq);
+        load_q(a.q + obase + (long)(f0 + 1) * sd, qq);
+        W3 = prim_of(qq);
+        load_q(a.q + obase + (long)(f0 + 2) * sd, qq);
+        W4 = prim_of(qq);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) Aa[m] = (float)__ldg(a.area[am + m] + obase + (long)f0 * sd);
+      }
+      // One face: the window (w0..w4 hold positions fc-2..fc+2, wn receives
+      // fc+3), the area vectors of positions fc (A0) and fc+1 (A1 receives).
+      // The unrolled loop below rotates the roles instead of moving values.
+      auto face = [&](int fc, NodePrim& w0, NodePrim& w1, NodePrim& w2, NodePrim& w3, NodePrim& w4, NodePrim& wn,
+                      float* A0, float* A1) {
+        const int u = fc - f0;
+        cp_async_wait_ring();  // the copies of step u have landed
+        if (valid) {
+          const int slot = u % SW_D;
+          double nq[5];
+#pragma unroll
+          for (int n = 0; n < 5; ++n) nq[n] = ws.v[slot][n][t];
+          wn = prim_of(nq);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) A1[m] = (float)ws.v[slot][5 + m][t];
+        }
+        issue(u + SW_D);  // refill the slot just read
+        if (valid) {
+          float nx, ny, nz;
+          face_unit_normal(A0, A1, nx, ny, nz);
+          auto P = [&](int q) { return q == 0 ? w0 : q == 1 ? w1 : q == 2 ? w2 : q == 3 ? w3 : q == 4 ? w4 : wn; };
+          features_of(P, nx, ny, nz, gamma, f);
+        } else {
+#pragma unroll
+          for (int m = 0; m < SN_IN; ++m) f[m] = 0.f;
+        }
+        return classify(cx, t, f, valid, e0 + fc * es);
+      };
+      for (int fc = f0; ok && fc < f1; fc += 6) {
+        ok = face(fc, W0, W1, W2, W3, W4, W5, Aa, Ab);
+        if (!ok || fc + 1 >= f1) break;
+        ok = face(fc + 1, W1, W2, W3, W4, W5, W0, Ab, Aa);
+        if (!ok || fc + 2 >= f1) break;
+        ok = face(fc + 2, W2, W3, W4, W5, W0, W1, Aa, Ab);
+        if (!ok || fc + 3 >= f1) break;
+        ok = face(fc + 3, W3, W4, W5, W0, W1, W2, Ab, Aa);
+        if (!ok || fc + 4 >= f1) break;
+        ok = face(fc + 4, W4, W5, W0, W1, W2, W3, Aa, Ab);
+        if (!ok || fc + 5 >= f1) break;
+        ok = face(fc + 5, W5, W0, W1, W2, W3, W4, Ab, Aa);
+      }
+      cp_async_wait_all();  // the ring is reused by the next item
     }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) nweno += __shfl_xor_sync(0xffffffffu, nweno, o);
-  if ((t & 31) == 0 && nweno) atomicAdd(&a.st->weno_faces, (unsigned long long)nweno);
+  if (!ok && t == 0) {  // decisions incomplete: the step takes WENO5 everywhere
+    atomicExch(&a.st->sensor_fail, 1);
+    atomicExch(&a.st->force_weno, 1);
+  }
   tc::fence_before_sync();
   __syncthreads();
   if (t < 32) {
@@ -111,19 +328,29 @@ __global__ void __launch_bounds__(128) sensor_mask_kernel(const MaskArgs a) {
 }  // namespace
 
 cudaError_t launch_sensor_mask(const MaskArgs& a, cudaStream_t s) {
-  const int smem = (int)sizeof(tc::Smem) + 128;
+  const int smem0 = (int)(sizeof(tc::Smem) + sizeof(RowSmem)) + 128;
+  const int smem1 = (int)(sizeof(tc::Smem) + sizeof(WinSmem)) + 128;
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(sensor_mask_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(sensor_mask_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem0);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(sensor_mask_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem1);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  const long nf = (long)(a.d.IM - 1) * (a.d.JM - 2) * (a.d.KM - 2) + (long)(a.d.IM - 2) * (a.d.JM - 1) * (a.d.KM - 2) +
-                  (long)(a.d.IM - 2) * (a.d.JM - 2) * (a.d.KM - 1);
-  const long ntiles = (nf + 127) / 128;
-  // 8 CTAs per SM fill the 512 TMEM columns (64 each) and hide the MMA round trips
-  const unsigned grid = (unsigned)(ntiles < 148L * 8 ? ntiles : 148L * 8);
-  sensor_mask_kernel<<<grid, 128, smem, s>>>(a);
+  const Dims& d = a.d;
+  const long rows = (long)(d.JM - 2) * (d.KM - 2);
+  const long nseg0 = (d.IM - 1 + SW_T - 1) / SW_T, nseg = (d.IM - 2 + SW_T - 1) / SW_T;
+  const long items0 = nseg0 * ((rows + SW_CH - 1) / SW_CH);
+  const long items1 = nseg * (d.KM - 2) * ((d.JM - 1 + SW_CH - 1) / SW_CH) +
+                      nseg * (d.JM - 2) * ((d.KM - 1 + SW_CH - 1) / SW_CH);
+  // at most 8 CTAs per SM hold TMEM (64 columns each of 512); the two
+  // launches run back to back on the stream
+  const long cap0 = 148L * 5, cap1 = 148L * 4;
+  sensor_mask_kernel<0><<<(unsigned)(items0 < cap0 ? items0 : cap0), SW_T, smem0, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  sensor_mask_kernel<1><<<(unsigned)(items1 < cap1 ? items1 : cap1), SW_T, smem1, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -49,10 +49,23 @@ template <typename S, typename R>
 struct Smem {
   S ring[6][NEQ][NC];
   S plane[NEQ][PH][PW];
-  S sx[3][TJ][TI + 2];  // J*grad(xi) at node (i0-1+c, j0+r)
-  S sy[3][TJ + 2][TI];  // J*grad(eta) at node (i0+c, j0-1+r)
+  // node area vectors in FP64 in every precision: the flux converts them,
+  // the stage-3 spectral radius (dt) uses them exactly
+  double sx[3][TJ][TI + 2];  // J*grad(xi) at node (i0-1+c, j0+r)
+  double sy[3][TJ + 2][TI];  // J*grad(eta) at node (i0+c, j0-1+r)
   R fi[NEQ][TJ][TI + 1];
   R fj[NEQ][TJ + 1][TI];
+};
+
+// Extra shared memory of the hybrid kernel: the plane's k+1/2 face fluxes and
+// normals (a WENO5 k-face may be evaluated by another thread than its
+// column's), and the list of the plane's faces that take WENO5.
+template <typename R>
+struct HybSmem {
+  R fk[NEQ][NC];
+  R kn[3][NC];
+  unsigned short list[NFI + NFJ + NC];  // round << 10 | index within the round
+  int count;
 };
 
 // 4th-order central derivative of a node field along a stride, at offset o.
@@ -120,14 +133,14 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
       }
     }
   };
-  auto load_zeta = [&](int kp, R z[3]) {
+  auto load_zeta = [&](int kp, double z[3]) {
     const long o = node_off(d, ci, cj, kp);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) z[m] = (R)__ldg(a.area[6 + m] + o);
+    for (int m = 0; m < 3; ++m) z[m] = __ldg(a.area[6 + m] + o);
   };
 
   // k-face between planes kk and kk+1 of this thread's column
-  auto k_face = [&](int kk, const R za[3], const R zb[3], R out[5]) {
+  auto k_face = [&](int kk, const double za[3], const double zb[3], R out[5]) {
     const int s0 = (kk - 2 + 6) % 6;
     auto ld = [&](int p, int n) -> R {
       int s = s0 + p;
@@ -135,12 +148,35 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
       return (R)sm.ring[s][n][t];
     };
     const long e = nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * kk);
-    flux(ld, R(0.5) * (za[0] + zb[0]), R(0.5) * (za[1] + zb[1]), R(0.5) * (za[2] + zb[2]), e, out);
+    flux(ld, R(0.5) * ((R)za[0] + (R)zb[0]), R(0.5) * ((R)za[1] + (R)zb[1]), R(0.5) * ((R)za[2] + (R)zb[2]), e, out);
+  };
+
+  // The FP32 kernels fetch the ring column of plane k+4 into registers while
+  // plane k is computed and store it at the top of the next iteration, so the
+  // ring load is off the critical path (the FP64 kernel has no registers to spare).
+  constexpr bool kPrefetch = sizeof(S) == 4;
+  double pre[NEQ];
+  auto fetch_ring = [&](int kp) {
+    if (col_thread && ci <= d.IM + 1 && cj <= d.JM + 1) {
+      const long o = node_off(d, ci, cj, kp);
+#pragma unroll
+      for (int n = 0; n < NEQ; ++n) pre[n] = __ldg(a.src + n * VOL + o);
+    }
+  };
+  auto store_ring = [&](int kp) {
+    if (col_thread && ci <= d.IM + 1 && cj <= d.JM + 1) {
+      S* dst = &sm.ring[(kp + 6) % 6][0][t];
+#pragma unroll
+      for (int n = 0; n < NEQ; ++n) dst[n * NC] = (S)pre[n];
+    }
   };
 
   // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
   for (int kp = kb - 3; kp <= kb + 2; ++kp) load_ring(kp);
-  R za[3] = {0, 0, 0}, zb[3] = {0, 0, 0};
+  if (kPrefetch) fetch_ring(kb + 3);
+  // the column's J*grad(zeta) at planes k and k+1, in FP64 (the stage-3
+  // spectral radius uses it exactly)
+  double za[3] = {0, 0, 0}, zb[3] = {0, 0, 0};
   if (col_valid) {
     load_zeta(kb - 1, za);
     load_zeta(kb, zb);
@@ -157,9 +193,17 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
   for (int k = kb; k < ke; ++k) {
     if (col_valid) load_zeta(k + 1, zb);  // consumed in round C
     __syncthreads();
-    load_ring(k + 3);
+    if (kPrefetch) {
+      store_ring(k + 3);
+      if (k + 1 < ke) fetch_ring(k + 4);
+    } else {
+      load_ring(k + 3);
+    }
     // plane k with halo: interior from the ring, halo from global memory
     {
+      if constexpr (HYB) {
+        if (t == 0) reinterpret_cast<HybSmem<R>*>(smem_raw + sizeof(Smem<S, R>))->count = 0;
+      }
       const int sk = k % 6;
       for (int e = t; e < NC; e += NT) {
         const int x = e % TI, y = e / TI;
@@ -195,7 +239,7 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
           if (gi <= d.IM + 1 && gj <= d.JM + 1) {
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) sm.sx[m][r][c] = (S)__ldg(a.area[m] + o);
+            for (int m = 0; m < 3; ++m) sm.sx[m][r][c] = __ldg(a.area[m] + o);
           }
         } else {
           const int e2 = e - NSX;
@@ -204,47 +248,196 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
           if (gi <= d.IM + 1 && gj <= d.JM + 1) {
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) sm.sy[m][r][c] = (S)__ldg(a.area[3 + m] + o);
+            for (int m = 0; m < 3; ++m) sm.sy[m][r][c] = __ldg(a.area[3 + m] + o);
           }
         }
       }
     }
     __syncthreads();
 
-    // round A: i-faces.  Face fx (0..TI) of row fy lies between tile columns fx-1 and fx.
-    if (t < NFI) {
-      const int fx = t % (TI + 1), fy = t / (TI + 1);
-      const int ga = ti0 + fx - 1, gj = tj0 + fy;
-      if (ga <= d.IM - 2 && gj <= d.JM - 2) {
-        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
-        R f[5];
-        const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
-        flux(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
-             R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
-             R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), e, f);
-#pragma unroll
-        for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
-      }
-    }
-    // round B: j-faces.  Face fy (0..TJ) of column fx lies between tile rows fy-1 and fy.
-    if (t < NFJ) {
-      const int fx = t % TI, fy = t / TI;
-      const int gi = ti0 + fx, ga = tj0 + fy - 1;
-      if (gi <= d.IM - 2 && ga <= d.JM - 2) {
-        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
-        R f[5];
-        const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
-        flux(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
-             R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
-             R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), e, f);
-#pragma unroll
-        for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
-      }
-    }
-    // round C: the k+1/2 face of this column
     R fkp[5];
-    if (col_valid) k_face(k, za, zb, fkp);
-    __syncthreads();
+    if (!HYB || all_weno) {
+      // round A: i-faces.  Face fx (0..TI) of row fy lies between tile columns fx-1 and fx.
+      if (t < NFI) {
+        const int fx = t % (TI + 1), fy = t / (TI + 1);
+        const int ga = ti0 + fx - 1, gj = tj0 + fy;
+        if (ga <= d.IM - 2 && gj <= d.JM - 2) {
+          auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
+          R f[5];
+          const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
+          flux(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
+               R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
+               R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), e, f);
+  #pragma unroll
+          for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
+        }
+      }
+      // round B: j-faces.  Face fy (0..TJ) of column fx lies between tile rows fy-1 and fy.
+      if (t < NFJ) {
+        const int fx = t % TI, fy = t / TI;
+        const int gi = ti0 + fx, ga = tj0 + fy - 1;
+        if (gi <= d.IM - 2 && ga <= d.JM - 2) {
+          auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
+          R f[5];
+          const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
+          flux(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
+               R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
+               R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), e, f);
+  #pragma unroll
+          for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
+        }
+      }
+      // round C: the k+1/2 face of this column
+      if (col_valid) k_face(k, za, zb, fkp);
+      __syncthreads();
+    } else if constexpr (HYB) {
+      // Hybrid, decisions in effect.  Phase 1: every thread evaluates the
+      // linear faces of its three rounds and queues the WENO5 faces; phase 2:
+      // all 256 threads share the queued WENO5 faces, so a warp pays for
+      // WENO5 only in proportion to the faces that need it.
+      HybSmem<R>& hs = *reinterpret_cast<HybSmem<R>*>(smem_raw + sizeof(Smem<S, R>));
+      const unsigned lane = t & 31;
+      auto push = [&](bool q, int code) {
+        const unsigned b = __ballot_sync(0xffffffffu, q);
+        if (b) {
+          int base = 0;
+          if (lane == 0) base = atomicAdd(&hs.count, __popc(b));
+          base = __shfl_sync(0xffffffffu, base, 0);
+          if (q) hs.list[base + __popc(b & ((1u << lane) - 1u))] = (unsigned short)code;
+        }
+      };
+      {  // round A: i-faces
+        bool q = false;
+        if (t < NFI) {
+          const int fx = t % (TI + 1), fy = t / (TI + 1);
+          const int ga = ti0 + fx - 1, gj = tj0 + fy;
+          if (ga <= d.IM - 2 && gj <= d.JM - 2) {
+            const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
+            if (__ldg(a.mask + e)) {
+              q = true;
+            } else {
+              auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
+              R f[5];
+              face_flux_linear<R>(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
+                                  R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
+                                  R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), C, f);
+#pragma unroll
+              for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
+            }
+          }
+        }
+        push(q, t);
+      }
+      {  // round B: j-faces
+        bool q = false;
+        if (t < NFJ) {
+          const int fx = t % TI, fy = t / TI;
+          const int gi = ti0 + fx, ga = tj0 + fy - 1;
+          if (gi <= d.IM - 2 && ga <= d.JM - 2) {
+            const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
+            if (__ldg(a.mask + e)) {
+              q = true;
+            } else {
+              auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
+              R f[5];
+              face_flux_linear<R>(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
+                                  R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
+                                  R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), C, f);
+#pragma unroll
+              for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
+            }
+          }
+        }
+        push(q, (1 << 10) | t);
+      }
+      {  // round C: the k+1/2 face of this column
+        bool q = false;
+        if (col_valid) {
+          const long e = nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * k);
+          const R nx = R(0.5) * ((R)za[0] + (R)zb[0]), ny = R(0.5) * ((R)za[1] + (R)zb[1]),
+                  nz = R(0.5) * ((R)za[2] + (R)zb[2]);
+          if (__ldg(a.mask + e)) {
+            q = true;
+            hs.kn[0][t] = nx;
+            hs.kn[1][t] = ny;
+            hs.kn[2][t] = nz;
+          } else {
+            const int s0 = (k - 2 + 6) % 6;
+            auto ld = [&](int p, int n) -> R {
+              int s = s0 + p;
+              s = s >= 6 ? s - 6 : s;
+              return (R)sm.ring[s][n][t];
+            };
+            R f[5];
+            face_flux_linear<R>(ld, nx, ny, nz, C, f);
+#pragma unroll
+            for (int n = 0; n < NEQ; ++n) hs.fk[n][t] = f[n];
+          }
+        }
+        push(q, (2 << 10) | t);
+      }
+      __syncthreads();
+      // phase 2: one WENO5 evaluation per queued face; the stencil of every
+      // kind of face is read through the same offsets, so the warp runs one
+      // copy of the flux code
+      const int cnt = hs.count;
+      const int s0 = (k - 2 + 6) % 6;
+      for (int w = t; w < cnt; w += NT) {
+        const int code = hs.list[w], r = code >> 10, x = code & 1023;
+        const S* base;
+        int off[6], ns;
+        R nx, ny, nz;
+        R* out;
+        int os;
+        if (r == 0) {
+          const int fx = x % (TI + 1), fy = x / (TI + 1);
+          base = &sm.plane[0][fy + H][fx];
+#pragma unroll
+          for (int p = 0; p < 6; ++p) off[p] = p;
+          ns = PH * PW;
+          nx = R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]);
+          ny = R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]);
+          nz = R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]);
+          out = &sm.fi[0][fy][fx];
+          os = TJ * (TI + 1);
+        } else if (r == 1) {
+          const int fx = x % TI, fy = x / TI;
+          base = &sm.plane[0][fy][fx + H];
+#pragma unroll
+          for (int p = 0; p < 6; ++p) off[p] = p * PW;
+          ns = PH * PW;
+          nx = R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]);
+          ny = R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]);
+          nz = R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]);
+          out = &sm.fj[0][fy][fx];
+          os = (TJ + 1) * TI;
+        } else {
+          base = &sm.ring[0][0][x];
+#pragma unroll
+          for (int p = 0; p < 6; ++p) {
+            int sp = s0 + p;
+            sp = sp >= 6 ? sp - 6 : sp;
+            off[p] = sp * NEQ * NC;
+          }
+          ns = NC;
+          nx = hs.kn[0][x];
+          ny = hs.kn[1][x];
+          nz = hs.kn[2][x];
+          out = &hs.fk[0][x];
+          os = NC;
+        }
+        auto ld = [&](int p, int n) -> R { return (R)base[off[p] + n * ns]; };
+        R f[5];
+        face_flux<R>(ld, nx, ny, nz, C, f);
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) out[n * os] = f[n];
+      }
+      __syncthreads();
+      if (col_valid) {
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) fkp[n] = hs.fk[n][t];
+      }
+    }
 
     if (col_valid) {
       const long o = node_off(d, ci, cj, k);
@@ -282,7 +475,10 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
           } else if (MODE == 2) {
             q[n] = 0.75 * __ldg(a.q0 + e) + 0.25 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L);
           } else {
-            q[n] = (a.q0[e] + 2.0 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L)) / 3.0;
+            // the plain (FP64) kernel divides by 3 as the reference does; the
+            // FP32-flux kernels multiply by the rounded 1/3 (one ulp apart)
+            const double sum = a.q0[e] + 2.0 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L);
+            q[n] = kExactRing ? sum / 3.0 : sum * (1.0 / 3.0);
           }
         }
 #pragma unroll
@@ -299,18 +495,15 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
             a.prim[4][o] = pp;
             a.prim[5][o] = a.gM2 * pp / r;
           } else {
-            // grad(xi), grad(eta), grad(zeta) = area vectors / J (FP64 in both precisions)
+            // grad(xi), grad(eta), grad(zeta) = area vectors / J (FP64 in both
+            // precisions: xi and eta from the FP64 staging, zeta from the
+            // registers (FP64 kernel) or memory)
             double g[9];
-            if (kExactRing) {
 #pragma unroll
-              for (int m = 0; m < 3; ++m) {
-                g[m] = (double)sm.sx[m][cy][cx + 1] * iJ;
-                g[3 + m] = (double)sm.sy[m][cy + 1][cx] * iJ;
-                g[6 + m] = (double)za[m] * iJ;
-              }
-            } else {
-#pragma unroll
-              for (int m = 0; m < 9; ++m) g[m] = __ldg(a.area[m] + o) * iJ;
+            for (int m = 0; m < 3; ++m) {
+              g[m] = sm.sx[m][cy][cx + 1] * iJ;
+              g[3 + m] = sm.sy[m][cy + 1][cx] * iJ;
+              g[6 + m] = za[m] * iJ;
             }
             const double cs = sqrt(a.gamma * pp / r);
             double s = 0.0;
@@ -350,9 +543,14 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
   }
 }
 
+template <typename R, bool HYB>
+constexpr size_t stage_smem() {
+  return sizeof(Smem<R, R>) + (HYB ? sizeof(HybSmem<R>) : 0);
+}
+
 template <typename R, bool VISC, int MODE, int NB, bool HYB>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
-  const size_t smem = sizeof(Smem<R, R>);
+  const size_t smem = stage_smem<R, HYB>();
   dim3 grid(a.ntile_i * a.ntile_j, (a.d.KM - 2 + a.kchunk - 1) / a.kchunk);
   stage_kernel<R, VISC, MODE, NB, HYB><<<grid, NT, smem, s>>>(a);
   return cudaGetLastError();
@@ -360,7 +558,7 @@ cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
 
 template <typename R, int NB, bool HYB>
 void prepare_nb() {
-  const int smem = (int)sizeof(Smem<R, R>);
+  const int smem = (int)stage_smem<R, HYB>();
   cudaFuncSetAttribute(stage_kernel<R, false, 0, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(stage_kernel<R, false, 1, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(stage_kernel<R, false, 2, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

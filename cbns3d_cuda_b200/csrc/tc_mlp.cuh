@@ -5,9 +5,11 @@
 //
 // One tile = 128 faces (MMA M = 128).  Layer 1: D1[128x32] = X[128x16] W1'[32x16]^T
 // where column 15 of X is 1 and column 15 of W1' is b1 (bias folded into K).
-// Layer 2: D2[128x32] = relu(D1)[128x32] W2[32x32]^T (two K = 16 MMAs).  The
-// output layer (32 -> 1, plus b2 and b3) runs on the CUDA cores from the
-// FP32 accumulators.
+// Layer 2: D2[128x32] = relu(D1)[128x32] W2[32x32]^T (two K = 16 MMAs) plus
+// b2 through a third MMA, ONE[128x16] B2'[32x16]^T, where columns 0 and 1 of
+// ONE are 1 and of B2' the BF16 high and low parts of b2 (b2 to ~16 bits).
+// The output layer (32 -> 1, plus b3) runs on the CUDA cores from the FP32
+// accumulators.
 //
 // Shared-memory operands use the canonical K-major layout without swizzle:
 // 8-row x 16-byte core matrices, element (r, k) at
@@ -28,8 +30,9 @@ constexpr int X_BYTES = 128 * 16 * 2;   // layer-1 A: 128 x 16
 constexpr int H_BYTES = 128 * 32 * 2;   // layer-2 A: 128 x 32
 constexpr int W1_BYTES = 32 * 16 * 2;   // layer-1 B: 32 x 16
 constexpr int W2_BYTES = 32 * 32 * 2;   // layer-2 B: 32 x 32
+constexpr int B2_BYTES = 32 * 16 * 2;   // layer-2 bias B: 32 x 16
 constexpr unsigned TMEM_COLS = 64;      // D1 at columns 0..31, D2 at 32..63
-constexpr unsigned WAIT_LIMIT = 1u << 22;
+constexpr unsigned WAIT_LIMIT = 1u << 20;
 
 // instruction descriptor: D = F32, A = B = BF16, both K-major, N = 32, M = 128
 constexpr unsigned IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
@@ -68,17 +71,21 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Wait for the given phase with an iteration limit; false on timeout.
+// Wait for the given phase with an iteration limit; false on timeout.  Each
+// try_wait may suspend the thread for up to SUSPEND_NS before it returns
+// false, so the wait costs few instructions and is bounded by about
+// WAIT_LIMIT x SUSPEND_NS.
+constexpr unsigned SUSPEND_NS = 1000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase) {
   const unsigned a = smem_u32(bar);
   for (unsigned it = 0; it < WAIT_LIMIT; ++it) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(a), "r"(phase)
+        : "r"(a), "r"(phase), "r"(SUSPEND_NS)
         : "memory");
     if (done) return true;
   }
@@ -121,13 +128,30 @@ __device__ __forceinline__ void tmem_ld32(unsigned taddr, float v[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 consecutive FP32 columns of this thread's TMEM lane
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float v[16]) {
+  unsigned r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // Shared memory of the tensor-core MLP (all operand tiles 128-byte aligned).
 struct alignas(128) Smem {
   unsigned char x[X_BYTES];    // layer-1 A (features + constant 1)
   unsigned char h[H_BYTES];    // layer-2 A (relu(D1))
+  unsigned char one[X_BYTES];  // bias A (columns 0, 1 = 1)
   unsigned char w1[W1_BYTES];  // layer-1 B ([W1 | b1])
   unsigned char w2[W2_BYTES];  // layer-2 B (W2)
-  float b2[SN_H], w3[SN_H];
+  unsigned char b2[B2_BYTES];  // bias B (columns 0, 1 = b2 high, low)
+  alignas(16) float w3[SN_H];
   float b3;
   unsigned long long bar;
   unsigned tmem;
@@ -145,10 +169,18 @@ __device__ __forceinline__ void load_weights(Smem& s, const float* P, int t, int
     const int n = e >> 5, k = e & 31;
     *reinterpret_cast<__nv_bfloat16*>(s.w2 + kmajor_off(n, k, 32)) = __float2bfloat16_rn(P[SP_W2 + e]);
   }
-  for (int e = t; e < SN_H; e += nthreads) {
-    s.b2[e] = P[SP_B2 + e];
-    s.w3[e] = P[SP_W3 + e];
+  for (int e = t; e < SN_H * 16; e += nthreads) {
+    const int n = e >> 4, k = e & 15;
+    const float b = P[SP_B2 + n];
+    const __nv_bfloat16 hi = __float2bfloat16_rn(b);
+    const float v = k == 0 ? b : (k == 1 ? b - __bfloat162float(hi) : 0.0f);
+    *reinterpret_cast<__nv_bfloat16*>(s.b2 + kmajor_off(n, k, 16)) = __float2bfloat16_rn(v);
   }
+  for (int e = t; e < 128 * 16; e += nthreads) {
+    const int r = e >> 4, k = e & 15;
+    *reinterpret_cast<__nv_bfloat16*>(s.one + kmajor_off(r, k, 16)) = __float2bfloat16_rn(k < 2 ? 1.0f : 0.0f);
+  }
+  for (int e = t; e < SN_H; e += nthreads) s.w3[e] = P[SP_W3 + e];
   if (t == 0) s.b3 = P[SP_B3];
 }
 
@@ -175,20 +207,24 @@ __device__ __forceinline__ bool run_tile(Smem& s, int t, unsigned& phase, float*
     mma_bf16(tmem, sdesc(smem_u32(s.x), 128, 256), sdesc(smem_u32(s.w1), 128, 256), false);
     mma_commit(&s.bar);
   }
-  bool ok = mbar_wait(&s.bar, phase);
+  // warp 0 waits on the barrier, the other warps at the CTA barrier (which
+  // issues nothing); every thread then takes the same branch
+  const int warp = t >> 5;
+  bool ok = warp == 0 ? mbar_wait(&s.bar, phase) : true;
   phase ^= 1u;
-  // every thread takes the same branch: stop issuing if any wait gave up
   if (!__syncthreads_and(ok)) return false;
   fence_after_sync();
-  const int warp = t >> 5;
   if (warp < 4) {
-    float d1[32];
-    tmem_ld32(tmem + ((unsigned)(32 * warp) << 16), d1);
     const int row = t;
 #pragma unroll
-    for (int k = 0; k < 32; k += 2) {
-      *reinterpret_cast<__nv_bfloat162*>(s.h + kmajor_off(row, k, 32)) =
-          __floats2bfloat162_rn(fmaxf(d1[k], 0.f), fmaxf(d1[k + 1], 0.f));
+    for (int half = 0; half < 2; ++half) {  // two 16-column loads keep register pressure down
+      float d1[16];
+      tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + 16 * half, d1);
+#pragma unroll
+      for (int k = 0; k < 16; k += 2) {
+        *reinterpret_cast<__nv_bfloat162*>(s.h + kmajor_off(row, 16 * half + k, 32)) =
+            __floats2bfloat162_rn(fmaxf(d1[k], 0.f), fmaxf(d1[k + 1], 0.f));
+      }
     }
   }
   fence_async_smem();
@@ -199,18 +235,27 @@ __device__ __forceinline__ bool run_tile(Smem& s, int t, unsigned& phase, float*
     const unsigned ha = smem_u32(s.h), wa = smem_u32(s.w2);
     mma_bf16(tmem + 32, sdesc(ha, 128, 512), sdesc(wa, 128, 512), false);
     mma_bf16(tmem + 32, sdesc(ha + 256, 128, 512), sdesc(wa + 256, 128, 512), true);
+    mma_bf16(tmem + 32, sdesc(smem_u32(s.one), 128, 256), sdesc(smem_u32(s.b2), 128, 256), true);
     mma_commit(&s.bar);
   }
-  ok = mbar_wait(&s.bar, phase);
+  ok = warp == 0 ? mbar_wait(&s.bar, phase) : true;
   phase ^= 1u;
   if (!__syncthreads_and(ok)) return false;
   fence_after_sync();
   if (warp < 4) {
-    float d2[32];
-    tmem_ld32(tmem + ((unsigned)(32 * warp) << 16) + 32, d2);
     float z = s.b3;
+    const float4* w3 = reinterpret_cast<const float4*>(s.w3);
 #pragma unroll
-    for (int k = 0; k < 32; ++k) z += s.w3[k] * fmaxf(d2[k] + s.b2[k], 0.f);
+    for (int half = 0; half < 2; ++half) {
+      float d2[16];
+      tmem_ld16(tmem + ((unsigned)(32 * warp) << 16) + 32 + 16 * half, d2);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float4 w = w3[4 * half + k];
+        z += w.x * fmaxf(d2[4 * k], 0.f) + w.y * fmaxf(d2[4 * k + 1], 0.f) + w.z * fmaxf(d2[4 * k + 2], 0.f) +
+             w.w * fmaxf(d2[4 * k + 3], 0.f);
+      }
+    }
     *logit = z;
   }
   fence_before_sync();

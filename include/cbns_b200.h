@@ -166,7 +166,9 @@ int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM, const doub
  * CBNS_SENSOR_NPARAM values: W1[32][15] b1[32] W2[32][32] b2[32] w3[32] b3.
  * Features of a face: the jumps of density, pressure and normal velocity
  * across its 5-point stencil, divided by the face's mean density, pressure and
- * sound speed, each compressed as asinh(f / 0.01) / asinh(100).  Label: 1 when the WENO5 nonlinear weights of the face's
+ * sound speed, each compressed as sign(f) log2(1 + |f| / 0.01).  Faces whose
+ * compressed features sum to less than 0.0045 in absolute value (flat
+ * stencils) take the linear flux without evaluating the network.  Label: 1 when the WENO5 nonlinear weights of the face's
  * characteristic reconstruction depart from the linear weights by more than
  * 0.05.  Pointers marked _dev are device pointers; stream is a cudaStream_t. */
 #define CBNS_SENSOR_NIN    15
@@ -199,9 +201,13 @@ int cbns_mlp_predict(const float* params_dev, const float* x_dev, unsigned n, fl
  * evaluated on every face of the step's starting state on the tensor cores;
  * faces with probability >= tau take the characteristic WENO5 flux, the others
  * the linear upwind-5 flux (same Lax-Friedrichs splitting, component-wise).
- * The decisions hold for the three stages of the step.  An audit recomputes,
- * on the linear faces with (global face index % audit_stride) equal to
- * (step % audit_stride), both fluxes; a relative difference above audit_bound
+ * The WENO5 decisions are then widened, per face direction, by 2 faces along
+ * the face's own grid line and 1 face in the two other index directions (a
+ * discontinuity moves less than a cell per step), and hold for the three
+ * stages of the step.  An audit recomputes,
+ * on the linear faces whose run of 128 consecutive global face indices r =
+ * index / 128 has r % audit_stride equal to step % audit_stride, both
+ * fluxes; a relative difference above audit_bound
  * on any of them makes the whole step take WENO5 everywhere.  A context of
  * precision HYBRID refuses to step (CBNS_ERR_STATE) until cbns_sensor_load.
  * params_host: CBNS_SENSOR_NPARAM floats in host memory. */
@@ -209,8 +215,8 @@ int cbns_sensor_load(cbns_ctx* ctx, const float* params_host, float tau);
 /* audit_stride >= 1 (1 audits every linear face every step); audit_bound > 0
  * (relative to the face's largest flux component).  Defaults 97 and 1e-2. */
 int cbns_sensor_audit(cbns_ctx* ctx, unsigned audit_stride, float audit_bound);
-/* Counters since the last cbns_sensor_stats_reset: faces sent to WENO5 by the
- * network (summed over steps), faces audited, steps whose decisions the audit
+/* Counters since the last cbns_sensor_stats_reset: faces that took WENO5
+ * (network decisions after widening, summed over steps), faces audited, steps whose decisions the audit
  * rejected, the largest relative difference the audit saw, and a non-zero
  * sensor_fail when a tensor-core wait timed out (the step then took WENO5). */
 typedef struct cbns_sensor_stats {
@@ -236,8 +242,8 @@ int cbns_autotune(cbns_ctx* ctx, int* chosen);
 
 /* Per-kernel device timing with CUDA events on the launch stream.  Kernel ids:
  * 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous node
- * fluxes, 3 dt/step bookkeeping, 4 hybrid sensor and audit.  total_ms is the
- * summed event time. */
+ * fluxes, 3 dt/step bookkeeping, 4 hybrid sensor network, 5 hybrid audit.
+ * total_ms is the summed event time. */
 int cbns_prof_enable(cbns_ctx* ctx, int on);
 int cbns_prof_read(cbns_ctx* ctx, int kernel_id, double* total_ms, unsigned* launches);
 int cbns_prof_reset(cbns_ctx* ctx);

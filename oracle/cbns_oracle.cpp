@@ -835,12 +835,12 @@ void orc_set_face_mask(void* h, const unsigned char* mask, long n) {
 // Sensor features and WENO-weight deviation of every grid face, in the order
 // i-faces, j-faces, k-faces (each i fastest), for the learned shock sensor
 // (no counterpart in the reference).  Restates the definitions of the
-// library's sensor.cuh in FP64: 15 normalised (then asinh-compressed) jumps of density, pressure and
+// library's sensor.cuh in FP64: 15 normalised (then log-compressed) jumps of density, pressure and
 // normal velocity; deviation = max |w_k - d_k| of the characteristic WENO5
 // weights (basis and Roe average of the flux) on both sides of all 5 fields.
 void orc_sensor_faces(void* h, int which, float* feat, float* dev) {
-  // each jump compressed as asinh(f / 0.01) / asinh(100)
-  auto compress = [](double f) { return std::asinh(f / 0.01) / std::asinh(100.0); };
+  // each jump compressed as sign(f) log2(1 + |f| / 0.01)
+  auto compress = [](double f) { return std::copysign(std::log2(1.0 + std::abs(f) / 0.01), f); };
   auto* o = static_cast<Oracle*>(h);
   const auto& Q = o->buf(which);
   const long IM = o->IM, JM = o->JM, KM = o->KM;

@@ -1,6 +1,7 @@
 """The hybrid flux (precision PREC_HYBRID) through the C ABI.
 
-* a sensor that sends every face to WENO5 reproduces the split path bit for bit;
+* a sensor that always answers WENO5 follows the split path (flat stencils,
+  which take the linear flux without the network, aside);
 * the GPU's own decisions (read back with cbns_sensor_mask_get) given to the
   oracle's hybrid flux reproduce the GPU right-hand side and steps to the
   accuracy of the split path's FP32 flux arithmetic;
@@ -74,20 +75,62 @@ def _both_used(m):
 SMALL = [lambda: cases.case_blast(24, 24, 24), lambda: cases.case_shock_vortex(40, 36, 12)]
 
 
+FLAT = 0.0045  # sum of |features| below which a stencil is flat (linear flux, no network)
+
+
+def _flat(X):
+    return np.abs(X.cpu().numpy().astype(np.float64)).sum(axis=1) < FLAT
+
+
+def _widen(dec, shape, along=2, across=1):
+    """The library's widening of WENO5 decisions: per face direction, a face
+    takes WENO5 when a face of the same direction within `along` faces on its
+    own grid line, or `across` faces in the other index directions, does."""
+    IM, JM, KM = shape
+    ni, nj = (IM - 1) * (JM - 2) * (KM - 2), (IM - 2) * (JM - 1) * (KM - 2)
+    # numpy axes (k, j, i); the face direction's own axis
+    parts = [(dec[:ni].reshape(KM - 2, JM - 2, IM - 1), 2), (dec[ni:ni + nj].reshape(KM - 2, JM - 1, IM - 2), 1),
+             (dec[ni + nj:].reshape(KM - 1, JM - 2, IM - 2), 0)]
+    out = []
+    for a, own in parts:
+        r = a.copy()
+        for ax in (2, 1, 0):
+            w = along if ax == own else across
+            src = r.copy()
+            n = src.shape[ax]
+            for o in range(1, w + 1):
+                lo = [slice(None)] * 3
+                hi = [slice(None)] * 3
+                lo[ax], hi[ax] = slice(0, n - o), slice(o, n)
+                r[tuple(lo)] |= src[tuple(hi)]
+                r[tuple(hi)] |= src[tuple(lo)]
+        out.append(r.reshape(-1))
+    return np.concatenate(out)
+
+
 @pytest.mark.parametrize("make", SMALL)
-def test_all_weno_sensor_equals_split(make):
+def test_always_weno_sensor_matches_split(make):
+    """A network that always answers WENO5: every non-flat face takes WENO5,
+    flat faces the linear flux, and the state follows the split path to
+    within FP32 round-off."""
     c = make()
     s = _block(c, PREC_SPLIT)
     h = _block(c, PREC_HYBRID, _constant_sensor(30.0))
     for b in (s, h):
         b.set_time(0.0)
         assert b.run(6) == 6
-    assert np.array_equal(h.get_conservative(), s.get_conservative())
+    rs = interior(s.get_conservative(), c.shape)[..., 0]
+    rh = interior(h.get_conservative(), c.shape)[..., 0]
+    assert np.sqrt(np.mean((rh - rs) ** 2) / np.mean(rs ** 2)) <= 1e-5
     st = h.sensor_stats()
-    assert st["weno_faces"] == 6 * st["faces_per_step"]
-    assert st["audit_faces"] == 0 and st["audit_fail_steps"] == 0 and st["sensor_fail"] == 0
+    assert 0 < st["weno_faces"] <= 6 * st["faces_per_step"]
+    assert st["audit_faces"] < st["faces_per_step"] and st["audit_fail_steps"] == 0 and st["sensor_fail"] == 0
+    h.eval_rhs(CBNS_Q)
     m, forced = h.sensor_mask()
-    assert np.all(m == 1) and not forced
+    X, _y, _d, idx = sensor.sample_faces(h, with_dev=True)
+    dec = np.zeros(m.size, np.uint8)
+    dec[idx.cpu().numpy()] = ~_flat(X)
+    assert not forced and np.array_equal(m, _widen(dec, c.shape))
 
 
 @pytest.mark.parametrize("make", SMALL)
@@ -132,6 +175,59 @@ def test_rhs_matches_oracle_under_gpu_decisions(make):
     o.set_face_mask(m)
     err = max(per_var_rel_linf(rhs, o.eval_rhs(CBNS_Q)))
     assert err <= tol, (err, err_split)
+
+
+def _check_widened(m, want, near, shape):
+    """m equals the widening of want, up to faces whose widened value depends
+    on a decision within 1e-4 of the threshold (either answer allowed)."""
+    lo = _widen(want & ~near, shape)
+    hi = _widen(want | near, shape)
+    return bool(np.all((m >= lo) & (m <= hi)))
+
+
+@pytest.mark.parametrize("make", SMALL + [lambda: cases.case_vortex(37, 23, 9)])
+def test_sensor_sweep_matches_sampled_faces(make):
+    """The per-step sensor (directional sweeps, tcgen05) decides every face as
+    the tensor-core predictor does on the sampled features of the same state."""
+    c = make()
+    h = _block(c, PREC_HYBRID, _constant_sensor(0.0))
+    P = _jump_sensor(h)
+    h.sensor_load(P, 0.5)
+    h.eval_rhs(CBNS_Q)
+    m, _ = h.sensor_mask()
+    X, _y, _d, idx = sensor.sample_faces(h, with_dev=True)
+    p = sensor.predict(torch.from_numpy(P).cuda(), X, tensor_cores=True).cpu().numpy()
+    idx = idx.cpu().numpy()
+    assert np.array_equal(np.sort(idx), np.arange(m.size))
+    near = np.zeros(m.size, bool)
+    near[idx] = np.abs(p - 0.5) < 1e-4  # the sweep tests logit >= logit(tau), here p >= tau
+    want = np.zeros(m.size, np.uint8)
+    want[idx] = (p >= 0.5) & ~_flat(X)
+    assert _check_widened(m, want, near, c.shape)
+    assert 0 < m.sum() < m.size
+
+
+def test_trained_sensor_sweep_matches_sampled_faces():
+    """The committed network: the sweep decides every face as the tensor-core
+    predictor on the sampled features (flat stencils linear, then widened)."""
+    from pathlib import Path
+    w = np.load(Path(__file__).resolve().parents[1] / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz")
+    P, tau = w["params"].astype(np.float32), float(w["tau"])
+    c = cases.case_shock_vortex(64, 64, 16)
+    h = _block(c, PREC_HYBRID, P, tau)
+    h.set_time(0.0)
+    assert h.run(5) == 5
+    h.eval_rhs(CBNS_Q)
+    m, _ = h.sensor_mask()
+    X, _y, _d, idx = sensor.sample_faces(h, with_dev=True)
+    p = sensor.predict(torch.from_numpy(P).cuda(), X, tensor_cores=True).cpu().numpy()
+    idx = idx.cpu().numpy()
+    near = np.zeros(m.size, bool)
+    near[idx] = np.abs(p - tau) < 1e-4
+    want = np.zeros(m.size, np.uint8)
+    want[idx] = (p >= tau) & ~_flat(X)
+    assert _check_widened(m, want, near, c.shape)
+    assert 0 < m.sum() < m.size
 
 
 def test_steps_match_oracle_under_gpu_decisions():

@@ -177,6 +177,9 @@ class Block:
     def sensor_audit(self, stride: int = 97, bound: float = 1.0e-2):
         _abi.check(self.lib.cbns_sensor_audit(self.h, int(stride), float(bound)), "cbns_sensor_audit")
 
+    def sensor_interval(self, every: int = 2):
+        _abi.check(self.lib.cbns_sensor_interval(self.h, int(every)), "cbns_sensor_interval")
+
     def sensor_stats(self) -> dict:
         s = _abi.SensorStats()
         _abi.check(self.lib.cbns_sensor_stats_get(self.h, C.byref(s)), "cbns_sensor_stats_get")

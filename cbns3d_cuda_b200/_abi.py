@@ -92,6 +92,7 @@ SIGNATURES = [
     ("cbns_mlp_predict", C.c_int, [_V, _V, C.c_uint, _V, C.c_int, _V, _V]),
     ("cbns_sensor_load", C.c_int, [_V, C.POINTER(C.c_float), C.c_float]),
     ("cbns_sensor_audit", C.c_int, [_V, C.c_uint, C.c_float]),
+    ("cbns_sensor_interval", C.c_int, [_V, C.c_uint]),
     ("cbns_sensor_stats_get", C.c_int, [_V, C.POINTER(SensorStats)]),
     ("cbns_sensor_stats_reset", C.c_int, [_V]),
     ("cbns_sensor_mask_get", C.c_int, [_V, _V, C.c_ulonglong, C.POINTER(C.c_int)]),

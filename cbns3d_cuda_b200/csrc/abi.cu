@@ -66,6 +66,7 @@ struct cbns_ctx {
   long nfaces = 0;
   float sensor_tau = 0.5f;
   unsigned audit_stride = 97;
+  unsigned sensor_every = 2;  // network evaluated every n-th step of cbns_run
   float audit_bound = 1.0e-2f;
   bool sensor_loaded = false;
   bool prof = false;
@@ -275,7 +276,10 @@ void drop_graph(cbns_ctx* c) {
 // The hybrid flux's decisions for the state q: the sensor network on every
 // face (tensor cores), then the audit of a rotating sample of its linear-flux
 // faces against WENO5 (which forces WENO5 for the step on a violation).
-int sensor_launch(cbns_ctx* c, const double* q, bool check_done) {
+// every_step: evaluate the network now (per-call path) instead of on every
+// sensor_every-th step of a run.
+int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step = false) {
+  const unsigned every = every_step ? 1u : c->sensor_every;
   MaskArgs m;
   m.d = c->d;
   m.gamma = (float)c->ph.gamma;
@@ -284,6 +288,7 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done) {
   for (int k = 0; k < 10; ++k) m.area[k] = c->f.area[k];
   m.params = c->sensor_params;
   m.tau = c->sensor_tau;
+  m.every = every;
   m.mask = c->mask_raw;
   m.st = c->st;
   m.check_done = check_done;
@@ -298,8 +303,11 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done) {
       w.in = bufs[dim];
       w.out = bufs[dim + 1];
       w.dim = dim;
+      w.along = 1 + (int)every;
+      w.across = (int)every;
       w.st = c->st;
       w.count = dim == 2;
+      w.every = every;
       w.check_done = check_done;
       CK(launch_sensor_dilate(w, c->stream));
     }
@@ -676,7 +684,7 @@ int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
   }
   if (hybrid(c) && stage == 1) {
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
-    RET(sensor_launch(c, c->qb[src], false));
+    RET(sensor_launch(c, c->qb[src], false, true));
   }
   const StageArgs a = stage_args(c, c->qb[src], c->qb[c->lq], c->qb[c->lp], c->qb[out], false);
   RET(stage_launch(c, a, (int)stage));
@@ -789,7 +797,7 @@ int cbns_eval_rhs(cbns_ctx* c, int which, double* rhs) {
   if (!rhs || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
   if (hybrid(c)) {
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
-    RET(sensor_launch(c, buf(c, which), false));
+    RET(sensor_launch(c, buf(c, which), false, true));
   }
   const StageArgs a = stage_args(c, buf(c, which), nullptr, nullptr, c->staging, false);
   RET(stage_launch(c, a, 0));
@@ -873,6 +881,13 @@ int cbns_sensor_audit(cbns_ctx* c, unsigned stride, float bound) {
   return CBNS_OK;
 }
 
+int cbns_sensor_interval(cbns_ctx* c, unsigned every) {
+  if (!c || every < 1 || every > 8) return CBNS_ERR_ARG;
+  c->sensor_every = every;
+  drop_graph(c);
+  return CBNS_OK;
+}
+
 int cbns_sensor_stats_get(cbns_ctx* c, cbns_sensor_stats* out) {
   if (!c || !out) return CBNS_ERR_ARG;
   StepState h;
@@ -921,7 +936,7 @@ int cbns_autotune(cbns_ctx* c, int* chosen) {
   // the hybrid kernel is timed on the sensor's decisions for this state
   if (hybrid(c)) {
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
-    RET(sensor_launch(c, c->qb[c->lq], false));
+    RET(sensor_launch(c, c->qb[c->lq], false, true));
   }
   const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
   cudaEvent_t e0, e1;

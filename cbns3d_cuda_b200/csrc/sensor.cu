@@ -209,6 +209,28 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float* __restrict__ 
 constexpr int DL = 16;
 __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) {
   if (a.check_done && a.st->done) return;
+  if (!sensor_step(a.st, a.every)) {
+    // decisions of an earlier step: only the statistics
+    if (a.count) {
+      const Dims& d = a.d;
+      const int dir = blockIdx.z / (d.KM - 1), x2 = blockIdx.z % (d.KM - 1);
+      const int n0 = dir == 0 ? d.IM - 1 : d.IM - 2, n1 = dir == 1 ? d.JM - 1 : d.JM - 2;
+      const int n2 = dir == 2 ? d.KM - 1 : d.KM - 2;
+      const int first = dir == 0 ? 0 : (dir == 1 ? (d.IM - 1) * (d.JM - 2) * (d.KM - 2)
+                                                 : (d.IM - 1) * (d.JM - 2) * (d.KM - 2) +
+                                                       (d.IM - 2) * (d.JM - 1) * (d.KM - 2));
+      const int x0 = blockIdx.x * blockDim.x + threadIdx.x;
+      unsigned cnt = 0;
+      if (x2 < n2 && x0 < n0) {
+        const int y0 = blockIdx.y * DL, y1 = min(n1, y0 + DL);
+        for (int x1 = y0; x1 < y1; ++x1) cnt += __ldg(a.out + first + x0 + n0 * (x1 + n1 * x2));
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+      if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&a.st->weno_faces, (unsigned long long)cnt);
+    }
+    return;
+  }
   const Dims& d = a.d;
   const int IM = d.IM, JM = d.JM, KM = d.KM;
   const int dir = blockIdx.z / (KM - 1), x2 = blockIdx.z % (KM - 1);
@@ -219,7 +241,7 @@ __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) 
                                              : (IM - 1) * (JM - 2) * (KM - 2) + (IM - 2) * (JM - 1) * (KM - 2));
   if (x2 >= n2) return;  // uniform per CTA
   const bool valid = x0 < n0;
-  const int w = a.dim == dir ? SN_DILATE_ALONG : SN_DILATE_ACROSS;
+  const int w = a.dim == dir ? a.along : a.across;
   const int len = a.dim == 0 ? n0 : (a.dim == 1 ? n1 : n2);
   const int stride = a.dim == 0 ? 1 : (a.dim == 1 ? n0 : n0 * n1);
   unsigned cnt = 0;
@@ -233,11 +255,8 @@ __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) 
       const int e = first + x0 + n0 * (x1 + n1 * x2);
       const int pos = a.dim == 0 ? x0 : (a.dim == 1 ? x1 : x2);
       unsigned char dec = 0;
-#pragma unroll
-      for (int o = -2; o <= 2; ++o) {
-        const int p = pos + o;
-        if (o >= -w && o <= w && p >= 0 && p < len) dec |= __ldg(in + e + o * stride);
-      }
+      const int lo = max(-w, -pos), hi = min(w, len - 1 - pos);
+      for (int o = lo; o <= hi; ++o) dec |= __ldg(in + e + o * stride);
       out[e] = dec;
       cnt += dec;
     }

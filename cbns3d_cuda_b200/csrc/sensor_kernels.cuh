@@ -29,6 +29,7 @@ struct MaskArgs {
   const double* area[10];
   const float* params;      // CBNS_SENSOR_NPARAM floats (device)
   float tau;
+  unsigned every;           // evaluate on steps with steps % every == 1 % every (1: always)
   unsigned char* mask;      // one byte per face
   StepState* st;            // statistics, failure flag, done flag
   int check_done;
@@ -42,17 +43,24 @@ struct MaskArgs {
 // curved front (a blast) reaches grid lines next to those it crossed at the
 // step's start, so those faces stay on WENO5 for the step's three stages.
 // Three separable passes (one per index direction); the last one counts the
-// WENO5 faces.
-constexpr int SN_DILATE_ALONG = 2, SN_DILATE_ACROSS = 1;
+// WENO5 faces.  When the network runs only every n-th step, its decisions
+// must hold for n steps: widths 1 + n along and n across.
 struct DilateArgs {
   Dims d;
   const unsigned char* in;
   unsigned char* out;
   int dim;                 // index direction of this pass: 0 = i, 1 = j, 2 = k
+  int along, across;       // widening widths (faces)
   StepState* st;           // WENO5 faces are counted when count != 0
   int count;
+  unsigned every;          // as MaskArgs::every; the count is kept every step
   int check_done;
 };
+
+// true when the sensor is evaluated in the current step (steps counts from 1)
+__device__ __forceinline__ bool sensor_step(const StepState* st, unsigned every) {
+  return every <= 1 || st->steps % every == 1;
+}
 
 // Audit of the decisions: on the runs of 128 consecutive faces with
 // (e / 128) % stride == steps % stride, the faces the sensor sent to the linear

@@ -109,7 +109,7 @@ __device__ __forceinline__ bool classify(SweepCtx& c, int t, const float f[SN_IN
 // launches, so that each path gets its own register allocation).
 template <int KIND>
 __global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(const MaskArgs a) {
-  if (a.check_done && a.st->done) return;
+  if ((a.check_done && a.st->done) || !sensor_step(a.st, a.every)) return;
   extern __shared__ unsigned char raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
   tc::Smem& s = *reinterpret_cast<tc::Smem*>(base);

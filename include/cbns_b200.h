@@ -204,7 +204,8 @@ int cbns_mlp_predict(const float* params_dev, const float* x_dev, unsigned n, fl
  * The WENO5 decisions are then widened, per face direction, by 2 faces along
  * the face's own grid line and 1 face in the two other index directions (a
  * discontinuity moves less than a cell per step), and hold for the three
- * stages of the step.  An audit recomputes,
+ * stages of the step (see cbns_sensor_interval for runs that evaluate the
+ * network every n-th step).  An audit recomputes,
  * on the linear faces whose run of 128 consecutive global face indices r =
  * index / 128 has r % audit_stride equal to step % audit_stride, both
  * fluxes; a relative difference above audit_bound
@@ -212,6 +213,13 @@ int cbns_mlp_predict(const float* params_dev, const float* x_dev, unsigned n, fl
  * precision HYBRID refuses to step (CBNS_ERR_STATE) until cbns_sensor_load.
  * params_host: CBNS_SENSOR_NPARAM floats in host memory. */
 int cbns_sensor_load(cbns_ctx* ctx, const float* params_host, float tau);
+/* Evaluate the network on every n-th step of cbns_run / cbns_run_async (1 <=
+ * n <= 8, default 2; the first step of each run always evaluates); in between,
+ * the decisions of the last evaluation hold, widened by 1 + n faces along and
+ * n faces across (a discontinuity moves less than a cell per step).  The
+ * audit runs every step.  The per-call path (cbns_update_rk3 stage 1,
+ * cbns_eval_rhs) evaluates the network on every call, with n = 1 widths. */
+int cbns_sensor_interval(cbns_ctx* ctx, unsigned every);
 /* audit_stride >= 1 (1 audits every linear face every step); audit_bound > 0
  * (relative to the face's largest flux component).  Defaults 97 and 1e-2. */
 int cbns_sensor_audit(cbns_ctx* ctx, unsigned audit_stride, float audit_bound);

@@ -230,6 +230,32 @@ def test_trained_sensor_sweep_matches_sampled_faces():
     assert 0 < m.sum() < m.size
 
 
+def test_sensor_interval_holds_and_widens_decisions():
+    """With the network evaluated every 3rd step, a 3-step run uses the first
+    step's decisions, widened by 4 along and 3 across, for all three steps."""
+    c = cases.case_shock_vortex(40, 36, 12)
+    h = _block(c, PREC_HYBRID, _constant_sensor(0.0), audit=(97, 1.0e30))
+    P = _jump_sensor(h)
+    h.sensor_load(P, 0.5)
+    h.sensor_interval(3)
+    X, _y, _d, idx = sensor.sample_faces(h, with_dev=True)  # the initial state
+    p = sensor.predict(torch.from_numpy(P).cuda(), X, tensor_cores=True).cpu().numpy()
+    idx = idx.cpu().numpy()
+    h.sensor_stats_reset()
+    h.set_time(0.0)
+    assert h.run(3) == 3
+    m, forced = h.sensor_mask()
+    near = np.zeros(m.size, bool)
+    near[idx] = np.abs(p - 0.5) < 1e-4
+    want = np.zeros(m.size, np.uint8)
+    want[idx] = (p >= 0.5) & ~_flat(X)
+    lo, hi = _widen(want & ~near, c.shape, 4, 3), _widen(want | near, c.shape, 4, 3)
+    assert not forced and np.all((m >= lo) & (m <= hi))
+    assert h.sensor_stats()["weno_faces"] == 3 * int(m.sum())
+    with pytest.raises(CbnsError):
+        h.sensor_interval(0)
+
+
 def test_steps_match_oracle_under_gpu_decisions():
     c = cases.case_shock_vortex(40, 36, 12)
     h = _block(c, PREC_HYBRID, _constant_sensor(0.0), audit=(1, 1.0e30))

@@ -49,6 +49,13 @@ sys.path.insert(0, str(ROOT))
 # bytes per cell-update the kernel must move: per stage the stage input (40 B),
 # the metrics (80 B) and the output (40 B), plus the RK base in stages 2 and 3
 ALG_BYTES_PER_UPDATE = 560.0
+# FP64 FLOP the plain path executes per cell-update (dadd + dmul + 2 dfma, ncu
+# counters of a stage-2 launch: 4,660 per node, times three stages;
+# profiles/stage_kernel_128x128x64.md), and the B200's FP64 peak: 64 DFMA lanes
+# per SM x 148 SMs x 2 FLOP x 1.965 GHz (ncu's peak_sustained of
+# sm__sass_thread_inst_executed_op_dfma_pred_on, at the maximum SM clock)
+FP64_FLOP_PER_UPDATE = 13980.0
+FP64_PEAK_TFLOPS = 64 * 148 * 2 * 1.965e9 / 1e12
 
 
 def args():
@@ -319,12 +326,19 @@ def run_ours(a):
     st_ms, st_n = kernh[0]
     alg_per_launch = ALG_BYTES_PER_UPDATE / 3.0 * N
     achieved = alg_per_launch / (st_ms / st_n / 1e3) / 1e9 if st_n else None
-    traffic = None
+    traffic = traffic64 = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         t = json.loads(tf.read_text())
         if "hybrid_stage_bytes_per_update" in t:
             traffic = t["hybrid_stage_bytes_per_update"] / 3.0 * N
+        if "fp64_stage_bytes_per_update" in t:
+            traffic64 = t["fp64_stage_bytes_per_update"] / 3.0 * N
+    # the plain path's stage kernel: HBM and FP64-pipe fractions
+    st64_ms, st64_n = kern64[0]
+    st64_launch_s = st64_ms / max(st64_n, 1) / 1e3
+    ach64 = alg_per_launch / st64_launch_s / 1e9 if st64_n else None
+    tfl64 = FP64_FLOP_PER_UPDATE / 3.0 * N / st64_launch_s / 1e12 if st64_n else None
 
     def kern_ms(k):
         return {name: {"ms_per_step": k[i][0] / K, "launches_per_step": k[i][1] / K}
@@ -346,7 +360,13 @@ def run_ours(a):
                        "l2": "inputs larger than L2 (3 state buffers + 10 metric arrays)",
                        "sensor": {"weights": os.path.relpath(a.sensor, ROOT), "tau": SENSOR[1]}},
             "rho_l2_vs_fp64": l2_h, "rho_linf_vs_fp64": linf_h,
-            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "kernels": kern_ms(kern64)},
+            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "kernels": kern_ms(kern64),
+                               "roofline_hbm": {"achieved": ach64, "peak": peak, "unit": "GB/s",
+                                                "frac": (ach64 / peak) if ach64 else None, "traffic": traffic64},
+                               "roofline_fp64": {"achieved": tfl64, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
+                                                 "frac": (tfl64 / FP64_PEAK_TFLOPS) if tfl64 else None,
+                                                 "flop_per_update": FP64_FLOP_PER_UPDATE,
+                                                 "peak_kind": "nominal (ncu DFMA peak x max SM clock)"}},
                       "split": {"value": value32, "ms_per_step": ms32 / K, "rho_l2_vs_fp64": l2_32,
                                 "rho_linf_vs_fp64": linf_32, "stage_variant": variant32,
                                 "kernels": kern_ms(kern32)},

@@ -91,6 +91,7 @@ SIGNATURES = [
     ("cbns_mlp_adam", C.c_int, [_V, _V, _V, _V, C.c_uint, C.c_float, _V]),
     ("cbns_mlp_predict", C.c_int, [_V, _V, C.c_uint, _V, C.c_int, _V, _V]),
     ("cbns_sensor_load", C.c_int, [_V, C.POINTER(C.c_float), C.c_float]),
+    ("cbns_sensor_load_file", C.c_int, [_V, C.c_char_p]),
     ("cbns_sensor_audit", C.c_int, [_V, C.c_uint, C.c_float]),
     ("cbns_sensor_interval", C.c_int, [_V, C.c_uint]),
     ("cbns_sensor_stats_get", C.c_int, [_V, C.POINTER(SensorStats)]),

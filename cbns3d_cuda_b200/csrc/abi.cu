@@ -873,6 +873,28 @@ int cbns_sensor_load(cbns_ctx* c, const float* params, float tau) {
   return sync(c);
 }
 
+int cbns_sensor_load_file(cbns_ctx* c, const char* path) {
+  if (!c || !path) return CBNS_ERR_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) {
+    g_last = "cannot open the sensor weights file";
+    return CBNS_ERR_ARG;
+  }
+  char magic[8];
+  unsigned n = 0;
+  float tau = 0.f;
+  std::vector<float> p(CBNS_SENSOR_NPARAM);
+  const bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "CBNSSNS1", 8) == 0 &&
+                  std::fread(&n, 4, 1, f) == 1 && n == CBNS_SENSOR_NPARAM && std::fread(&tau, 4, 1, f) == 1 &&
+                  std::fread(p.data(), 4, CBNS_SENSOR_NPARAM, f) == CBNS_SENSOR_NPARAM;
+  std::fclose(f);
+  if (!ok) {
+    g_last = "malformed sensor weights file";
+    return CBNS_ERR_ARG;
+  }
+  return cbns_sensor_load(c, p.data(), tau);
+}
+
 int cbns_sensor_audit(cbns_ctx* c, unsigned stride, float bound) {
   if (!c || stride == 0 || !(bound > 0.f)) return CBNS_ERR_ARG;
   c->audit_stride = stride;

@@ -63,6 +63,7 @@ void copy_block_info(const Block3dInfo* block_info) {
 void allocate_mem(const Block3dInfo* block_info, Block3dData* block_data) {
   const cbns_params p = params_of(block_info);
   SHIM_CHECK(cbns_create(&p, &block_data->ctx));
+  if (p.precision == CBNS_PREC_HYBRID) SHIM_CHECK(cbns_sensor_load_file(block_data->ctx, block_info->sensor_weights));
   block_data->Q = reinterpret_cast<value_type*>(&g_tag_q);
   block_data->Q_p = reinterpret_cast<value_type*>(&g_tag_qp);
 }

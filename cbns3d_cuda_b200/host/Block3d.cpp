@@ -59,6 +59,7 @@ void Block3d::read_input() {
   info_.is_viscous = opt_.viscous;
   info_.precision = opt_.precision;
   info_.vis_divergence = opt_.vis_divergence;
+  info_.sensor_weights = opt_.sensor.empty() ? nullptr : opt_.sensor.c_str();
 }
 
 // ASCII Plot3D single block: IM JM KM, then x, y, z with i fastest (src/Block3d.cpp:151-202).

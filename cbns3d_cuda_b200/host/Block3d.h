@@ -19,6 +19,7 @@ class Block3d {
     int vis_divergence = CBNS_VISDIV_REFERENCE;
     int viscous = CBNS_SHIM_VISCOUS_DEFAULT;
     std::string input = "input.txt";
+    std::string sensor = "";  // learned-sensor weights (precision hybrid)
   };
 
   explicit Block3d(const Options& o) : opt_(o) {}

@@ -3,10 +3,15 @@
 // directory like the reference.
 //   --quiet          no per-step output line
 //   --graph          whole steps replayed from a CUDA graph, dt on the device
-//   --precision P    fp64 (default) | split
+//   --precision P    fp64 (default) | split | hybrid
+//   --sensor FILE    learned-sensor weights for the hybrid (default: the
+//                    trained weights shipped beside this executable,
+//                    ../data/sensor_weights.bin)
 //   --visdiv D       reference (default) | centered
 //   --inviscid / --viscous   override the build-time default
 //   --input FILE     parameter file (default input.txt)
+#include <unistd.h>
+
 #include <cstring>
 #include <iostream>
 #include <string>
@@ -31,13 +36,27 @@ int main(int argc, char** argv) {
     else if (s == "--input") o.input = next();
     else if (s == "--precision") {
       const std::string v = next();
-      o.precision = v == "split" ? CBNS_PREC_SPLIT : CBNS_PREC_FP64;
+      o.precision = v == "split" ? CBNS_PREC_SPLIT : (v == "hybrid" ? CBNS_PREC_HYBRID : CBNS_PREC_FP64);
+    } else if (s == "--sensor") {
+      o.sensor = next();
     } else if (s == "--visdiv") {
       o.vis_divergence = next() == "centered" ? CBNS_VISDIV_CENTERED : CBNS_VISDIV_REFERENCE;
     } else {
       std::cerr << "unknown option " << s << "\n";
       return 2;
     }
+  }
+  if (o.precision == CBNS_PREC_HYBRID && o.sensor.empty()) {
+    // the weights shipped with the library: <package>/data, the executable in <package>/bin
+    char exe[4096];
+    const ssize_t n = readlink("/proc/self/exe", exe, sizeof(exe) - 1);
+    std::string dir = ".";
+    if (n > 0) {
+      exe[n] = 0;
+      dir = std::string(exe);
+      dir = dir.substr(0, dir.find_last_of('/'));
+    }
+    o.sensor = dir + "/../data/sensor_weights.bin";
   }
   Block3d block(o);
   return block.solve();

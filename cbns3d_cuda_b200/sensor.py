@@ -120,6 +120,16 @@ def train(X, Y, epochs=3, batch=16384, lr=3e-3, pos_weight=None, seed=0, params=
     return P, hist
 
 
+def save_weights_bin(path, params, tau):
+    """The weights file cbns_sensor_load_file reads: "CBNSSNS1", uint32 1601,
+    float32 tau, 1601 float32 parameters (little endian)."""
+    import struct
+    p = np.ascontiguousarray(params, dtype="<f4").reshape(-1)
+    assert p.size == NPARAM
+    with open(path, "wb") as f:
+        f.write(b"CBNSSNS1" + struct.pack("<If", NPARAM, float(tau)) + p.tobytes())
+
+
 def choose_threshold(prob, Y, recall=0.995):
     """Smallest threshold whose recall of WENO-needing faces is at least `recall`
     (faces at or above it take WENO: uncertain faces fall back to WENO)."""

@@ -2,6 +2,9 @@
 
     python -m cbns3d_cuda_b200.train_sensor --out cbns3d_cuda_b200/data/sensor_weights.npz
 
+writes the weights as .npz (parameters, tau, a JSON summary of the run) and as
+the .bin file the C ABI and the host driver read (cbns_sensor_load_file).
+
 Data: solver states of three flows, run with the split-precision path and
 sampled every few steps: the isentropic vortex on the perturbed box (64 x 32 x
 16), the spherical blast on the stretched, skewed box (96^3) and the Mach 1.2
@@ -155,7 +158,9 @@ def main(argv=None):
     log(json.dumps(summary))
     np.savez(args.out, params=params, tau=np.float32(tau),
              summary=np.array(json.dumps(summary)))
-    log(f"wrote {args.out}")
+    binp = str(args.out).rsplit(".", 1)[0] + ".bin"
+    sensor.save_weights_bin(binp, params, tau)
+    log(f"wrote {args.out} and {binp}")
 
 
 if __name__ == "__main__":

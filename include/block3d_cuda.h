@@ -90,6 +90,9 @@ struct Block3dInfo {
   int is_viscous = CBNS_SHIM_VISCOUS_DEFAULT;
   int precision = CBNS_PREC_FP64;
   int vis_divergence = CBNS_VISDIV_REFERENCE;
+  /* weights file of the learned sensor (cbns_sensor_load_file), required when
+   * precision is CBNS_PREC_HYBRID */
+  const char* sensor_weights = nullptr;
 };
 
 struct Block3dData {

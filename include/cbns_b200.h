@@ -213,6 +213,11 @@ int cbns_mlp_predict(const float* params_dev, const float* x_dev, unsigned n, fl
  * precision HYBRID refuses to step (CBNS_ERR_STATE) until cbns_sensor_load.
  * params_host: CBNS_SENSOR_NPARAM floats in host memory. */
 int cbns_sensor_load(cbns_ctx* ctx, const float* params_host, float tau);
+/* The same from a weights file: 8 bytes "CBNSSNS1", uint32 CBNS_SENSOR_NPARAM,
+ * float32 tau, CBNS_SENSOR_NPARAM float32 parameters (little endian), as
+ * written by cbns3d_cuda_b200/train_sensor.py.  CBNS_ERR_ARG if the file is
+ * missing or malformed. */
+int cbns_sensor_load_file(cbns_ctx* ctx, const char* path);
 /* Evaluate the network on every n-th step of cbns_run / cbns_run_async (1 <=
  * n <= 8, default 2; the first step of each run always evaluates); in between,
  * the decisions of the last evaluation hold, widened by 1 + n faces along and

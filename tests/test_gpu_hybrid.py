@@ -305,6 +305,37 @@ def test_audit_rotating_sample_and_pass():
     assert h.sensor_stats()["audit_faces"] == 0
 
 
+def test_weights_file_and_driver():
+    """cbns_sensor_load_file gives the same decisions as the parameters loaded
+    from memory, and the host driver runs the hybrid from its input files."""
+    import subprocess
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    w = np.load(root / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz")
+    c = cases.case_shock_vortex(48, 48, 12)
+    a = _block(c, PREC_HYBRID, w["params"].astype(np.float32), float(w["tau"]))
+    b = _setup(Block(make_params(*c.shape, **c.params, precision=PREC_HYBRID)), c)
+    from cbns3d_cuda_b200 import _abi
+    _abi.check(b.lib.cbns_sensor_load_file(b.h, str(root / "cbns3d_cuda_b200" / "data" / "sensor_weights.bin").encode()),
+               "cbns_sensor_load_file")
+    assert np.array_equal(a.eval_rhs(CBNS_Q), b.eval_rhs(CBNS_Q))
+    assert np.array_equal(a.sensor_mask()[0], b.sensor_mask()[0])
+    with pytest.raises(CbnsError):
+        _abi.check(b.lib.cbns_sensor_load_file(b.h, b"/nonexistent/weights.bin"), "cbns_sensor_load_file")
+    exe = root / "cbns3d_cuda_b200" / "bin" / "cbns3d_b200"
+    tmp = Path(__import__("tempfile").mkdtemp())
+    outs = {}
+    for prec in ("fp64", "hybrid"):
+        d = c.write(tmp / prec, nsteps=20, checkpoint_freq=20)
+        r = subprocess.run([str(exe), "--quiet", "--graph", "--inviscid", "--precision", prec], cwd=d,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+        outs[prec] = cases.read_checkpoint(d / "checkpoint.dat")[1]
+    r64 = interior(outs["fp64"], c.shape)[..., 0]
+    rh = interior(outs["hybrid"], c.shape)[..., 0]
+    assert 0 < np.sqrt(np.mean((rh - r64) ** 2) / np.mean(r64 ** 2)) <= 1e-4
+
+
 def test_hybrid_needs_sensor_and_rejects_bad_arguments():
     c = cases.case_vortex(20, 14, 10)
     h = _setup(Block(make_params(*c.shape, **c.params, precision=PREC_HYBRID)), c)

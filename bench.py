@@ -64,7 +64,8 @@ def args():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--case", default="shock_vortex", choices=["shock_vortex", "blast", "vortex"])
+    ap.add_argument("--case", default="shock_vortex", choices=["shock_vortex", "blast", "vortex", "batch"])
+    ap.add_argument("--blocks", type=int, default=64, help="--case batch: number of blocks (configs[4]: 64)")
     ap.add_argument("--size", default=None, help="IMxJMxKM (default: the case's config size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -433,9 +434,90 @@ def run_reference(a):
     }))
 
 
+def run_batch(a):
+    """independent viscous blocks of uneven size (seeded draw),
+    learned-sensor hybrid, advanced by one persistent work-queue launch of the
+    stage kernel per RK stage (cbns_batch_run) with per-block dt; beside it the
+    same blocks stepped one after the other on the same stream (one CUDA graph
+    per block).  Both timed with CUDA events on that stream."""
+    import torch
+    from cbns3d_cuda_b200 import CBNS_Q, PREC_HYBRID, Batch, Block, cases, make_params
+    torch.cuda.set_device(0)
+    load_sensor(a.sensor)
+    cs, draw = cases.case_batch(a.blocks, seed=0)
+    K, W = a.steps, a.warmup
+    N = sum((c.shape[0] - 2) * (c.shape[1] - 2) * (c.shape[2] - 2) for c in cs)
+
+    def make():
+        out = []
+        for c in cs:
+            b = Block(make_params(*c.shape, **c.params, precision=PREC_HYBRID))
+            b.calc_metrics(c.x, c.y, c.z)
+            b.set_conservative(c.Q0)
+            b.calc_primitive(CBNS_Q)
+            b.set_bc_calc_primitive(CBNS_Q)
+            b.calc_viscous_terms()
+            b.sensor_load(*SENSOR)
+            b.set_time(0.0)
+            out.append(b)
+        return out
+
+    stream = torch.cuda.Stream()  # every launch of both passes goes to this stream
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    blocks = make()
+    bt = Batch(blocks, stream.cuda_stream)
+    bt.run(W)
+    clk = Clocks(0)
+    clk.__enter__()
+    ms_batch = timed(lambda: bt.run_async(K))
+    clk.__exit__(None, None, None)
+    clocks = clk.summary()
+    bt.close()
+    for b in blocks:
+        b.close()
+    blocks = make()
+    for b in blocks:
+        b.set_stream(stream.cuda_stream)
+        b.run(W)
+
+    def one_by_one():
+        for b in blocks:
+            b.run_async(K)
+
+    ms_alone = timed(one_by_one)
+    for b in blocks:
+        b.close()
+    value = N * K / (ms_batch / 1e3)
+    print(json.dumps({
+        "metric": "cell-updates/s: learned-hybrid FP32 vs plain FP64 WENO5, same B200, rho-L2<=1e-5",
+        "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": K, "warmup": W,
+        "ms_per_step": ms_batch / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 flux / f64 state", "data": "synthetic",
+        "config": {"workload": f"configs[4]: {len(cs)} viscous blocks, sizes 32^3..128x64x64 (seed 0), "
+                               "Mach U[0.3,2], Re U[1e3,1e5], learned-sensor hybrid, per-block dt",
+                   "cell_updates_per_step": N, "blocks": len(cs),
+                   "shapes": [d["shape"] for d in draw]},
+        "paths": {"batch": {"value": value, "ms_per_step": ms_batch / K},
+                  "blocks_one_by_one": {"value": N * K / (ms_alone / 1e3), "ms_per_step": ms_alone / K},
+                  "batch_over_one_by_one": ms_alone / ms_batch},
+        "clocks": clocks,
+    }))
+
+
 if __name__ == "__main__":
     a = args()
     if a.impl == "reference":
         run_reference(a)
+    elif a.case == "batch":
+        run_batch(a)
     else:
         run_ours(a)

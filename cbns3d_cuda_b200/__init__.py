@@ -15,7 +15,7 @@ from . import _abi
 from ._abi import (CBNS_Q, CBNS_QP, PREC_FP64, PREC_HYBRID, PREC_SPLIT, VISDIV_CENTERED,  # noqa: F401
                    VISDIV_REFERENCE, CbnsError, Params)
 
-__all__ = ["Block", "Params", "CbnsError", "CBNS_Q", "CBNS_QP", "PREC_FP64", "PREC_SPLIT", "PREC_HYBRID",
+__all__ = ["Block", "Batch", "Params", "CbnsError", "CBNS_Q", "CBNS_QP", "PREC_FP64", "PREC_SPLIT", "PREC_HYBRID",
            "VISDIV_REFERENCE", "VISDIV_CENTERED", "make_params"]
 
 NG = 2
@@ -217,6 +217,48 @@ class Block:
         n = C.c_ulonglong()
         _abi.check(self.lib.cbns_launch_count(self.h, C.byref(n)), "cbns_launch_count")
         return n.value
+
+
+class Batch:
+    """Independent blocks advanced together (cbns_batch_*): one persistent
+    work-queue launch of the stage kernel per RK stage for all blocks, per-block
+    dt, a whole step as one CUDA graph.  The blocks stay usable on their own
+    (get_conservative, ...); close the batch before them."""
+
+    def __init__(self, blocks, stream_ptr: int | None = None):
+        self.lib = _abi.load()
+        self.blocks = list(blocks)
+        arr = (C.c_void_p * len(self.blocks))(*[b.h.value if isinstance(b.h, C.c_void_p) else b.h
+                                                 for b in self.blocks])
+        h = C.c_void_p()
+        _abi.check(self.lib.cbns_batch_create(arr, len(self.blocks), C.c_void_p(stream_ptr or 0), C.byref(h)),
+                   "cbns_batch_create")
+        self.h = h
+
+    def run(self, nsteps: int, t_end: float = 1.0e30) -> int:
+        n = C.c_uint()
+        _abi.check(self.lib.cbns_batch_run(self.h, int(nsteps), float(t_end), C.byref(n)), "cbns_batch_run")
+        return n.value
+
+    def run_async(self, nsteps: int, t_end: float = 1.0e30):
+        _abi.check(self.lib.cbns_batch_run_async(self.h, int(nsteps), float(t_end)), "cbns_batch_run_async")
+
+    def close(self):
+        if getattr(self, "h", None):
+            _abi.check(self.lib.cbns_batch_destroy(self.h), "cbns_batch_destroy")
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def calc_gradient(f: np.ndarray):

@@ -92,6 +92,10 @@ SIGNATURES = [
     ("cbns_mlp_predict", C.c_int, [_V, _V, C.c_uint, _V, C.c_int, _V, _V]),
     ("cbns_sensor_load", C.c_int, [_V, C.POINTER(C.c_float), C.c_float]),
     ("cbns_sensor_load_file", C.c_int, [_V, C.c_char_p]),
+    ("cbns_batch_create", C.c_int, [C.POINTER(_V), C.c_uint, _V, C.POINTER(_V)]),
+    ("cbns_batch_destroy", C.c_int, [_V]),
+    ("cbns_batch_run", C.c_int, [_V, C.c_uint, C.c_double, C.POINTER(C.c_uint)]),
+    ("cbns_batch_run_async", C.c_int, [_V, C.c_uint, C.c_double]),
     ("cbns_sensor_audit", C.c_int, [_V, C.c_uint, C.c_float]),
     ("cbns_sensor_interval", C.c_int, [_V, C.c_uint]),
     ("cbns_sensor_stats_get", C.c_int, [_V, C.POINTER(SensorStats)]),

@@ -287,6 +287,34 @@ def case_blast(IM=384, JM=384, KM=384, t_end=0.05, CFL=0.5):
     return Case("blast", x, y, z, params, Q, t_end=t_end, nsteps=100000)
 
 
+def case_batch(nblocks=64, seed=0, size_lo=(32, 32, 32), size_hi=(128, 64, 64), viscous=True, CFL=0.5):
+    """independent blocks for the batched form.  Per block (seeded
+    draw): grid points uniform in size_lo..size_hi per dimension, free-stream
+    Mach uniform in [0.3, 2.0], Reynolds number uniform in [1e3, 1e5], an
+    isentropic vortex of strength uniform in [1, 5] at a random position of
+    the middle half of the perturbed 10 x 5 x 2.5 box; viscous by default.
+    Boundaries as configs[0] (the reference's modes: i faces pressure-reset
+    extrapolation, j faces held at the initial state, k faces zero-gradient).
+    Returns the list of Cases and the draw."""
+    rng = np.random.default_rng(seed)
+    out, draw = [], []
+    for b in range(nblocks):
+        IM, JM, KM = (int(rng.integers(lo, hi + 1)) for lo, hi in zip(size_lo, size_hi))
+        Mach = float(rng.uniform(0.3, 2.0))
+        Re = float(rng.uniform(1.0e3, 1.0e5))
+        beta = float(rng.uniform(1.0, 5.0))
+        xc, yc = float(rng.uniform(2.5, 7.5)), float(rng.uniform(1.25, 3.75))
+        x, y, z = perturbed_box(IM, JM, KM)
+        xg, yg = ghost_extend(x), ghost_extend(y)
+        g = 1.4
+        Q = conservative(*isentropic_vortex(xg, yg, Mach, beta, xc, yc, 1.0, g), g)
+        params = dict(CFL=CFL, Mach=Mach, gamma=g, i_begin=1, i_end=0, Re=Re, Pr=0.72, T_inf=288.15,
+                      viscous=viscous)
+        out.append(Case(f"batch{b}", x, y, z, params, Q, t_end=1.0e30, nsteps=500))
+        draw.append(dict(shape=(IM, JM, KM), Mach=Mach, Re=Re, beta=beta, centre=(xc, yc)))
+    return out, draw
+
+
 def case_shock_vortex(IM=256, JM=256, KM=128, nsteps=100, CFL=0.5, Ms=1.2, eps=0.3, rc=0.075):
     """a stationary Mach 1.2 normal shock at x = 0.5 of the 5%-skewed
     [0,1]x[0,1]x[0,0.5] box, with an isentropic vortex (strength 0.3, radius

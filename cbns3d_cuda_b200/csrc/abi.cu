@@ -378,6 +378,160 @@ int check_flux_ready(cbns_ctx* c) {
   return CBNS_OK;
 }
 
+// Start of a run: the step counter, finish and NaN flags reset, t_end set,
+// and the spectral-radius maximum of the current state available.
+int run_prepare(cbns_ctx* c, double t_end) {
+  RET(check_flux_ready(c));
+  StepState h;
+  CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  RET(sync(c));
+  h.t_end = t_end;
+  h.done = 0;
+  h.nan_dt = 0;
+  h.steps = 0;
+  CK(cudaMemcpyAsync(c->st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  RET(sync(c));
+  if (!c->sigma_valid) {
+    RET(sigma_launch(c));
+    c->sigma_valid = true;
+  }
+  return CBNS_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- batches
+struct cbns_batch {
+  std::vector<cbns_ctx*> blk;
+  cudaStream_t stream = nullptr;           // the caller's, or owned by the batch
+  bool own_stream = false;
+  std::vector<cudaStream_t> saved;         // the blocks' streams before the batch
+  bool visc = false, fp32 = false, hyb = false;
+  StageArgs* args = nullptr;  // device: 3 stages x nblocks
+  int* start = nullptr;       // device: nblocks + 1
+  unsigned* counter = nullptr;
+  int total = 0;
+  std::vector<int> roles;     // (lq, lp, ls) per block at capture
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+};
+
+namespace {
+
+void batch_drop_graph(cbns_batch* b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->gexec = nullptr;
+  b->graph = nullptr;
+}
+
+// The StageArgs of the three stages of every block for the fixed buffer roles
+// P0 = Q, P1 = spare, P2 = Q_p (as enqueue_step), uploaded to the device.
+int batch_tables(cbns_batch* b) {
+  const int nb = (int)b->blk.size();
+  std::vector<StageArgs> tab(3 * nb);
+  std::vector<int> start(nb + 1, 0);
+  b->roles.clear();
+  for (int i = 0; i < nb; ++i) {
+    cbns_ctx* c = b->blk[i];
+    double* P0 = c->qb[c->lq];
+    double* P1 = c->qb[c->ls];
+    double* P2 = c->qb[c->lp];
+    tab[0 * nb + i] = stage_args(c, P0, P0, P0, P1, false);
+    tab[1 * nb + i] = stage_args(c, P1, P0, P1, P2, false);
+    tab[2 * nb + i] = stage_args(c, P2, P0, P2, P0, !b->visc);
+    start[i + 1] = start[i] + c->ntile_i * c->ntile_j * ((c->d.KM - 2 + c->kchunk - 1) / c->kchunk);
+    b->roles.insert(b->roles.end(), {c->lq, c->lp, c->ls});
+  }
+  b->total = start[nb];
+  CK(cudaMemcpyAsync(b->args, tab.data(), tab.size() * sizeof(StageArgs), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaStreamSynchronize(b->stream));
+  return CBNS_OK;
+}
+
+// One SSP-RK3 step of every block: per-block prologue (own dt) and sensor,
+// then per stage one persistent launch over all blocks' tiles followed by the
+// blocks' boundary (and viscous) kernels.
+int batch_enqueue_step(cbns_batch* b) {
+  const int nb = (int)b->blk.size();
+  for (cbns_ctx* c : b->blk) {
+    CK(launch_step_prologue(c->st, c->ph.CFL, b->stream));
+    c->launches += 1;
+    if (b->hyb) RET(sensor_launch(c, c->qb[c->lq], true));
+  }
+  for (int k = 0; k < 3; ++k) {
+    const bool last = k == 2;
+    CK(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), b->stream));
+    BatchStage bs;
+    bs.args = b->args + k * nb;
+    bs.start = b->start;
+    bs.nblocks = nb;
+    bs.total = b->total;
+    bs.counter = b->counter;
+    CK(launch_stage_batched(bs, k + 1, b->visc, b->fp32, b->hyb, b->stream));
+    b->blk[0]->launches += 1;
+    for (cbns_ctx* c : b->blk) {
+      double* out = k == 0 ? c->qb[c->ls] : (k == 1 ? c->qb[c->lp] : c->qb[c->lq]);
+      RET(bc_launch(c, bc_args(c, out, true, last && !b->visc), false));
+      if (b->visc) RET(visc_launch(c, visc_args(c, true, last)));
+    }
+  }
+  return CBNS_OK;
+}
+
+int batch_run(cbns_batch* b, unsigned nsteps, double t_end, bool wait, unsigned* steps_min) {
+  if (!b) return CBNS_ERR_ARG;
+  for (cbns_ctx* c : b->blk) RET(run_prepare(c, t_end));
+  bool stale = !b->gexec;
+  for (size_t i = 0; i < b->blk.size() && !stale; ++i) {
+    const cbns_ctx* c = b->blk[i];
+    stale = b->roles[3 * i] != c->lq || b->roles[3 * i + 1] != c->lp || b->roles[3 * i + 2] != c->ls;
+  }
+  if (stale) {
+    batch_drop_graph(b);
+    RET(batch_tables(b));
+    std::vector<unsigned long long> l0;
+    for (cbns_ctx* c : b->blk) l0.push_back(c->launches);
+    CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = batch_enqueue_step(b);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ee = cudaStreamEndCapture(b->stream, &g);
+    for (size_t i = 0; i < b->blk.size(); ++i) {
+      b->blk[i]->launches_per_step = (int)(b->blk[i]->launches - l0[i]);
+      b->blk[i]->launches = l0[i];
+    }
+    if (rc != CBNS_OK) {
+      if (g) cudaGraphDestroy(g);
+      return rc;
+    }
+    CK(ee);
+    b->graph = g;
+    CK(cudaGraphInstantiate(&b->gexec, g, 0));
+  }
+  for (unsigned n = 0; n < nsteps; ++n) {
+    CK(cudaGraphLaunch(b->gexec, b->stream));
+    for (cbns_ctx* c : b->blk) c->launches += c->launches_per_step;
+  }
+  for (cbns_ctx* c : b->blk)
+    if (c->ph.viscous) c->prims_of = c->lq;
+  if (!wait) return CBNS_OK;
+  CK(cudaStreamSynchronize(b->stream));
+  unsigned mn = ~0u;
+  bool nan = false;
+  for (cbns_ctx* c : b->blk) {
+    StepState h;
+    CK(cudaMemcpy(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost));
+    mn = std::min(mn, h.steps);
+    if (h.nan_dt) {
+      nan = true;
+      c->sigma_valid = false;
+    }
+  }
+  if (steps_min) *steps_min = mn;
+  return nan ? CBNS_ERR_NAN_DT : CBNS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -729,22 +883,7 @@ int cbns_get_time(cbns_ctx* c, double* t_cur, double* dt_last) {
 }
 
 static int run_impl(cbns_ctx* c, unsigned nsteps, double t_end, bool wait, unsigned* steps_done) {
-  RET(check_flux_ready(c));
-  {
-    StepState h;
-    CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-    RET(sync(c));
-    h.t_end = t_end;
-    h.done = 0;
-    h.nan_dt = 0;
-    h.steps = 0;
-    CK(cudaMemcpyAsync(c->st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
-    RET(sync(c));
-  }
-  if (!c->sigma_valid) {
-    RET(sigma_launch(c));
-    c->sigma_valid = true;
-  }
+  RET(run_prepare(c, t_end));
   if (c->prof) {
     for (unsigned n = 0; n < nsteps; ++n) RET(enqueue_step(c));
   } else {
@@ -1044,6 +1183,87 @@ int cbns_launch_count(cbns_ctx* c, unsigned long long* n) {
   if (!c || !n) return CBNS_ERR_ARG;
   *n = c->launches;
   return CBNS_OK;
+}
+
+int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, cbns_batch** out) {
+  if (!blocks || !out || nblocks == 0) return CBNS_ERR_ARG;
+  for (unsigned i = 0; i < nblocks; ++i) {
+    if (!blocks[i]) return CBNS_ERR_ARG;
+    for (unsigned j = 0; j < i; ++j)
+      if (blocks[j] == blocks[i]) return CBNS_ERR_ARG;
+    RET(check_flux_ready(blocks[i]));
+    if (blocks[i]->ph.viscous != blocks[0]->ph.viscous || blocks[i]->ph.precision != blocks[0]->ph.precision) {
+      g_last = "the blocks of a batch share the precision and the viscous flag";
+      return CBNS_ERR_ARG;
+    }
+  }
+  cbns_batch* b = new cbns_batch;
+  b->blk.assign(blocks, blocks + nblocks);
+  b->visc = blocks[0]->ph.viscous != 0;
+  b->fp32 = blocks[0]->ph.precision != CBNS_PREC_FP64;
+  b->hyb = blocks[0]->ph.precision == CBNS_PREC_HYBRID;
+  cudaError_t e = cudaSuccess;
+  if (stream) {
+    b->stream = static_cast<cudaStream_t>(stream);
+  } else {
+    e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      delete b;
+      g_last = "stream creation failed";
+      return CBNS_ERR_CUDA;
+    }
+    b->own_stream = true;
+  }
+  // every block works on the batch's stream while the batch exists
+  for (cbns_ctx* c : b->blk) {
+    b->saved.push_back(c->stream == c->own ? nullptr : c->stream);
+    const int rc = cbns_set_stream(c, b->stream);
+    if (rc != CBNS_OK) {
+      for (size_t i = 0; i + 1 < b->saved.size(); ++i) cbns_set_stream(b->blk[i], b->saved[i]);
+      if (b->own_stream) cudaStreamDestroy(b->stream);
+      delete b;
+      return rc;
+    }
+  }
+  e = cudaMalloc(&b->args, 3 * nblocks * sizeof(StageArgs));
+  if (e == cudaSuccess) e = cudaMalloc(&b->start, (nblocks + 1) * sizeof(int));
+  if (e == cudaSuccess) e = cudaMalloc(&b->counter, sizeof(unsigned));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(b->args);
+    cudaFree(b->start);
+    cudaFree(b->counter);
+    for (size_t i = 0; i < b->blk.size(); ++i) cbns_set_stream(b->blk[i], b->saved[i]);
+    if (b->own_stream) cudaStreamDestroy(b->stream);
+    delete b;
+    g_last = "device allocation failed";
+    return CBNS_ERR_NOMEM;
+  }
+  *out = b;
+  return CBNS_OK;
+}
+
+int cbns_batch_destroy(cbns_batch* b) {
+  if (!b) return CBNS_ERR_ARG;
+  cudaStreamSynchronize(b->stream);
+  batch_drop_graph(b);
+  // the blocks go back to the streams they had
+  for (size_t i = 0; i < b->blk.size(); ++i) cbns_set_stream(b->blk[i], b->saved[i]);
+  cudaFree(b->args);
+  cudaFree(b->start);
+  cudaFree(b->counter);
+  if (b->own_stream) cudaStreamDestroy(b->stream);
+  delete b;
+  return CBNS_OK;
+}
+
+int cbns_batch_run(cbns_batch* b, unsigned nsteps, double t_end, unsigned* steps_min) {
+  return batch_run(b, nsteps, t_end, true, steps_min);
+}
+
+int cbns_batch_run_async(cbns_batch* b, unsigned nsteps, double t_end) {
+  return batch_run(b, nsteps, t_end, false, nullptr);
 }
 
 }  // extern "C"

@@ -78,10 +78,10 @@ __device__ __forceinline__ double d4(const double* f, long o, long s) {
 // memory allows no more); FP32 is built for 2 (128 registers, no spills) and 3
 // (80 registers, a few spills) and cbns_autotune keeps the faster.
 // HYB: hybrid flux (learned-sensor decision per face, see the flux lambda).
+// The work of one CTA: tile `tile` of the block's (i, j) tiling, k chunk `kc`.
 template <typename R, bool VISC, int MODE, int NB, bool HYB>
-__global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
+__device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc, unsigned char* smem_raw) {
   using S = R;  // shared-memory storage type
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem<S, R>& sm = *reinterpret_cast<Smem<S, R>*>(smem_raw);
 
   const StepState* st = a.st;
@@ -90,10 +90,9 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
 
   const Dims& d = a.d;
   const int t = threadIdx.x;
-  const int tile = blockIdx.x;
   const int ti0 = 1 + TI * (tile % a.ntile_i);
   const int tj0 = 1 + TJ * (tile / a.ntile_i);
-  const int kb = 1 + a.kchunk * blockIdx.y;
+  const int kb = 1 + a.kchunk * kc;
   const int ke = min(kb + a.kchunk, d.KM - 1);
   if (kb >= ke) return;
   const long VOL = d.VOL;
@@ -543,9 +542,79 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
   }
 }
 
+template <typename R, bool VISC, int MODE, int NB, bool HYB>
+__global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  stage_body<R, VISC, MODE, NB, HYB>(a, blockIdx.x, blockIdx.y, smem_raw);
+}
+
+// Many blocks in one launch: persistent CTAs take work items (block, tile, k
+// chunk) from a queue (one atomic counter); each item's StageArgs are copied
+// from the table into shared memory.  Items are numbered block by block, tiles
+// fastest, so CTAs of one block work on neighbouring columns together.
+template <typename R, bool VISC, int MODE, bool HYB>
+__global__ void __launch_bounds__(NT, 2) stage_kernel_batched(const BatchStage b) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ StageArgs args;
+  __shared__ int item;
+  for (;;) {
+    if (threadIdx.x == 0) item = (int)atomicAdd(b.counter, 1u);
+    __syncthreads();
+    const int w = item;
+    if (w >= b.total) break;
+    int blk = 0;
+    while (blk + 1 < b.nblocks && __ldg(b.start + blk + 1) <= w) ++blk;
+    const int* src = reinterpret_cast<const int*>(b.args + blk);
+    int* dst = reinterpret_cast<int*>(&args);
+    for (int e = threadIdx.x; e < (int)(sizeof(StageArgs) / sizeof(int)); e += NT) dst[e] = __ldg(src + e);
+    __syncthreads();
+    const int local = w - __ldg(b.start + blk);
+    const int ntiles = args.ntile_i * args.ntile_j;
+    stage_body<R, VISC, MODE, 2, HYB>(args, local % ntiles, local / ntiles, smem_raw);
+    __syncthreads();  // args, item and the shared staging are reused by the next item
+  }
+}
+
 template <typename R, bool HYB>
 constexpr size_t stage_smem() {
   return sizeof(Smem<R, R>) + (HYB ? sizeof(HybSmem<R>) : 0);
+}
+
+template <typename R, bool VISC, int MODE, bool HYB>
+cudaError_t launch_batched_t(const BatchStage& b, cudaStream_t s) {
+  const int smem = (int)stage_smem<R, HYB>();
+  static int grid = 0;
+  if (grid == 0) {
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, HYB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0, dev = 0, nsm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel_batched<R, VISC, MODE, HYB>, NT, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    grid = nsm * (per_sm > 0 ? per_sm : 1);
+  }
+  const int g = b.total < grid ? b.total : grid;
+  if (g <= 0) return cudaSuccess;
+  stage_kernel_batched<R, VISC, MODE, HYB><<<g, NT, smem, s>>>(b);
+  return cudaGetLastError();
+}
+
+template <typename R, bool HYB>
+cudaError_t launch_batched_r(const BatchStage& b, int mode, bool visc, cudaStream_t s) {
+  if (visc) {
+    switch (mode) {
+      case 1: return launch_batched_t<R, true, 1, HYB>(b, s);
+      case 2: return launch_batched_t<R, true, 2, HYB>(b, s);
+      default: return launch_batched_t<R, true, 3, HYB>(b, s);
+    }
+  }
+  switch (mode) {
+    case 1: return launch_batched_t<R, false, 1, HYB>(b, s);
+    case 2: return launch_batched_t<R, false, 2, HYB>(b, s);
+    default: return launch_batched_t<R, false, 3, HYB>(b, s);
+  }
 }
 
 template <typename R, bool VISC, int MODE, int NB, bool HYB>
@@ -608,6 +677,13 @@ void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j) {
 }
 
 int stage_variants(bool fp32) { return fp32 ? 2 : 1; }
+
+cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool fp32, bool hybrid, cudaStream_t s) {
+  if (mode < 1 || mode > 3) return cudaErrorInvalidValue;
+  if (!fp32) return launch_batched_r<double, false>(b, mode, visc, s);
+  if (hybrid) return launch_batched_r<float, true>(b, mode, visc, s);
+  return launch_batched_r<float, false>(b, mode, visc, s);
+}
 
 cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s) {
   if (!fp32) return launch_r<double, 2, false>(a, mode, visc, s);

@@ -24,10 +24,23 @@ struct StageArgs {
   int sigma;           // accumulate the interior spectral-radius max (inviscid stage 3)
 };
 
+// Many blocks in one launch (a persistent work queue): args[b] are the
+// StageArgs of block b, its work items (tile, k chunk) are numbered
+// start[b] .. start[b+1]-1 of total, and *counter (zeroed before the launch)
+// hands them out.
+struct BatchStage {
+  const StageArgs* args;  // device, nblocks entries
+  const int* start;       // device, nblocks + 1 entries
+  int nblocks, total;
+  unsigned* counter;      // device
+};
+
 // mode 0: dense RHS output; 1..3: RK stage.  fp32: split-precision flux arithmetic.
 // variant: a compiled occupancy variant, 0 .. stage_variants(fp32)-1.
 cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s);
 int stage_variants(bool fp32);
+// modes 1..3 only; hybrid: the StageArgs carry decision masks.
+cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool fp32, bool hybrid, cudaStream_t s);
 void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j);
 
 }  // namespace cbns

@@ -248,6 +248,25 @@ int cbns_sensor_stats_get(cbns_ctx* ctx, cbns_sensor_stats* stats);
 int cbns_sensor_mask_get(cbns_ctx* ctx, unsigned char* mask_host, unsigned long long n, int* forced);
 int cbns_sensor_stats_reset(cbns_ctx* ctx);
 
+/* Batches (no counterpart in the reference, which holds one block per
+ * process): independent blocks, each a context created and initialised as
+ * usual (its own grid, parameters, state and, for the hybrid, sensor),
+ * advanced together.  Per RK stage one persistent launch of the stage kernel
+ * works through a queue of the tiles of every block; each block keeps its own
+ * time step (per-block dt) and boundary conditions; a whole step of the
+ * batch is one CUDA graph.  The blocks share the precision and the viscous
+ * flag; while the batch exists they work on the batch's stream — the
+ * caller's `stream` (a cudaStream_t) or, when null, one the batch creates —
+ * and go back to their previous streams at cbns_batch_destroy; the batch does
+ * not own them (destroy the batch first).  cbns_batch_run advances every block by
+ * nsteps steps (or to t_end), *steps_min receiving the fewest steps any block
+ * took; CBNS_ERR_NAN_DT if any block's dt became NaN. */
+typedef struct cbns_batch cbns_batch;
+int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, cbns_batch** batch);
+int cbns_batch_destroy(cbns_batch* batch);
+int cbns_batch_run(cbns_batch* batch, unsigned nsteps, double t_end, unsigned* steps_min);
+int cbns_batch_run_async(cbns_batch* batch, unsigned nsteps, double t_end);
+
 /* Pick, by timing on the current state, the fastest compiled variant of the
  * stage kernel for this context's precision (the state is not modified);
  * *chosen (may be null) receives the variant index.  Later steps use it. */

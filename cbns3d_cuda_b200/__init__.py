@@ -177,7 +177,7 @@ class Block:
     def sensor_audit(self, stride: int = 97, bound: float = 1.0e-2):
         _abi.check(self.lib.cbns_sensor_audit(self.h, int(stride), float(bound)), "cbns_sensor_audit")
 
-    def sensor_interval(self, every: int = 2):
+    def sensor_interval(self, every: int = 3):
         _abi.check(self.lib.cbns_sensor_interval(self.h, int(every)), "cbns_sensor_interval")
 
     def sensor_stats(self) -> dict:

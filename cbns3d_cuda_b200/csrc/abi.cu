@@ -66,7 +66,7 @@ struct cbns_ctx {
   long nfaces = 0;
   float sensor_tau = 0.5f;
   unsigned audit_stride = 97;
-  unsigned sensor_every = 2;  // network evaluated every n-th step of cbns_run
+  unsigned sensor_every = 3;  // network evaluated every n-th step of cbns_run
   float audit_bound = 1.0e-2f;
   bool sensor_loaded = false;
   bool prof = false;

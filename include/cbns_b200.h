@@ -219,7 +219,7 @@ int cbns_sensor_load(cbns_ctx* ctx, const float* params_host, float tau);
  * missing or malformed. */
 int cbns_sensor_load_file(cbns_ctx* ctx, const char* path);
 /* Evaluate the network on every n-th step of cbns_run / cbns_run_async (1 <=
- * n <= 8, default 2; the first step of each run always evaluates); in between,
+ * n <= 8, default 3; the first step of each run always evaluates); in between,
  * the decisions of the last evaluation hold, widened by 1 + n faces along and
  * n faces across (a discontinuity moves less than a cell per step).  The
  * audit runs every step.  The per-call path (cbns_update_rk3 stage 1,

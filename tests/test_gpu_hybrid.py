@@ -116,6 +116,7 @@ def test_always_weno_sensor_matches_split(make):
     c = make()
     s = _block(c, PREC_SPLIT)
     h = _block(c, PREC_HYBRID, _constant_sensor(30.0))
+    h.sensor_interval(1)  # fresh decisions every step
     for b in (s, h):
         b.set_time(0.0)
         assert b.run(6) == 6

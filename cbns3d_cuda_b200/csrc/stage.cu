@@ -44,6 +44,23 @@ constexpr int NFI = (TI + 1) * TJ;  // 255 i-faces
 constexpr int NFJ = TI * (TJ + 1);  // 256 j-faces
 constexpr int NSX = (TI + 2) * TJ;  // i-face nodes (i0-1 .. i0+16)
 constexpr int NSY = TI * (TJ + 2);  // j-face nodes (j0-1 .. j0+15)
+constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;  // halo nodes of a plane: i-halo, j-halo
+
+// The FP32 kernels built for 2 CTAs per SM stage the next plane's halo (raw
+// FP64) and face-node area vectors with asynchronous copies while the current
+// plane is computed: the second area-vector buffer and the halo buffer.
+struct AsyncSmem {
+  double sx[3][TJ][TI + 2];
+  double sy[3][TJ + 2][TI];
+  double halo[NEQ][NHI + NHJ];
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <typename S, typename R>
 struct Smem {
@@ -67,6 +84,21 @@ struct HybSmem {
   unsigned short list[NFI + NFJ + NC];  // round << 10 | index within the round
   int count;
 };
+
+template <typename R, bool HYB>
+__host__ __device__ constexpr size_t hyb_bytes() {
+  return HYB ? (sizeof(HybSmem<R>) + 15) / 16 * 16 : 0;
+}
+
+template <typename R, int NB>
+__host__ __device__ constexpr bool async_staging() {
+  return sizeof(R) == 4 && NB == 2;
+}
+
+template <typename R, bool HYB, int NB>
+__host__ __device__ constexpr size_t stage_smem() {
+  return sizeof(Smem<R, R>) + hyb_bytes<R, HYB>() + (async_staging<R, NB>() ? sizeof(AsyncSmem) : 0);
+}
 
 // 4th-order central derivative of a node field along a stride, at offset o.
 __device__ __forceinline__ double d4(const double* f, long o, long s) {
@@ -170,9 +202,63 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     }
   };
 
+  constexpr bool kAsync = async_staging<R, NB>();
+  AsyncSmem* as = reinterpret_cast<AsyncSmem*>(smem_raw + sizeof(Smem<S, R>) + hyb_bytes<R, HYB>());
+  // halo node e of a plane: tile-relative (x, y)
+  auto halo_xy = [&](int e, int& x, int& y) {
+    if (e < NHI) {
+      const int c6 = e % (2 * H);
+      y = e / (2 * H);
+      x = c6 < H ? c6 - H : TI + (c6 - H);
+    } else {
+      const int e2 = e - NHI;
+      const int r6 = e2 / TI;
+      x = e2 % TI;
+      y = r6 < H ? r6 - H : TJ + (r6 - H);
+    }
+  };
+  // asynchronous copies of plane kp's halo and face-node area vectors (buffer
+  // kp & 1: 0 = Smem, 1 = AsyncSmem)
+  auto issue_plane = [&](int kp) {
+    for (int e = t; e < NHI + NHJ; e += NT) {
+      int x, y;
+      halo_xy(e, x, y);
+      const int gi = ti0 + x, gj = tj0 + y;
+      if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+        const long o = node_off(d, gi, gj, kp);
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) cp_async8(&as->halo[n][e], a.src + n * VOL + o);
+      }
+    }
+    double(&SX)[3][TJ][TI + 2] = (kp & 1) ? as->sx : sm.sx;
+    double(&SY)[3][TJ + 2][TI] = (kp & 1) ? as->sy : sm.sy;
+    for (int e = t; e < NSX + NSY; e += NT) {
+      if (e < NSX) {
+        const int c = e % (TI + 2), r = e / (TI + 2);
+        const int gi = ti0 - 1 + c, gj = tj0 + r;
+        if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+          const long o = node_off(d, gi, gj, kp);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) cp_async8(&SX[m][r][c], a.area[m] + o);
+        }
+      } else {
+        const int e2 = e - NSX;
+        const int c = e2 % TI, r = e2 / TI;
+        const int gi = ti0 + c, gj = tj0 - 1 + r;
+        if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+          const long o = node_off(d, gi, gj, kp);
+#pragma unroll
+          for (int m = 0; m < 3; ++m) cp_async8(&SY[m][r][c], a.area[3 + m] + o);
+        }
+      }
+    }
+    cp_async_commit();
+  };
+
   // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
   for (int kp = kb - 3; kp <= kb + 2; ++kp) load_ring(kp);
   if (kPrefetch) fetch_ring(kb + 3);
+  if (kAsync) issue_plane(kb);
   // the column's J*grad(zeta) at planes k and k+1, in FP64 (the stage-3
   // spectral radius uses it exactly)
   double za[3] = {0, 0, 0}, zb[3] = {0, 0, 0};
@@ -191,7 +277,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
 
   for (int k = kb; k < ke; ++k) {
     if (col_valid) load_zeta(k + 1, zb);  // consumed in round C
+    if (kAsync) cp_async_wait_all();     // plane k's halo and area vectors have landed
     __syncthreads();
+    // plane k's face-node area vectors
+    double(&SXk)[3][TJ][TI + 2] = (kAsync && (k & 1)) ? as->sx : sm.sx;
+    double(&SYk)[3][TJ + 2][TI] = (kAsync && (k & 1)) ? as->sy : sm.sy;
     if (kPrefetch) {
       store_ring(k + 3);
       if (k + 1 < ke) fetch_ring(k + 4);
@@ -210,35 +300,30 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
         for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = sm.ring[sk][n][e];
       }
       // halo: 6 columns x TJ rows (i-halo) then 6 rows x TI columns (j-halo)
-      constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;
       for (int e = t; e < NHI + NHJ; e += NT) {
         int x, y;
-        if (e < NHI) {
-          const int c6 = e % (2 * H);
-          y = e / (2 * H);
-          x = c6 < H ? c6 - H : TI + (c6 - H);
-        } else {
-          const int e2 = e - NHI;
-          const int r6 = e2 / TI;
-          x = e2 % TI;
-          y = r6 < H ? r6 - H : TJ + (r6 - H);
-        }
+        halo_xy(e, x, y);
         const int gi = ti0 + x, gj = tj0 + y;
         if (gi <= d.IM + 1 && gj <= d.JM + 1) {
-          const long o = node_off(d, gi, gj, k);
+          if (kAsync) {
 #pragma unroll
-          for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = (S)__ldg(a.src + n * VOL + o);
+            for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = (S)as->halo[n][e];
+          } else {
+            const long o = node_off(d, gi, gj, k);
+#pragma unroll
+            for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = (S)__ldg(a.src + n * VOL + o);
+          }
         }
       }
-      // area vectors of the face nodes of plane k
-      for (int e = t; e < NSX + NSY; e += NT) {
+      // area vectors of the face nodes of plane k (synchronous kernels)
+      for (int e = t; !kAsync && e < NSX + NSY; e += NT) {
         if (e < NSX) {
           const int c = e % (TI + 2), r = e / (TI + 2);
           const int gi = ti0 - 1 + c, gj = tj0 + r;
           if (gi <= d.IM + 1 && gj <= d.JM + 1) {
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) sm.sx[m][r][c] = __ldg(a.area[m] + o);
+            for (int m = 0; m < 3; ++m) SXk[m][r][c] = __ldg(a.area[m] + o);
           }
         } else {
           const int e2 = e - NSX;
@@ -247,12 +332,15 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
           if (gi <= d.IM + 1 && gj <= d.JM + 1) {
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) sm.sy[m][r][c] = __ldg(a.area[3 + m] + o);
+            for (int m = 0; m < 3; ++m) SYk[m][r][c] = __ldg(a.area[3 + m] + o);
           }
         }
       }
     }
     __syncthreads();
+    // plane k+1's halo and area vectors travel while plane k is computed (the
+    // buffers they overwrite were last read by plane k-1 and by the staging)
+    if (kAsync && k + 1 < ke) issue_plane(k + 1);
 
     R fkp[5];
     if (!HYB || all_weno) {
@@ -264,9 +352,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
           auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
           R f[5];
           const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
-          flux(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
-               R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
-               R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), e, f);
+          flux(ld, R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]),
+               R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]),
+               R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), e, f);
   #pragma unroll
           for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
         }
@@ -279,9 +367,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
           auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
           R f[5];
           const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
-          flux(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
-               R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
-               R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), e, f);
+          flux(ld, R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]),
+               R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]),
+               R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), e, f);
   #pragma unroll
           for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
         }
@@ -317,9 +405,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
             } else {
               auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
               R f[5];
-              face_flux_linear<R>(ld, R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]),
-                                  R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]),
-                                  R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]), C, f);
+              face_flux_linear<R>(ld, R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]),
+                                  R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]),
+                                  R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), C, f);
 #pragma unroll
               for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
             }
@@ -339,9 +427,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
             } else {
               auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
               R f[5];
-              face_flux_linear<R>(ld, R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]),
-                                  R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]),
-                                  R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]), C, f);
+              face_flux_linear<R>(ld, R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]),
+                                  R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]),
+                                  R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), C, f);
 #pragma unroll
               for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
             }
@@ -394,9 +482,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
 #pragma unroll
           for (int p = 0; p < 6; ++p) off[p] = p;
           ns = PH * PW;
-          nx = R(0.5) * ((R)sm.sx[0][fy][fx] + (R)sm.sx[0][fy][fx + 1]);
-          ny = R(0.5) * ((R)sm.sx[1][fy][fx] + (R)sm.sx[1][fy][fx + 1]);
-          nz = R(0.5) * ((R)sm.sx[2][fy][fx] + (R)sm.sx[2][fy][fx + 1]);
+          nx = R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]);
+          ny = R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]);
+          nz = R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]);
           out = &sm.fi[0][fy][fx];
           os = TJ * (TI + 1);
         } else if (r == 1) {
@@ -405,9 +493,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
 #pragma unroll
           for (int p = 0; p < 6; ++p) off[p] = p * PW;
           ns = PH * PW;
-          nx = R(0.5) * ((R)sm.sy[0][fy][fx] + (R)sm.sy[0][fy + 1][fx]);
-          ny = R(0.5) * ((R)sm.sy[1][fy][fx] + (R)sm.sy[1][fy + 1][fx]);
-          nz = R(0.5) * ((R)sm.sy[2][fy][fx] + (R)sm.sy[2][fy + 1][fx]);
+          nx = R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]);
+          ny = R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]);
+          nz = R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]);
           out = &sm.fj[0][fy][fx];
           os = (TJ + 1) * TI;
         } else {
@@ -500,8 +588,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
             double g[9];
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
-              g[m] = sm.sx[m][cy][cx + 1] * iJ;
-              g[3 + m] = sm.sy[m][cy + 1][cx] * iJ;
+              g[m] = SXk[m][cy][cx + 1] * iJ;
+              g[3 + m] = SYk[m][cy + 1][cx] * iJ;
               g[6 + m] = za[m] * iJ;
             }
             const double cs = sqrt(a.gamma * pp / r);
@@ -523,6 +611,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     for (int m = 0; m < 3; ++m) za[m] = zb[m];
   }
 
+  if (kAsync) cp_async_wait_all();  // nothing in flight when the CTA moves on
   if (MODE != 0 && !VISC && a.sigma) {
     // CTA max, one atomic per CTA
     __shared__ double red[NT / 32];
@@ -575,14 +664,10 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel_batched(const BatchStage b
   }
 }
 
-template <typename R, bool HYB>
-constexpr size_t stage_smem() {
-  return sizeof(Smem<R, R>) + (HYB ? sizeof(HybSmem<R>) : 0);
-}
 
 template <typename R, bool VISC, int MODE, bool HYB>
 cudaError_t launch_batched_t(const BatchStage& b, cudaStream_t s) {
-  const int smem = (int)stage_smem<R, HYB>();
+  const int smem = (int)stage_smem<R, HYB, 2>();
   static int grid = 0;
   if (grid == 0) {
     cudaError_t e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, HYB>,
@@ -619,7 +704,7 @@ cudaError_t launch_batched_r(const BatchStage& b, int mode, bool visc, cudaStrea
 
 template <typename R, bool VISC, int MODE, int NB, bool HYB>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
-  const size_t smem = stage_smem<R, HYB>();
+  const size_t smem = stage_smem<R, HYB, NB>();
   dim3 grid(a.ntile_i * a.ntile_j, (a.d.KM - 2 + a.kchunk - 1) / a.kchunk);
   stage_kernel<R, VISC, MODE, NB, HYB><<<grid, NT, smem, s>>>(a);
   return cudaGetLastError();
@@ -627,7 +712,7 @@ cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
 
 template <typename R, int NB, bool HYB>
 void prepare_nb() {
-  const int smem = (int)stage_smem<R, HYB>();
+  const int smem = (int)stage_smem<R, HYB, NB>();
   cudaFuncSetAttribute(stage_kernel<R, false, 0, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(stage_kernel<R, false, 1, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   cudaFuncSetAttribute(stage_kernel<R, false, 2, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

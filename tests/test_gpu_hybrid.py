@@ -6,7 +6,7 @@
   oracle's hybrid flux reproduce the GPU right-hand side and steps to the
   accuracy of the split path's FP32 flux arithmetic;
 * the audit catches a sensor that sends shock faces to the linear flux and
-  the step then equals the all-WENO5 step;
+  the step then equals the all-WENO5 step (to the FP32 rounding of the flux);
 * a hybrid context refuses to step before its sensor is loaded.
 """
 import numpy as np
@@ -290,7 +290,10 @@ def test_audit_forces_weno():
     assert st["audit_faces"] == 4 * st["faces_per_step"]
     m, forced = h.sensor_mask()
     assert forced and np.all(m == 0)
-    assert np.array_equal(h.get_conservative(), s.get_conservative())
+    # the forced step runs the split path's flux code (a separate compilation,
+    # so equal up to the FP32 rounding of the flux)
+    qh, qs = h.get_conservative(), s.get_conservative()
+    assert np.max(np.abs(qh - qs)) <= 1e-6 * np.max(np.abs(qs))
 
 
 def test_audit_rotating_sample_and_pass():

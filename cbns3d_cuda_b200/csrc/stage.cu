@@ -672,6 +672,9 @@ cudaError_t launch_batched_t(const BatchStage& b, cudaStream_t s) {
   if (grid == 0) {
     cudaError_t e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, HYB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, HYB>,
+                               cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     int per_sm = 0, dev = 0, nsm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel_batched<R, VISC, MODE, HYB>, NT, smem);
@@ -713,14 +716,19 @@ cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
 template <typename R, int NB, bool HYB>
 void prepare_nb() {
   const int smem = (int)stage_smem<R, HYB, NB>();
-  cudaFuncSetAttribute(stage_kernel<R, false, 0, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, false, 1, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, false, 2, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, false, 3, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 0, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 1, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 2, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  cudaFuncSetAttribute(stage_kernel<R, true, 3, NB, HYB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  // the largest shared-memory carveout, so that NB CTAs fit on an SM
+  auto set = [&](const void* f) {
+    cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
+  };
+  set((const void*)stage_kernel<R, false, 0, NB, HYB>);
+  set((const void*)stage_kernel<R, false, 1, NB, HYB>);
+  set((const void*)stage_kernel<R, false, 2, NB, HYB>);
+  set((const void*)stage_kernel<R, false, 3, NB, HYB>);
+  set((const void*)stage_kernel<R, true, 0, NB, HYB>);
+  set((const void*)stage_kernel<R, true, 1, NB, HYB>);
+  set((const void*)stage_kernel<R, true, 2, NB, HYB>);
+  set((const void*)stage_kernel<R, true, 3, NB, HYB>);
 }
 
 template <typename R, int NB, bool HYB>

@@ -204,7 +204,7 @@ def device_pass(case, precision, K, W, torch, dist, clocks=None):
     b.prof_enable(True)
     b.prof_reset()
     b.run(K)
-    out["kern"] = {kid: b.prof_read(kid) for kid in range(6)}
+    out["kern"] = {kid: b.prof_read(kid) for kid in range(7)}
     b.prof_enable(False)
     b.close()
     return out
@@ -343,7 +343,7 @@ def run_ours(a):
 
     def kern_ms(k):
         return {name: {"ms_per_step": k[i][0] / K, "launches_per_step": k[i][1] / K}
-                for i, name in enumerate(["stage", "bc", "viscous", "dt", "sensor", "audit"]) if k[i][1]}
+                for i, name in enumerate(["stage", "bc", "viscous", "dt", "sensor", "audit", "weno_faces"]) if k[i][1]}
 
     weno_frac = stats["weno_faces"] / (K * stats["faces_per_step"]) if stats["faces_per_step"] else None
     if rank == 0:

@@ -37,7 +37,7 @@ namespace cbns {
 void stage_prepare();
 }
 
-enum { PK_STAGE = 0, PK_BC = 1, PK_VISC = 2, PK_STEP = 3, PK_SENSOR = 4, PK_AUDIT = 5, PK_N = 6 };
+enum { PK_STAGE = 0, PK_BC = 1, PK_VISC = 2, PK_STEP = 3, PK_SENSOR = 4, PK_AUDIT = 5, PK_WENO = 6, PK_N = 7 };
 
 struct cbns_ctx {
   cbns_params prm;
@@ -63,6 +63,8 @@ struct cbns_ctx {
   float* sensor_params = nullptr;  // device, CBNS_SENSOR_NPARAM floats
   unsigned char* mask = nullptr;   // device, one byte per face: the decisions the fluxes use
   unsigned char* mask_raw = nullptr;  // device: the network's decisions before widening
+  float* wflux = nullptr;  // device, 8 floats per face: WENO5 fluxes of the stage's WENO5 faces
+  int2* wlist = nullptr;   // device, up to one entry per face: the step's WENO5 faces
   long nfaces = 0;
   float sensor_tau = 0.5f;
   unsigned audit_stride = 97;
@@ -203,10 +205,17 @@ StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const dou
   a.visdiv = c->ph.visdiv;
   a.sigma = sigma;
   a.mask = c->ph.precision == CBNS_PREC_HYBRID ? c->mask : nullptr;
+  a.wflux = c->wflux;
+  for (int m = 0; m < 6; ++m) a.area32[m] = c->f.area32[m];
   return a;
 }
 
 int stage_launch(cbns_ctx* c, const StageArgs& a, int mode) {
+  if (a.mask) {
+    Prof p(c, PK_WENO);
+    CK(launch_weno_faces(a, mode, c->nfaces, c->wlist, c->stream));
+    c->launches += 1;
+  }
   Prof p(c, PK_STAGE);
   CK(launch_stage(a, mode, c->ph.viscous != 0, c->ph.precision != CBNS_PREC_FP64, c->stage_variant, c->stream));
   c->launches += 1;
@@ -328,7 +337,11 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step
     Prof p(c, PK_AUDIT);
     CK(launch_sensor_audit(a, c->stream));
   }
-  c->launches += 6;  // two sensor sweeps, three widening passes and the audit
+  {
+    Prof p(c, PK_WENO);
+    CK(launch_weno_list(c->d, c->mask, c->nfaces, c->st, c->wlist, check_done, c->stream));
+  }
+  c->launches += 7;  // two sensor sweeps, three widening passes, the audit and the WENO5-face list
   return CBNS_OK;
 }
 
@@ -408,6 +421,7 @@ struct cbns_batch {
   std::vector<cudaStream_t> saved;         // the blocks' streams before the batch
   bool visc = false, fp32 = false, hyb = false;
   StageArgs* args = nullptr;  // device: 3 stages x nblocks
+  std::vector<StageArgs> host_args;  // the same, on the host (hybrid: WENO5-face passes)
   int* start = nullptr;       // device: nblocks + 1
   unsigned* counter = nullptr;
   int total = 0;
@@ -444,6 +458,7 @@ int batch_tables(cbns_batch* b) {
     b->roles.insert(b->roles.end(), {c->lq, c->lp, c->ls});
   }
   b->total = start[nb];
+  b->host_args = tab;
   CK(cudaMemcpyAsync(b->args, tab.data(), tab.size() * sizeof(StageArgs), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaStreamSynchronize(b->stream));
@@ -463,6 +478,11 @@ int batch_enqueue_step(cbns_batch* b) {
   for (int k = 0; k < 3; ++k) {
     const bool last = k == 2;
     CK(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), b->stream));
+    if (b->hyb)
+      for (int i = 0; i < nb; ++i) {
+        CK(launch_weno_faces(b->host_args[k * nb + i], k + 1, b->blk[i]->nfaces, b->blk[i]->wlist, b->stream));
+        b->blk[i]->launches += 1;
+      }
     BatchStage bs;
     bs.args = b->args + k * nb;
     bs.start = b->start;
@@ -599,6 +619,13 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   for (int b = 0; b < 3 && rc == CBNS_OK; ++b) rc = dalloc(c, &c->qb[b], (size_t)NEQ * d.VOL);
   for (int m = 0; m < 10 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.met[m], d.VOL);
   for (int m = 0; m < 10 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.area[m], d.VOL);
+  for (int m = 0; m < 6; ++m) c->f.area32[m] = nullptr;
+  if (p->precision != CBNS_PREC_FP64)
+    for (int m = 0; m < 6 && rc == CBNS_OK; ++m) {
+      double* tmp = nullptr;
+      rc = dalloc(c, &tmp, (size_t)(d.VOL + 1) / 2);
+      c->f.area32[m] = reinterpret_cast<float*>(tmp);
+    }
   for (int m = 0; m < 7 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.prim[m], d.VOL);
   for (int m = 0; m < 12; ++m) c->f.vflux[m] = nullptr;
   if (p->viscous)
@@ -608,7 +635,7 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   if (rc == CBNS_OK) rc = dalloc(c, &c->staging, c->staging_elems);
   c->nfaces = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2) + (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2) +
               (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 1);
-  if (rc == CBNS_OK && p->precision == CBNS_PREC_HYBRID && c->nfaces >= (1L << 31)) {
+  if (rc == CBNS_OK && p->precision == CBNS_PREC_HYBRID && (c->nfaces >= (1L << 31) || d.VOL >= (1L << 30))) {
     g_last = "the hybrid flux indexes faces with 32-bit integers: grid too large";
     rc = CBNS_ERR_TOO_LARGE;
   }
@@ -618,6 +645,10 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
     c->mask = reinterpret_cast<unsigned char*>(tmp);
     if (rc == CBNS_OK) rc = dalloc(c, &tmp, (size_t)(c->nfaces + 7) / 8);
     c->mask_raw = reinterpret_cast<unsigned char*>(tmp);
+    if (rc == CBNS_OK) rc = dalloc(c, &tmp, (size_t)c->nfaces * 4);
+    c->wflux = reinterpret_cast<float*>(tmp);
+    if (rc == CBNS_OK) rc = dalloc(c, &tmp, (size_t)c->nfaces);
+    c->wlist = reinterpret_cast<int2*>(tmp);
     if (rc == CBNS_OK) {
       rc = dalloc(c, &tmp, (CBNS_SENSOR_NPARAM + 1) / 2);
       c->sensor_params = reinterpret_cast<float*>(tmp);
@@ -651,6 +682,8 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   for (int b = 0; b < 3; ++b) cudaMemsetAsync(c->qb[b], 0, (size_t)NEQ * d.VOL * sizeof(double), c->stream);
   for (int m = 0; m < 10; ++m) cudaMemsetAsync(c->f.met[m], 0, d.VOL * sizeof(double), c->stream);
   for (int m = 0; m < 10; ++m) cudaMemsetAsync(c->f.area[m], 0, d.VOL * sizeof(double), c->stream);
+  for (int m = 0; m < 6; ++m)
+    if (c->f.area32[m]) cudaMemsetAsync(c->f.area32[m], 0, d.VOL * sizeof(float), c->stream);
   for (int m = 0; m < 7; ++m) cudaMemsetAsync(c->f.prim[m], 0, d.VOL * sizeof(double), c->stream);
   if (p->viscous)
     for (int m = 0; m < 12; ++m) cudaMemsetAsync(c->f.vflux[m], 0, d.VOL * sizeof(double), c->stream);
@@ -661,6 +694,7 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   int nchunk = std::max(1, std::min((4 * 296 + ntiles - 1) / ntiles, nint / 8));
   c->kchunk = (nint + nchunk - 1) / nchunk;
   stage_prepare();
+  if (p->precision == CBNS_PREC_HYBRID) (void)weno_prepare();
   if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
     g_last = "context initialisation failed";
     cbns_destroy(c);
@@ -701,7 +735,8 @@ int cbns_calc_metrics(cbns_ctx* c, const double* x, const double* y, const doubl
   CK(cudaMemcpyAsync(sx, x, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(sx + N, y, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(sx + 2 * N, z, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(launch_metrics(c->d, sx, sx + N, sx + 2 * N, c->f.met, c->f.area, c->stream));
+  CK(launch_metrics(c->d, sx, sx + N, sx + 2 * N, c->f.met, c->f.area,
+                    c->f.area32[0] ? c->f.area32 : nullptr, c->stream));
   c->launches += 3;
   RET(sync(c));
   c->have_metrics = true;
@@ -1092,7 +1127,7 @@ int cbns_sensor_stats_reset(cbns_ctx* c) {
 int cbns_autotune(cbns_ctx* c, int* chosen) {
   RET(check_flux_ready(c));
   const bool fp32 = c->ph.precision != CBNS_PREC_FP64;
-  const int nv = stage_variants(fp32);
+  const int nv = stage_variants(fp32, hybrid(c));
   // time every variant on the current state (RHS-only mode: nothing is updated);
   // the hybrid kernel is timed on the sensor's decisions for this state
   if (hybrid(c)) {

@@ -46,6 +46,7 @@ struct Phys {
 struct Fields {
   double* met[10];   // xi_x, xi_y, xi_z, eta_x, eta_y, eta_z, zeta_x, zeta_y, zeta_z, Jac
   double* area[10];  // J*grad(xi) (3), J*grad(eta) (3), J*grad(zeta) (3), 1/J
+  float* area32[6];  // FP32 and hybrid contexts: J*grad(xi), J*grad(eta) rounded to FP32
   double* prim[7];   // rho, u, v, w, p, T, mu (viscous upkeep; on-demand otherwise)
   double* vflux[12]; // E0..E3, F0..F3, G0..G3 (viscous node fluxes, times J-scaled normals)
 };
@@ -65,6 +66,7 @@ struct StepState {
   unsigned long long audit_faces; // hybrid: faces the audit re-evaluated
   float audit_max;                // hybrid: largest relative flux difference the audit saw
   int sensor_fail;                // hybrid: a tensor-core wait timed out
+  unsigned weno_listed;           // hybrid: length of the step's list of WENO5 faces
 };
 
 // Positive doubles order like their bit patterns; a NaN (either sign) compares

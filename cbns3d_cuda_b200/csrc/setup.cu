@@ -79,7 +79,13 @@ __global__ void metrics_ghosts(Dims d, Met M) {
 // Node area vectors J*grad(xi), J*grad(eta), J*grad(zeta) and 1/J over the
 // ghosted box: the face normal of the reference is the mean of the two nodes'
 // J*grad(xi) (src/rec_riemann_kernel.cu:44-49), so it is formed once here.
-__global__ void area_kernel(Dims d, Met M, Met A) {
+// The FP32 kernels stage FP32 copies of J*grad(xi) and J*grad(eta) (A32, may
+// be absent).
+struct Area32 {
+  float* m[6];
+};
+
+__global__ void area_kernel(Dims d, Met M, Met A, Area32 A32) {
   const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (e >= (long)d.IG * d.JG * d.KG) return;
   const int i = (int)(e % d.IG) - NG;
@@ -89,6 +95,10 @@ __global__ void area_kernel(Dims d, Met M, Met A) {
 #pragma unroll
   for (int m = 0; m < 9; ++m) A.m[m][o] = M.m[m][o] * J;
   A.m[9][o] = 1.0 / J;
+  if (A32.m[0]) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) A32.m[m][o] = (float)A.m[m][o];
+  }
 }
 
 struct Prims {
@@ -198,15 +208,17 @@ inline unsigned nb(long n) { return (unsigned)((n + 255) / 256); }
 }  // namespace
 
 cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, const double* z, double* const met[10],
-                           double* const area[10], cudaStream_t s) {
+                           double* const area[10], float* const area32[6], cudaStream_t s) {
   Met M, A;
+  Area32 A32;
   for (int m = 0; m < 10; ++m) {
     M.m[m] = met[m];
     A.m[m] = area[m];
   }
+  for (int m = 0; m < 6; ++m) A32.m[m] = area32 ? area32[m] : nullptr;
   metrics_nodes<<<nb((long)d.IM * d.JM * d.KM), 256, 0, s>>>(d, x, y, z, M);
   metrics_ghosts<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M);
-  area_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M, A);
+  area_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M, A, A32);
   return cudaGetLastError();
 }
 

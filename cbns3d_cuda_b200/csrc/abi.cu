@@ -59,6 +59,7 @@ struct cbns_ctx {
   int g_q = -1, g_p = -1, g_s = -1;
   int ntile_i = 1, ntile_j = 1, kchunk = 1;
   int stage_variant = 0;  // compiled occupancy variant of the stage kernel (cbns_autotune)
+  int nsm = 148;          // SMs of the device
   // hybrid flux: the learned sensor's parameters and per-face decisions
   float* sensor_params = nullptr;  // device, CBNS_SENSOR_NPARAM floats
   unsigned char* mask = nullptr;   // device, one byte per face: the decisions the fluxes use
@@ -105,6 +106,45 @@ int dalloc(cbns_ctx* c, double** p, size_t elems) {
 }
 
 inline long round_up(long x, long m) { return (x + m - 1) / m * m; }
+
+// k planes per CTA of the stage kernel.  The CTAs (tiles x k chunks) run in
+// waves of `slots` (SMs x CTAs per SM); a chunk costs its planes plus some
+// warm-up (the ring's first planes and the first k-face), `warm` planes'
+// worth.  The chunk count whose waves x (planes + warm) is least, keeping
+// chunks of at least 8 planes.
+int kchunk_by_waves(int ntiles, int nint, int slots, double warm) {
+  const int maxchunk = std::max(1, nint / 8);
+  double best = 1e300;
+  int best_k = nint;
+  for (int nchunk = 1; nchunk <= maxchunk; ++nchunk) {
+    const int kc = (nint + nchunk - 1) / nchunk;
+    const long items = (long)ntiles * ((nint + kc - 1) / kc);
+    const long waves = (items + slots - 1) / slots;
+    const double cost = (double)waves * (kc + warm);
+    if (cost < best - 1e-9) {
+      best = cost;
+      best_k = kc;
+    }
+  }
+  return best_k;
+}
+
+// The default: about four CTAs per slot of 2 CTAs per SM, chunks of at least 8 planes.
+int kchunk_default(int ntiles, int nint, int nsm) {
+  const int nchunk = std::max(1, std::min((4 * 2 * nsm + ntiles - 1) / ntiles, nint / 8));
+  return (nint + nchunk - 1) / nchunk;
+}
+
+// Candidate chunkings for cbns_autotune at `per_sm` CTAs per SM (distinct values).
+std::vector<int> kchunk_candidates(const cbns_ctx* c, int per_sm) {
+  const int ntiles = c->ntile_i * c->ntile_j, nint = c->d.KM - 2;
+  std::vector<int> v = {kchunk_default(ntiles, nint, c->nsm)};
+  for (double warm : {0.5, 2.0}) {
+    const int kc = kchunk_by_waves(ntiles, nint, c->nsm * per_sm, warm);
+    if (std::find(v.begin(), v.end(), kc) == v.end()) v.push_back(kc);
+  }
+  return v;
+}
 
 cudaEvent_t take_event(cbns_ctx* c) {
   cudaEvent_t e;
@@ -744,8 +784,12 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   stage_tiles(d, &c->ntile_i, &c->ntile_j);
   const int ntiles = c->ntile_i * c->ntile_j;
   const int nint = d.KM - 2;
-  int nchunk = std::max(1, std::min((4 * 296 + ntiles - 1) / ntiles, nint / 8));
-  c->kchunk = (nint + nchunk - 1) / nchunk;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    c->kchunk = kchunk_default(ntiles, nint, c->nsm);
+  }
   stage_prepare();
   if (p->precision == CBNS_PREC_HYBRID) (void)weno_prepare();
   if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
@@ -1187,29 +1231,35 @@ int cbns_autotune(cbns_ctx* c, int* chosen) {
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
     RET(sensor_launch(c, c->qb[c->lq], false, true));
   }
-  const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  int best = 0;
+  int best = 0, best_kc = c->kchunk;
   float best_ms = 1e30f;
   for (int v = 0; v < nv; ++v) {
-    c->stage_variant = v;
-    RET(stage_launch(c, a, 0));  // warm-up
-    CK(cudaEventRecord(e0, c->stream));
-    for (int r = 0; r < 3; ++r) RET(stage_launch(c, a, 0));
-    CK(cudaEventRecord(e1, c->stream));
-    CK(cudaEventSynchronize(e1));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = v;
+    // variant v runs 2 + v CTAs per SM; each with its candidate k chunks
+    for (int kc : kchunk_candidates(c, 2 + v)) {
+      c->stage_variant = v;
+      c->kchunk = kc;
+      const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
+      RET(stage_launch(c, a, 0));  // warm-up
+      CK(cudaEventRecord(e0, c->stream));
+      for (int r = 0; r < 3; ++r) RET(stage_launch(c, a, 0));
+      CK(cudaEventRecord(e1, c->stream));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = v;
+        best_kc = kc;
+      }
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->stage_variant = best;
+  c->kchunk = best_kc;
   drop_graph(c);
   if (chosen) *chosen = best;
   return CBNS_OK;

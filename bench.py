@@ -382,9 +382,9 @@ def run_ours(a):
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "kernel": "stage_kernel, hybrid (fused WENO5-char or linear/LF sweeps + RK3 update)",
+                         "kernel": "stage_kernel, hybrid (linear upwind-5/LF faces, WENO5 faces read from the WENO5-face pass, RK3 update)",
                          "alg_bytes_per_launch": alg_per_launch, "peak_kind": peak_kind,
-                         "note": "FP32 pipe and latency bound, not HBM bound"},
+                         "note": "load-latency and issue bound, not HBM bound"},
             "cpu_baseline": cpu,
             "clocks": clocks,
         }

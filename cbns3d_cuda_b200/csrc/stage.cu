@@ -71,6 +71,9 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
                : "memory");
 }
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
@@ -140,9 +143,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
   const bool all_weno = HYB && st->force_weno;
   const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
   const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
-  auto flux = [&](const auto& ld, R nx, R ny, R nz, long e, R out[5]) {
+  // wb: the face's decision when already loaded (0/1), -1 to read it here
+  auto flux = [&](const auto& ld, R nx, R ny, R nz, long e, int wb, R out[5]) {
     if constexpr (HYB) {
-      if (all_weno || __ldg(a.mask + e)) {
+      if (all_weno || (wb >= 0 ? wb != 0 : __ldg(a.mask + e) != 0)) {
         const float* w = a.wflux + 8 * e;
         const float4 v = __ldg(reinterpret_cast<const float4*>(w));
         out[0] = v.x;
@@ -181,7 +185,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
   };
 
   // k-face between planes kk and kk+1 of this thread's column
-  auto k_face = [&](int kk, const double za[3], const double zb[3], R out[5]) {
+  auto k_face = [&](int kk, const double za[3], const double zb[3], int wb, R out[5]) {
     const int s0 = (kk - 2 + 6) % 6;
     auto ld = [&](int p, int n) -> R {
       int s = s0 + p;
@@ -189,7 +193,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
       return (R)sm.ring[s][n][t];
     };
     const long e = nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * kk);
-    flux(ld, R(0.5) * ((R)za[0] + (R)zb[0]), R(0.5) * ((R)za[1] + (R)zb[1]), R(0.5) * ((R)za[2] + (R)zb[2]), e, out);
+    flux(ld, R(0.5) * ((R)za[0] + (R)zb[0]), R(0.5) * ((R)za[1] + (R)zb[1]), R(0.5) * ((R)za[2] + (R)zb[2]), e, wb,
+         out);
   };
 
   // The FP32 kernels fetch the ring column of plane k+4 into registers while
@@ -280,15 +285,62 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
   }
   __syncthreads();
   R fkm[5] = {0, 0, 0, 0, 0};
-  if (col_valid) k_face(kb - 1, za, zb, fkm);
+  if (col_valid) k_face(kb - 1, za, zb, -1, fkm);
 #pragma unroll
   for (int m = 0; m < 3; ++m) za[m] = zb[m];
 
   double smax = 0.0;  // running spectral-radius max (stage 3, inviscid)
   bool snan = false;
 
+  // Hybrid: the decisions of this thread's i-, j- and k-face of plane k (bits
+  // 0, 1, 2), read one plane ahead; the WENO5 fluxes of the set ones are
+  // asked into L1 at the top of the plane, before the staging, so the face
+  // rounds find them there.
+  auto mask_bits = [&](int k) -> unsigned {
+    unsigned m = 0;
+    if constexpr (HYB) {
+      if (t < NFI) {
+        const int fx = t % (TI + 1), fy = t / (TI + 1), ga = ti0 + fx - 1, gj = tj0 + fy;
+        if (ga <= d.IM - 2 && gj <= d.JM - 2)
+          m |= __ldg(a.mask + ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1))) != 0;
+      }
+      {
+        const int fx = t % TI, fy = t / TI, gi = ti0 + fx, ga = tj0 + fy - 1;
+        if (gi <= d.IM - 2 && ga <= d.JM - 2)
+          m |= (unsigned)(__ldg(a.mask + nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1))) != 0)
+               << 1;
+      }
+      if (col_valid)
+        m |= (unsigned)(__ldg(a.mask + nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * k)) !=
+                        0)
+             << 2;
+    }
+    return m;
+  };
+  auto prefetch_weno = [&](int k, unsigned m) {
+    if constexpr (HYB) {
+      if (m & 1u) {
+        const int fx = t % (TI + 1), fy = t / (TI + 1), ga = ti0 + fx - 1, gj = tj0 + fy;
+        prefetch_l1(a.wflux + 8 * (ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1))));
+      }
+      if (m & 2u) {
+        const int fx = t % TI, fy = t / TI, gi = ti0 + fx, ga = tj0 + fy - 1;
+        prefetch_l1(a.wflux + 8 * (nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1))));
+      }
+      if (m & 4u) prefetch_l1(a.wflux + 8 * (nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * k)));
+    }
+  };
+  unsigned mnext = (HYB && !all_weno) ? mask_bits(kb) : 0u;
+
   for (int k = kb; k < ke; ++k) {
     if (col_valid) load_zeta(k + 1, zb);  // consumed in round C
+    const unsigned mcur = mnext;
+    if constexpr (HYB) {
+      if (!all_weno) {
+        prefetch_weno(k, mcur);
+        if (k + 1 < ke) mnext = mask_bits(k + 1);
+      }
+    }
     // the FP32 kernels ask L2 for the next plane's RK operands and 1/J now, so
     // the update's loads one plane later find them there
     if (sizeof(S) == 4 && MODE != 0 && col_valid && k + 1 < ke) {
@@ -385,7 +437,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
         const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
         flux(ld, R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]),
              R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]),
-             R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), e, f);
+             R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), e, HYB ? (int)(mcur & 1u) : 0, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
       }
@@ -400,13 +452,13 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
         const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
         flux(ld, R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]),
              R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]),
-             R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), e, f);
+             R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), e, HYB ? (int)((mcur >> 1) & 1u) : 0, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
       }
     }
     // round C: the k+1/2 face of this column
-    if (col_valid) k_face(k, za, zb, fkp);
+    if (col_valid) k_face(k, za, zb, HYB ? (int)((mcur >> 2) & 1u) : 0, fkp);
     __syncthreads();
 
     if (col_valid) {

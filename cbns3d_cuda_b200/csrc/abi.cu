@@ -52,6 +52,8 @@ struct cbns_ctx {
   StepState* st = nullptr;
   unsigned* counter = nullptr;  // device counter for face sampling
   bool have_metrics = false, sigma_valid = false;
+  bool sigma_pending = false;  // per-call path: stage 3 accumulated the interior spectral radii
+  unsigned percall_hold = 0;   // per-call path: steps the current decisions still hold
   int prims_of = -1;     // physical buffer whose interior primitives the arrays hold
   int pending_src = -1;  // buffer given to calc_numerical_flux, consumed by update_rk3
   cudaGraph_t graph = nullptr;
@@ -325,10 +327,14 @@ void drop_graph(cbns_ctx* c) {
 // The hybrid flux's decisions for the state q: the sensor network on every
 // face (tensor cores), then the audit of a rotating sample of its linear-flux
 // faces against WENO5 (which forces WENO5 for the step on a violation).
-// every_step: evaluate the network now (per-call path) instead of on every
-// sensor_every-th step of a run.
-int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step = false) {
+// every_step: evaluate the network now instead of on every sensor_every-th
+// step of a run; widen: widening interval (0: that of the evaluation
+// schedule).  hold: the per-call path's steps between evaluations — only the
+// audit and the WENO5-face count run, the decisions (and their list) stand.
+int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step = false, unsigned widen = 0,
+                  bool hold = false) {
   const unsigned every = every_step ? 1u : c->sensor_every;
+  const unsigned wn = widen ? widen : every;
   MaskArgs m;
   m.d = c->d;
   m.gamma = (float)c->ph.gamma;
@@ -341,24 +347,30 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step
   m.mask = c->mask_raw;
   m.st = c->st;
   m.check_done = check_done;
+  int n = 0;
   {
     Prof p(c, PK_SENSOR);
-    CK(launch_sensor_mask(m, c->stream));
-    // widening in i, j, k: raw -> mask -> raw -> mask
+    if (!hold) {
+      CK(launch_sensor_mask(m, c->stream));
+      n += 2;
+    }
+    // widening in i, j, k: raw -> mask -> raw -> mask (held: the count only)
     unsigned char* bufs[4] = {c->mask_raw, c->mask, c->mask_raw, c->mask};
-    for (int dim = 0; dim < 3; ++dim) {
+    for (int dim = hold ? 2 : 0; dim < 3; ++dim) {
       DilateArgs w;
       w.d = c->d;
       w.in = bufs[dim];
       w.out = bufs[dim + 1];
       w.dim = dim;
-      w.along = 1 + (int)every;
-      w.across = (int)every;
+      w.along = 1 + (int)wn;
+      w.across = (int)wn;
       w.st = c->st;
       w.count = dim == 2;
       w.every = every;
+      w.hold = hold;
       w.check_done = check_done;
       CK(launch_sensor_dilate(w, c->stream));
+      n += 1;
     }
   }
   AuditArgs a;
@@ -377,11 +389,13 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step
     Prof p(c, PK_AUDIT);
     CK(launch_sensor_audit(a, c->stream));
   }
-  {
+  n += 1;
+  if (!hold) {
     Prof p(c, PK_WENO);
     CK(launch_weno_list(c->d, c->mask, c->nfaces, c->st, c->wlist, check_done, c->stream));
+    n += 1;
   }
-  c->launches += 7;  // two sensor sweeps, three widening passes, the audit and the WENO5-face list
+  c->launches += n;  // sensor sweeps, widening passes, the audit, the WENO5-face list
   return CBNS_OK;
 }
 
@@ -595,6 +609,10 @@ int batch_enqueue_step(cbns_batch* b) {
 
 int batch_run(cbns_batch* b, unsigned nsteps, double t_end, bool wait, unsigned* steps_min) {
   if (!b) return CBNS_ERR_ARG;
+  for (cbns_ctx* c : b->blk) {
+    c->percall_hold = 0;  // a run's decisions follow its own schedule
+    c->sigma_pending = false;
+  }
   for (cbns_ctx* c : b->blk) RET(run_prepare(c, t_end));
   bool stale = !b->gexec;
   for (size_t i = 0; i < b->blk.size() && !stale; ++i) {
@@ -838,6 +856,8 @@ int cbns_calc_metrics(cbns_ctx* c, const double* x, const double* y, const doubl
   RET(sync(c));
   c->have_metrics = true;
   c->sigma_valid = false;
+  c->sigma_pending = false;
+  c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
   return CBNS_OK;
 }
 
@@ -870,6 +890,8 @@ int cbns_calc_conservative(cbns_ctx* c, int which) {
   c->launches += 1;
   RET(replicate_q(c));
   c->sigma_valid = false;
+  c->sigma_pending = false;
+  c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
   c->prims_of = -1;
   return sync(c);
 }
@@ -882,6 +904,8 @@ int cbns_set_conservative(cbns_ctx* c, const double* Q) {
   c->launches += 1;
   RET(replicate_q(c));
   c->sigma_valid = false;
+  c->sigma_pending = false;
+  c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
   c->prims_of = -1;
   return sync(c);
 }
@@ -927,9 +951,12 @@ int cbns_set_bc_calc_primitive(cbns_ctx* c, int which) {
   if (which != CBNS_Q && which != CBNS_QP) return CBNS_ERR_ARG;
   const int pb = phys(c, which);
   const bool interior = c->ph.viscous && c->prims_of != pb;
-  RET(bc_launch(c, bc_args(c, c->qb[pb], false, false), interior));
+  // after an inviscid stage 3: add the boundary nodes to its spectral radii
+  const bool sigma = c->sigma_pending && which == CBNS_Q && !c->ph.viscous;
+  RET(bc_launch(c, bc_args(c, c->qb[pb], false, sigma), interior));
   if (c->ph.viscous) c->prims_of = pb;
-  c->sigma_valid = false;
+  c->sigma_valid = sigma;
+  c->sigma_pending = false;
   return sync(c);
 }
 
@@ -969,10 +996,19 @@ int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
     c->launches += 1;
   }
   if (hybrid(c) && stage == 1) {
+    // the network runs on every sensor_every-th call of a sequence of steps
+    // (as in cbns_run), its decisions widened to hold until the next one
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
-    RET(sensor_launch(c, c->qb[src], false, true));
+    const bool hold = c->percall_hold > 0;
+    RET(sensor_launch(c, c->qb[src], false, true, c->sensor_every, hold));
+    c->percall_hold = hold ? c->percall_hold - 1 : c->sensor_every - 1;
   }
-  const StageArgs a = stage_args(c, c->qb[src], c->qb[c->lq], c->qb[c->lp], c->qb[out], false);
+  // inviscid stage 3 accumulates the spectral radius of the interior nodes it
+  // updates; set_bc_calc_primitive(Q) adds the boundary nodes, and the next
+  // cbns_calc_dt reads the maximum instead of sweeping the grid again
+  const bool sigma = stage == 3 && !c->ph.viscous;
+  if (sigma) CK(cudaMemsetAsync(&c->st->sigma_bits, 0, sizeof(unsigned long long), c->stream));
+  const StageArgs a = stage_args(c, c->qb[src], c->qb[c->lq], c->qb[c->lp], c->qb[out], sigma);
   RET(stage_launch(c, a, (int)stage));
   if (swap) {
     if (stage == 3) std::swap(c->lq, c->ls);
@@ -980,13 +1016,14 @@ int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
   }
   if (c->ph.viscous) c->prims_of = out;
   c->sigma_valid = false;
+  c->sigma_pending = sigma;
   return sync(c);
 }
 
 int cbns_calc_dt(cbns_ctx* c, double* dt) {
   RET(check_ready(c));
   if (!dt) return CBNS_ERR_ARG;
-  RET(sigma_launch(c));
+  if (!c->sigma_valid) RET(sigma_launch(c));
   unsigned long long bits = 0;
   CK(cudaMemcpyAsync(&bits, &c->st->sigma_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
   RET(sync(c));
@@ -1016,6 +1053,8 @@ int cbns_get_time(cbns_ctx* c, double* t_cur, double* dt_last) {
 
 static int run_impl(cbns_ctx* c, unsigned nsteps, double t_end, bool wait, unsigned* steps_done) {
   RET(run_prepare(c, t_end));
+  c->percall_hold = 0;  // a run's decisions follow its own schedule
+  c->sigma_pending = false;
   if (c->prof) {
     for (unsigned n = 0; n < nsteps; ++n) RET(enqueue_step(c));
   } else {
@@ -1069,6 +1108,7 @@ int cbns_eval_rhs(cbns_ctx* c, int which, double* rhs) {
   if (hybrid(c)) {
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
     RET(sensor_launch(c, buf(c, which), false, true));
+    c->percall_hold = 0;  // unwidened decisions: the next per-call step evaluates again
   }
   const StageArgs a = stage_args(c, buf(c, which), nullptr, nullptr, c->staging, false);
   RET(stage_launch(c, a, 0));
@@ -1140,6 +1180,7 @@ int cbns_sensor_load(cbns_ctx* c, const float* params, float tau) {
                      c->stream));
   c->sensor_tau = tau;
   c->sensor_loaded = true;
+  c->percall_hold = 0;
   drop_graph(c);
   return sync(c);
 }
@@ -1177,6 +1218,7 @@ int cbns_sensor_audit(cbns_ctx* c, unsigned stride, float bound) {
 int cbns_sensor_interval(cbns_ctx* c, unsigned every) {
   if (!c || every < 1 || every > 8) return CBNS_ERR_ARG;
   c->sensor_every = every;
+  c->percall_hold = 0;
   drop_graph(c);
   return CBNS_OK;
 }
@@ -1230,6 +1272,7 @@ int cbns_autotune(cbns_ctx* c, int* chosen) {
   if (hybrid(c)) {
     CK(cudaMemsetAsync(&c->st->force_weno, 0, sizeof(int), c->stream));
     RET(sensor_launch(c, c->qb[c->lq], false, true));
+    c->percall_hold = 0;
   }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));

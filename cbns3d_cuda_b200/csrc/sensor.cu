@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float* __restrict__ 
 constexpr int DL = 16;
 __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) {
   if (a.check_done && a.st->done) return;
-  if (!sensor_step(a.st, a.every)) {
+  if (a.hold || !sensor_step(a.st, a.every)) {
     // decisions of an earlier step: only the statistics
     if (a.count) {
       const Dims& d = a.d;

@@ -54,6 +54,7 @@ struct DilateArgs {
   StepState* st;           // WENO5 faces are counted when count != 0
   int count;
   unsigned every;          // as MaskArgs::every; the count is kept every step
+  int hold;                // the decisions hold this step: count only (per-call path)
   int check_done;
 };
 

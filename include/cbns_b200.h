@@ -118,6 +118,10 @@ int cbns_calc_numerical_flux(cbns_ctx* ctx, int which);
 int cbns_calc_viscous_terms(cbns_ctx* ctx);
 int cbns_calc_viscous_flux_contribution(cbns_ctx* ctx);
 int cbns_update_rk3(cbns_ctx* ctx, double dt, unsigned stage);
+/* dt = CFL / max spectral radius of Q.  After an inviscid stage 3 followed by
+ * cbns_set_bc_calc_primitive(CBNS_Q) (the reference's step order) the maximum
+ * was accumulated by those two calls and is only read back; otherwise the
+ * grid is swept (src/time_step_kernel.cu:13-96). */
 int cbns_calc_dt(cbns_ctx* ctx, double* dt);
 
 /* Whole SSP-RK3 steps with the time step kept on the device: per step the CFL
@@ -222,8 +226,12 @@ int cbns_sensor_load_file(cbns_ctx* ctx, const char* path);
  * n <= 8, default 3; the first step of each run always evaluates); in between,
  * the decisions of the last evaluation hold, widened by 1 + n faces along and
  * n faces across (a discontinuity moves less than a cell per step).  The
- * audit runs every step.  The per-call path (cbns_update_rk3 stage 1,
- * cbns_eval_rhs) evaluates the network on every call, with n = 1 widths. */
+ * audit runs every step.  The per-call path follows the same schedule over
+ * its cbns_update_rk3 stage-1 calls: the first call after a new state
+ * (cbns_set_conservative, cbns_calc_conservative, cbns_calc_metrics), a run,
+ * cbns_eval_rhs, cbns_autotune, cbns_sensor_load or cbns_sensor_interval
+ * evaluates, the next n - 1 hold.  cbns_eval_rhs evaluates on every call,
+ * with n = 1 widths. */
 int cbns_sensor_interval(cbns_ctx* ctx, unsigned every);
 /* audit_stride >= 1 (1 audits every linear face every step); audit_bound > 0
  * (relative to the face's largest flux component).  Defaults 97 and 1e-2. */

@@ -54,6 +54,7 @@ struct cbns_ctx {
   bool have_metrics = false, sigma_valid = false;
   bool sigma_pending = false;  // per-call path: stage 3 accumulated the interior spectral radii
   unsigned percall_hold = 0;   // per-call path: steps the current decisions still hold
+  bool percall_restart = true; // per-call path: the next stage 1 starts a new sequence of steps
   int prims_of = -1;     // physical buffer whose interior primitives the arrays hold
   int pending_src = -1;  // buffer given to calc_numerical_flux, consumed by update_rk3
   cudaGraph_t graph = nullptr;
@@ -611,6 +612,7 @@ int batch_run(cbns_batch* b, unsigned nsteps, double t_end, bool wait, unsigned*
   if (!b) return CBNS_ERR_ARG;
   for (cbns_ctx* c : b->blk) {
     c->percall_hold = 0;  // a run's decisions follow its own schedule
+    c->percall_restart = true;
     c->sigma_pending = false;
   }
   for (cbns_ctx* c : b->blk) RET(run_prepare(c, t_end));
@@ -858,6 +860,7 @@ int cbns_calc_metrics(cbns_ctx* c, const double* x, const double* y, const doubl
   c->sigma_valid = false;
   c->sigma_pending = false;
   c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
+  c->percall_restart = true;
   return CBNS_OK;
 }
 
@@ -892,6 +895,7 @@ int cbns_calc_conservative(cbns_ctx* c, int which) {
   c->sigma_valid = false;
   c->sigma_pending = false;
   c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
+  c->percall_restart = true;
   c->prims_of = -1;
   return sync(c);
 }
@@ -906,6 +910,7 @@ int cbns_set_conservative(cbns_ctx* c, const double* Q) {
   c->sigma_valid = false;
   c->sigma_pending = false;
   c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
+  c->percall_restart = true;
   c->prims_of = -1;
   return sync(c);
 }
@@ -992,7 +997,8 @@ int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
   if (swap) out = c->ls;
   {
     Prof p(c, PK_STEP);
-    CK(launch_set_dt(c->st, dt, c->stream));
+    CK(launch_set_dt(c->st, dt, stage == 1, stage == 1 && c->percall_restart, c->stream));
+    if (stage == 1) c->percall_restart = false;
     c->launches += 1;
   }
   if (hybrid(c) && stage == 1) {
@@ -1054,6 +1060,7 @@ int cbns_get_time(cbns_ctx* c, double* t_cur, double* dt_last) {
 static int run_impl(cbns_ctx* c, unsigned nsteps, double t_end, bool wait, unsigned* steps_done) {
   RET(run_prepare(c, t_end));
   c->percall_hold = 0;  // a run's decisions follow its own schedule
+  c->percall_restart = true;
   c->sigma_pending = false;
   if (c->prof) {
     for (unsigned n = 0; n < nsteps; ++n) RET(enqueue_step(c));

@@ -89,9 +89,14 @@ __global__ void step_prologue(StepState* st, double CFL) {
   st->steps += 1;
 }
 
-__global__ void set_dt_kernel(StepState* st, double dt) {
+// The per-call path's dt for the stages that follow; new_step (stage 1) also
+// counts the step, as step_prologue does (restart: the count starts over), so
+// the audit's rotating sample advances as in a run.
+__global__ void set_dt_kernel(StepState* st, double dt, int new_step, int restart) {
   st->dt = dt;
   st->done = 0;
+  if (restart) st->steps = 0;
+  if (new_step) st->steps += 1;
 }
 
 }  // namespace
@@ -109,8 +114,8 @@ cudaError_t launch_step_prologue(StepState* st, double CFL, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_set_dt(StepState* st, double dt, cudaStream_t s) {
-  set_dt_kernel<<<1, 1, 0, s>>>(st, dt);
+cudaError_t launch_set_dt(StepState* st, double dt, bool new_step, bool restart, cudaStream_t s) {
+  set_dt_kernel<<<1, 1, 0, s>>>(st, dt, new_step, restart);
   return cudaGetLastError();
 }
 

@@ -19,6 +19,7 @@ struct SigmaArgs {
 // Zero the accumulator and reduce the spectral radius over all grid nodes.
 cudaError_t launch_sigma_nodes(const SigmaArgs& a, cudaStream_t s);
 cudaError_t launch_step_prologue(StepState* st, double CFL, cudaStream_t s);
-cudaError_t launch_set_dt(StepState* st, double dt, cudaStream_t s);
+// new_step: count a step (per-call stage 1); restart: the count starts over first
+cudaError_t launch_set_dt(StepState* st, double dt, bool new_step, bool restart, cudaStream_t s);
 
 }  // namespace cbns

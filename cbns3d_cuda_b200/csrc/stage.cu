@@ -26,7 +26,16 @@
 // Every thread computes 3 faces per plane; face fluxes never leave the SM and
 // no global load sits inside a face evaluation.
 // HBM traffic per node and stage: the stage input (40 B, halos from L2),
-// area vectors and 1/J (80 B), the RK base (0-40 B) and the output (40 B).
+// area vectors and 1/J (80 B; the FP32 kernels stage FP32 copies of the xi
+// and eta vectors, 56 B), the RK base (0-40 B) and the output (40 B).
+//
+// Hybrid (HYB): each face's sensor decision selects the linear upwind-5 flux,
+// evaluated here, or the characteristic WENO5 flux, evaluated before this
+// kernel by the WENO5-face pass (weno_faces.cu) and read from its face array.
+// The decisions of plane k+1 are read while plane k is computed, and the
+// WENO5 fluxes of plane k are asked into L1 before the plane's staging, so
+// the face rounds wait on neither.  Holding no WENO5 code, the hybrid kernel
+// runs at 3 CTAs per SM.
 #include <type_traits>
 
 #include "cbns_common.cuh"

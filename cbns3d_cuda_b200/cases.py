@@ -61,6 +61,59 @@ def read_checkpoint(path):
     return t, Q
 
 
+def read_vtk(path):
+    """Legacy VTK STRUCTURED_GRID as the driver writes it (ASCII or BINARY):
+    returns (dims (IM, JM, KM), points (n, 3), {name: array (n,)})."""
+    data = Path(path).read_bytes()
+    pos = 0
+
+    def line():
+        nonlocal pos
+        e = data.index(b"\n", pos)
+        s = data[pos:e].decode()
+        pos = e + 1
+        return s
+
+    line()
+    line()
+    binary = line().strip() == "BINARY"
+    line()
+    dims = tuple(int(v) for v in line().split()[1:4])
+    n = int(line().split()[1])
+
+    def values(count):
+        nonlocal pos
+        if binary:
+            a = np.frombuffer(data[pos:pos + 8 * count], dtype=">f8").astype(np.float64)
+            pos += 8 * count + 1  # the newline after the block
+            return a
+        out = []
+        while len(out) < count:
+            out.extend(float(v) for v in line().split())
+        return np.array(out)
+
+    pts = values(3 * n).reshape(n, 3)
+    line()  # POINT_DATA
+    nf = int(line().split()[2])
+    fields = {}
+    for _ in range(nf):
+        name = line().split()[0]
+        fields[name] = values(n)
+    return dims, pts, fields
+
+
+def read_plot3d_binary(xyz_path, q_path):
+    """The driver's binary Plot3D pair: returns (x, y, z, (Mach, alpha, Re, t), q (5, KM, JM, IM))."""
+    with open(xyz_path, "rb") as f:
+        IM, JM, KM = struct.unpack("<3i", f.read(12))
+        g = np.frombuffer(f.read(), dtype="<f8").reshape(3, KM, JM, IM)
+    with open(q_path, "rb") as f:
+        assert struct.unpack("<3i", f.read(12)) == (IM, JM, KM)
+        head = struct.unpack("<4d", f.read(32))
+        q = np.frombuffer(f.read(), dtype="<f8").reshape(5, KM, JM, IM)
+    return g[0], g[1], g[2], head, q
+
+
 def write_input(path, **v):
     missing = [k for k in INPUT_ORDER if k not in v]
     if missing:

@@ -5,8 +5,10 @@
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <iostream>
+#include <sstream>
 #include <stdexcept>
 
 namespace {
@@ -112,6 +114,82 @@ void Block3d::output_vtk() const {
   }
   std::cout << "The output is successful!\n";
   std::fclose(f);
+}
+
+namespace {
+
+// legacy VTK binary data are big-endian
+void put_be(std::vector<unsigned char>& buf, double v) {
+  unsigned char b[8];
+  std::memcpy(b, &v, 8);
+  for (int i = 7; i >= 0; --i) buf.push_back(b[i]);
+}
+
+}  // namespace
+
+// The same data set as output_vtk in legacy VTK BINARY: the header lines as
+// text, each array as big-endian doubles followed by a newline.  One write per
+// array instead of one formatted line per value.
+void Block3d::output_vtk_binary() const {
+  std::ofstream f("output.vtk", std::ios::out | std::ios::binary);
+  if (!f) return;
+  const size_t n = (size_t)IM_ * JM_ * KM_;
+  std::ostringstream h;
+  h << "# vtk DataFile Version 3.0\nvtk output\nBINARY\nDATASET STRUCTURED_GRID\n";
+  h << "DIMENSIONS " << IM_ << " " << JM_ << " " << KM_ << "\n";
+  h << "POINTS " << n << " double\n";
+  f << h.str();
+  std::vector<unsigned char> buf;
+  buf.reserve(3 * n * 8 + 1);
+  for (size_t i = 0; i < n; ++i) {
+    put_be(buf, x_[i]);
+    put_be(buf, y_[i]);
+    put_be(buf, z_[i]);
+  }
+  buf.push_back('\n');
+  f.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)buf.size());
+  f << "POINT_DATA " << n << "\nFIELD FieldData 5\n";
+  const char* names[5] = {"rho", "u", "v", "w", "p"};
+  const std::vector<value_type>* arrs[5] = {&rho_, &u_, &v_, &w_, &p_};
+  for (int a = 0; a < 5; ++a) {
+    f << names[a] << " 1 " << n << " double\n";
+    buf.clear();
+    for (size_type k = 0; k < KM_; ++k)
+      for (size_type j = 0; j < JM_; ++j)
+        for (size_type i = 0; i < IM_; ++i) put_be(buf, (*arrs[a])[(NG + i) + IM_G_ * ((NG + j) + JM_G_ * (NG + k))]);
+    buf.push_back('\n');
+    f.write(reinterpret_cast<const char*>(buf.data()), (std::streamsize)buf.size());
+  }
+  std::cout << "The output is successful!\n";
+}
+
+// Binary Plot3D (whole 3D, single block, no record markers, native byte
+// order): output.xyz = int32 IM JM KM, then x, y, z (float64, i fastest);
+// output.q = int32 IM JM KM, float64 Mach, angle of attack, Re, time, then
+// rho, rho u, rho v, rho w, rho E at the grid nodes (float64, i fastest).
+void Block3d::output_plot3d() const {
+  const int dims[3] = {(int)IM_, (int)JM_, (int)KM_};
+  const size_t n = (size_t)IM_ * JM_ * KM_;
+  {
+    std::ofstream f("output.xyz", std::ios::out | std::ios::binary);
+    if (!f) return;
+    f.write(reinterpret_cast<const char*>(dims), sizeof(dims));
+    for (const auto* a : {&x_, &y_, &z_}) f.write(reinterpret_cast<const char*>(a->data()), n * sizeof(value_type));
+  }
+  std::ofstream f("output.q", std::ios::out | std::ios::binary);
+  if (!f) return;
+  f.write(reinterpret_cast<const char*>(dims), sizeof(dims));
+  const double head[4] = {info_.Mach, info_.angle_attack, info_.Re, t_cur_};
+  f.write(reinterpret_cast<const char*>(head), sizeof(head));
+  std::vector<double> q(n);
+  for (int m = 0; m < NEQ; ++m) {
+    size_t e = 0;
+    for (size_type k = 0; k < KM_; ++k)
+      for (size_type j = 0; j < JM_; ++j)
+        for (size_type i = 0; i < IM_; ++i)
+          q[e++] = Q_[m + NEQ * ((NG + i) + IM_G_ * ((NG + j) + JM_G_ * (NG + k)))];
+    f.write(reinterpret_cast<const char*>(q.data()), n * sizeof(double));
+  }
 }
 
 // Checkpoint: double t_cur; uint32 IM_G, JM_G, KM_G; double Q[5*IM_G*JM_G*KM_G]
@@ -222,7 +300,12 @@ int Block3d::solve() {
     output_bin(checkpoint_fname_);
   }
   get_primitive(&info_, &data, rho_.data(), u_.data(), v_.data(), w_.data(), p_.data());
-  output_vtk();
+  if (opt_.vtk_binary) output_vtk_binary();
+  else output_vtk();
+  if (opt_.plot3d) {
+    get_conservative(&info_, &data, Q_.data());
+    output_plot3d();
+  }
   free_mem(&data);
   return 0;
 }

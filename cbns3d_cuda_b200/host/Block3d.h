@@ -20,6 +20,8 @@ class Block3d {
     int viscous = CBNS_SHIM_VISCOUS_DEFAULT;
     std::string input = "input.txt";
     std::string sensor = "";  // learned-sensor weights (precision hybrid)
+    bool vtk_binary = false;  // output.vtk as legacy VTK BINARY (big-endian) instead of ASCII
+    bool plot3d = false;      // also write output.xyz / output.q (binary Plot3D grid and solution)
   };
 
   explicit Block3d(const Options& o) : opt_(o) {}
@@ -29,6 +31,8 @@ class Block3d {
   void read_input();
   void read_mesh();
   void output_vtk() const;
+  void output_vtk_binary() const;
+  void output_plot3d() const;
   void output_bin(const std::string& fname) const;
   void read_bin(const std::string& fname);
   bool is_finished() const;

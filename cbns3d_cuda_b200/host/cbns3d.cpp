@@ -10,6 +10,9 @@
 //   --visdiv D       reference (default) | centered
 //   --inviscid / --viscous   override the build-time default
 //   --input FILE     parameter file (default input.txt)
+//   --vtk-binary     output.vtk in legacy VTK BINARY (same data set as the
+//                    reference's ASCII file, written in one pass per array)
+//   --plot3d         also write output.xyz / output.q (binary Plot3D)
 #include <unistd.h>
 
 #include <cstring>
@@ -34,6 +37,8 @@ int main(int argc, char** argv) {
     else if (s == "--inviscid") o.viscous = 0;
     else if (s == "--viscous") o.viscous = 1;
     else if (s == "--input") o.input = next();
+    else if (s == "--vtk-binary") o.vtk_binary = true;
+    else if (s == "--plot3d") o.plot3d = true;
     else if (s == "--precision") {
       const std::string v = next();
       o.precision = v == "split" ? CBNS_PREC_SPLIT : (v == "hybrid" ? CBNS_PREC_HYBRID : CBNS_PREC_FP64);

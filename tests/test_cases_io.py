@@ -74,3 +74,41 @@ def test_naca_grid_spacing():
     dist = np.hypot(x[0, -1] - x[0, 0], y[0, -1] - y[0, 0])
     assert np.allclose(dist, 20.0)
     assert 1.0 < r < 2.0
+
+
+def _write_vtk(path, dims, pts, fields, binary):
+    """The driver's legacy VTK layout (Block3d::output_vtk / output_vtk_binary)."""
+    n = pts.shape[0]
+    with open(path, "wb") as f:
+        f.write(b"# vtk DataFile Version 3.0\nvtk output\n" + (b"BINARY" if binary else b"ASCII") +
+                b"\nDATASET STRUCTURED_GRID\n")
+        f.write(f"DIMENSIONS {dims[0]} {dims[1]} {dims[2]}\nPOINTS {n} double\n".encode())
+        if binary:
+            f.write(pts.astype(">f8").tobytes() + b"\n")
+        else:
+            f.write("".join(f"{a:E} {b:E} {c:E}\n" for a, b, c in pts).encode())
+        f.write(f"POINT_DATA {n}\nFIELD FieldData {len(fields)}\n".encode())
+        for name, v in fields.items():
+            f.write(f"{name} 1 {n} double\n".encode())
+            if binary:
+                f.write(v.astype(">f8").tobytes() + b"\n")
+            else:
+                f.write("".join(f"{a:E}\n" for a in v).encode())
+
+
+def test_read_vtk_ascii_and_binary(tmp_path):
+    rng = np.random.default_rng(0)
+    dims = (4, 3, 2)
+    n = 24
+    pts = rng.standard_normal((n, 3))
+    fields = {k: rng.standard_normal(n) for k in ("rho", "u", "v", "w", "p")}
+    for binary in (False, True):
+        path = tmp_path / f"o{int(binary)}.vtk"
+        _write_vtk(path, dims, pts, fields, binary)
+        d, p, f = cases.read_vtk(path)
+        assert d == dims and sorted(f) == sorted(fields)
+        # BINARY is exact; ASCII carries %E's 7 significant digits
+        tol = 0.0 if binary else 1e-6
+        assert np.max(np.abs(p - pts)) <= tol * np.max(np.abs(pts))
+        for k in fields:
+            assert np.max(np.abs(f[k] - fields[k])) <= tol * np.max(np.abs(fields[k]))

@@ -503,7 +503,7 @@ def run_batch(a):
         "ms_per_step": ms_batch / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 flux / f64 state", "data": "synthetic",
         "config": {"workload": f"configs[4]: {len(cs)} viscous blocks, sizes 32^3..128x64x64 (seed 0), "
-                               "Mach U[0.3,2], Re U[1e3,1e5], learned-sensor hybrid, per-block dt",
+                               "Mach U[0.3,2], Re U[1e3,1e5], far-field boundaries, learned-sensor hybrid, per-block dt",
                    "cell_updates_per_step": N, "blocks": len(cs),
                    "shapes": [d["shape"] for d in draw]},
         "paths": {"batch": {"value": value, "ms_per_step": ms_batch / K},

@@ -31,6 +31,9 @@ PREC_HYBRID = 2
 VISDIV_REFERENCE = 0
 VISDIV_CENTERED = 1
 
+BC_REFERENCE = 0  # the reference's boundary conditions (parity contract)
+BC_FARFIELD = 1   # every boundary and ghost node holds the state it was set to
+
 
 class Params(C.Structure):
     """cbns_params: the fields Block3d::read_input fills plus run-time switches."""
@@ -42,7 +45,7 @@ class Params(C.Structure):
         ("Mach", C.c_double), ("Re", C.c_double), ("gamma", C.c_double),
         ("Pr", C.c_double), ("Pr_t", C.c_double), ("T_inf", C.c_double),
         ("viscous", C.c_int), ("precision", C.c_int), ("vis_divergence", C.c_int),
-        ("reserved", C.c_int * 5),
+        ("bc_mode", C.c_int), ("reserved", C.c_int * 4),
     ]
 
 

@@ -346,8 +346,8 @@ def case_batch(nblocks=64, seed=0, size_lo=(32, 32, 32), size_hi=(128, 64, 64), 
     Mach uniform in [0.3, 2.0], Reynolds number uniform in [1e3, 1e5], an
     isentropic vortex of strength uniform in [1, 5] at a random position of
     the middle half of the perturbed 10 x 5 x 2.5 box; viscous by default.
-    Boundaries as configs[0] (the reference's modes: i faces pressure-reset
-    extrapolation, j faces held at the initial state, k faces zero-gradient).
+    Far-field boundaries on every face (bc_mode = 1, BC_FARFIELD: boundary and
+    ghost nodes hold the initial state), as the configuration asks.
     Returns the list of Cases and the draw."""
     rng = np.random.default_rng(seed)
     out, draw = [], []
@@ -362,7 +362,7 @@ def case_batch(nblocks=64, seed=0, size_lo=(32, 32, 32), size_hi=(128, 64, 64), 
         g = 1.4
         Q = conservative(*isentropic_vortex(xg, yg, Mach, beta, xc, yc, 1.0, g), g)
         params = dict(CFL=CFL, Mach=Mach, gamma=g, i_begin=1, i_end=0, Re=Re, Pr=0.72, T_inf=288.15,
-                      viscous=viscous)
+                      viscous=viscous, bc_mode=1)
         out.append(Case(f"batch{b}", x, y, z, params, Q, t_end=1.0e30, nsteps=500))
         draw.append(dict(shape=(IM, JM, KM), Mach=Mach, Re=Re, beta=beta, centre=(xc, yc)))
     return out, draw

@@ -11,6 +11,9 @@
 //            copy of Q and primitives for every (i,j) (:417-492); (c) in
 //            inviscid runs, the spectral radius of every boundary node for the
 //            next time step (the boundary half of src/time_step_kernel.cu).
+// With CBNS_BC_FARFIELD (no counterpart in the reference) one kernel replaces
+// the three: boundary and ghost nodes keep their Q (a free-stream far field on
+// every face), only their primitives and spectral radii are formed.
 // The reference runs these as __syncthreads-separated phases of one kernel, so
 // its cross-CTA reads (wake mirror, k-face copies of j-face results) are races;
 // separate launches give the program-order result, which is what the reference
@@ -254,6 +257,34 @@ __global__ void bc_phase3(const BCArgs a) {
   if (!a.viscous && a.sigma) warp_sigma_max(a, sg, has);
 }
 
+// CBNS_BC_FARFIELD: every node of the ghosted box outside the interior keeps
+// its Q; its primitives (viscous runs) follow from that Q, and in inviscid
+// runs the grid's boundary nodes add their spectral radii for the next dt.
+__global__ void bc_farfield(const BCArgs a) {
+  if (a.check_done && a.st->done) return;
+  const Dims& d = a.d;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double sg = 0.0;
+  bool has = false;
+  if (e < (long)d.IG * d.JG * d.KG) {
+    const int i = (int)(e % d.IG) - NG;
+    const long r = e / d.IG;
+    const int j = (int)(r % d.JG) - NG, k = (int)(r / d.JG) - NG;
+    const bool interior = i >= 1 && i <= d.IM - 2 && j >= 1 && j <= d.JM - 2 && k >= 1 && k <= d.KM - 2;
+    if (!interior) {
+      const long o = node_off(d, i, j, k);
+      const PrimV s = prim_of(a.q, o, d.VOL, a.gam1);
+      if (a.viscous) {
+        put_prim(a, o, s);
+      } else if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && k >= 0 && k < d.KM) {
+        sg = sigma_inv(a, o, s);
+        has = true;
+      }
+    }
+  }
+  if (!a.viscous && a.sigma) warp_sigma_max(a, sg, has);
+}
+
 // Interior primitives (rho,u,v,w,p,T) from Q, the first part of
 // primitive_bc_kernel (:59-79); needed when the primitive arrays do not yet
 // describe the buffer the boundary conditions act on.
@@ -280,6 +311,14 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
   if (interior_prims && a.viscous) {
     bc_interior_prims<<<nblk((long)(d.IM - 2) * (d.JM - 2) * (d.KM - 2), B), B, 0, s>>>(a);
     ++nl;
+  }
+  if (a.farfield) {
+    if (a.viscous || a.sigma) {
+      bc_farfield<<<nblk((long)d.IG * d.JG * d.KG, B), B, 0, s>>>(a);
+      ++nl;
+    }
+    if (launches) *launches += nl;
+    return cudaGetLastError();
   }
   bc_phase1<<<nblk(2L * (d.JM - 2) * (d.KM - 2), B), B, 0, s>>>(a);
   ++nl;

@@ -16,6 +16,7 @@ struct BCArgs {
   StepState* st;
   int check_done;        // return at once when st->done is set (graph-replayed steps)
   int sigma;             // inviscid: accumulate boundary-node spectral radii
+  int farfield;          // CBNS_BC_FARFIELD: boundary and ghost nodes hold their state
 };
 
 // interior_prims: also recompute interior primitives (viscous runs), when the

@@ -68,6 +68,16 @@ extern "C" {
                                    in both transverse directions                        */
 #define CBNS_VISDIV_CENTERED  1 /* every derivative taken at the node itself           */
 
+/* cbns_params.bc_mode.  REFERENCE: the reference's boundary conditions
+ * (src/primitive_bc_kernel.cu:13-494), the parity contract.  FARFIELD (no
+ * counterpart in the reference): every boundary and ghost node holds the state
+ * it was given by cbns_set_conservative / cbns_calc_conservative — the
+ * free-stream far field on all faces that the vortex and batched-block
+ * configurations ask for; only their primitives (viscous runs) and spectral
+ * radii are recomputed. */
+#define CBNS_BC_REFERENCE 0
+#define CBNS_BC_FARFIELD  1
+
 /* Run parameters: the fields of Block3dInfo that Block3d::read_input fills
  * (src/Block3d.cpp:33-138, include/Block3d_cuda.h:32-78) plus build-time
  * switches of the reference that are run-time options here.  The derived
@@ -84,7 +94,8 @@ typedef struct cbns_params {
   int      viscous;         /* 0: INVIS_MODE=ON build; 1: viscous build            */
   int      precision;       /* CBNS_PREC_*                                         */
   int      vis_divergence;  /* CBNS_VISDIV_*                                       */
-  int      reserved[5];     /* must be zero                                        */
+  int      bc_mode;         /* CBNS_BC_*                                           */
+  int      reserved[4];     /* must be zero                                        */
 } cbns_params;
 
 typedef struct cbns_ctx cbns_ctx;

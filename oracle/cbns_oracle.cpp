@@ -377,6 +377,18 @@ struct Oracle {
     for (long k = 1; k < KM - 1; ++k)
       for (long j = 1; j < JM - 1; ++j)
         for (long i = 1; i < IM - 1; ++i) put_prim(g(i, j, k), to_prim(&Q[5 * g(i, j, k)], gam1));
+    if (P.bc_mode == CBNS_BC_FARFIELD) {
+      // no counterpart in the reference: boundary and ghost nodes keep their Q,
+      // their primitives follow from it
+#pragma omp parallel for schedule(static)
+      for (long k = -NG; k < KM + NG; ++k)
+        for (long j = -NG; j < JM + NG; ++j)
+          for (long i = -NG; i < IM + NG; ++i) {
+            if (i >= 1 && i < IM - 1 && j >= 1 && j < JM - 1 && k >= 1 && k < KM - 1) continue;
+            put_prim(g(i, j, k), to_prim(&Q[5 * g(i, j, k)], gam1));
+          }
+      return;
+    }
     // phase 1b: i faces (:84-186)
 #pragma omp parallel for schedule(static)
     for (long k = 1; k < KM - 1; ++k)

@@ -90,6 +90,14 @@ class Block:
         assert q.size == NEQ * self.IG * self.JG * self.KG
         _abi.check(self.lib.cbns_set_conservative(self.h, _abi.dptr(q)), "cbns_set_conservative")
 
+    def init_case(self, kind: int, x, y, z, prm):
+        """The case's initial state formed on the device (cbns_init_case):
+        kind _abi.CASE_*, prm its parameters, x/y/z the grid (KM, JM, IM)."""
+        a = [np.ascontiguousarray(v, dtype=np.float64).reshape(-1) for v in (x, y, z)]
+        pv = np.ascontiguousarray(prm, dtype=np.float64).reshape(-1)
+        _abi.check(self.lib.cbns_init_case(self.h, int(kind), *(_abi.dptr(v) for v in a), _abi.dptr(pv), len(pv)),
+                   "cbns_init_case")
+
     def get_conservative(self, which=CBNS_Q, out: np.ndarray | None = None) -> np.ndarray:
         n = NEQ * self.IG * self.JG * self.KG
         q = out if out is not None else np.empty(n)

@@ -31,6 +31,10 @@ PREC_HYBRID = 2
 VISDIV_REFERENCE = 0
 VISDIV_CENTERED = 1
 
+CASE_VORTEX = 0
+CASE_BLAST = 1
+CASE_SHOCK_VORTEX = 2
+
 BC_REFERENCE = 0  # the reference's boundary conditions (parity contract)
 BC_FARFIELD = 1   # every boundary and ghost node holds the state it was set to
 
@@ -72,6 +76,7 @@ SIGNATURES = [
     ("cbns_initial_condition", C.c_int, [_V]),
     ("cbns_calc_conservative", C.c_int, [_V, C.c_int]),
     ("cbns_set_conservative", C.c_int, [_V, _D]),
+    ("cbns_init_case", C.c_int, [_V, C.c_int, _D, _D, _D, _D, C.c_uint]),
     ("cbns_get_conservative", C.c_int, [_V, C.c_int, _D]),
     ("cbns_get_primitive", C.c_int, [_V, _D, _D, _D, _D, _D, _D]),
     ("cbns_set_bc_calc_primitive", C.c_int, [_V, C.c_int]),

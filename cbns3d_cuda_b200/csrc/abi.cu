@@ -917,6 +917,26 @@ int cbns_set_conservative(cbns_ctx* c, const double* Q) {
   return sync(c);
 }
 
+int cbns_init_case(cbns_ctx* c, int kind, const double* x, const double* y, const double* z, const double* prm,
+                   unsigned nprm) {
+  if (!c || !x || !y || !z || (nprm > 0 && !prm) || nprm > 8) return CBNS_ERR_ARG;
+  if (kind != CBNS_CASE_VORTEX && kind != CBNS_CASE_BLAST && kind != CBNS_CASE_SHOCK_VORTEX) return CBNS_ERR_ARG;
+  const size_t N = (size_t)c->d.IM * c->d.JM * c->d.KM;
+  double* sx = c->staging;
+  CK(cudaMemcpyAsync(sx, x, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(sx + N, y, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(sx + 2 * N, z, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_case_ic(c->d, sx, sx + N, sx + 2 * N, kind, prm, (int)nprm, c->ph.gamma, c->qb[c->lq], c->stream));
+  c->launches += 1;
+  RET(replicate_q(c));
+  c->sigma_valid = false;
+  c->sigma_pending = false;
+  c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
+  c->percall_restart = true;
+  c->prims_of = -1;
+  return sync(c);
+}
+
 int cbns_get_conservative(cbns_ctx* c, int which, double* Q) {
   if (!c || !Q || (which != CBNS_Q && which != CBNS_QP)) return CBNS_ERR_ARG;
   const size_t n = (size_t)NEQ * c->d.IG * c->d.JG * c->d.KG;

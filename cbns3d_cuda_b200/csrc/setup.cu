@@ -203,6 +203,105 @@ __global__ void gradient_dense(int IM, int JM, int KM, const double* f, double* 
   fz[e] = dax(f + e, (long)IM * JM, k, KM);
 }
 
+// Case initialisation on the device (no counterpart in the reference, whose
+// driver reads a checkpoint or starts from the free stream).  The grid's
+// coordinates are extended into the ghost layers by odd reflection, axis by
+// axis in the order k, j, i (x(-l) = 2 x(0) - x(l)), and the configurations'
+// initial states are formed on the whole ghosted box in the reference's units.
+struct CaseParams {
+  double v[8];
+};
+
+// coordinate f (IM x JM x KM, i fastest) at ghosted node (i, j, k)
+__device__ __forceinline__ double coord_ext(const Dims& d, const double* f, int i, int j, int k) {
+  auto at = [&](int ii, int jj, int kk) -> double { return f[ii + (long)d.IM * (jj + (long)d.JM * kk)]; };
+  auto ek = [&](int ii, int jj) -> double {  // along k
+    if (k < 0) return 2.0 * at(ii, jj, 0) - at(ii, jj, -k);
+    if (k > d.KM - 1) return 2.0 * at(ii, jj, d.KM - 1) - at(ii, jj, 2 * (d.KM - 1) - k);
+    return at(ii, jj, k);
+  };
+  auto ejk = [&](int ii) -> double {  // along j, on the k-extended values
+    if (j < 0) return 2.0 * ek(ii, 0) - ek(ii, -j);
+    if (j > d.JM - 1) return 2.0 * ek(ii, d.JM - 1) - ek(ii, 2 * (d.JM - 1) - j);
+    return ek(ii, j);
+  };
+  if (i < 0) return 2.0 * ejk(0) - ejk(-i);  // along i, on the (k, j)-extended values
+  if (i > d.IM - 1) return 2.0 * ejk(d.IM - 1) - ejk(2 * (d.IM - 1) - i);
+  return ejk(i);
+}
+
+__global__ void case_ic_kernel(Dims d, const double* x, const double* y, const double* z, int kind, CaseParams cp,
+                               double g, double* q) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= (long)d.IG * d.JG * d.KG) return;
+  const int i = (int)(e % d.IG) - NG;
+  const long r = e / d.IG;
+  const int j = (int)(r % d.JG) - NG, k = (int)(r / d.JG) - NG;
+  const double xg = coord_ext(d, x, i, j, k), yg = coord_ext(d, y, i, j, k);
+  const double PI = 3.14159265358979323846;
+  double rho, u, v, w = 0.0, p;
+  if (kind == CBNS_CASE_VORTEX) {
+    // isentropic vortex of strength beta (free-stream sound-speed units) and
+    // Gaussian radius R in a free stream of Mach number M along (dirx, diry)
+    const double M = cp.v[0], beta = cp.v[1], xc = cp.v[2], yc = cp.v[3], R = cp.v[4], dirx = cp.v[5],
+                 diry = cp.v[6];
+    const double dx = (xg - xc) / R, dy = (yg - yc) / R;
+    const double r2 = dx * dx + dy * dy;
+    const double f = exp(0.5 * (1.0 - r2));
+    const double U = M * sqrt(g);
+    const double ua = U * dirx - beta / (2.0 * PI) * dy * f;
+    const double va = U * diry + beta / (2.0 * PI) * dx * f;
+    const double T = 1.0 - (g - 1.0) * (beta * beta) / (8.0 * g * (PI * PI)) * exp(1.0 - r2);
+    rho = pow(T, 1.0 / (g - 1.0));
+    u = ua / U;
+    v = va / U;
+    p = rho * T / (U * U);
+  } else if (kind == CBNS_CASE_BLAST) {
+    // pressure p_in where x^2 + y^2 + z^2 < r2_in, p_out elsewhere, unit
+    // density, at rest
+    const double zg = coord_ext(d, z, i, j, k);
+    const double r2 = xg * xg + yg * yg + zg * zg;
+    rho = 1.0;
+    u = v = 0.0;
+    p = r2 < cp.v[0] ? cp.v[1] : cp.v[2];
+  } else {
+    // stationary normal shock of Mach Ms at x = xs; upstream (rho, u, p) =
+    // (1, 1, 1/(g Ms^2)) with a vortex (strength eps, radius rc, centre
+    // (xc, yc), u_theta = eps c1 tau exp(a (1 - tau^2)), a = 0.204)
+    const double Ms = cp.v[0], eps = cp.v[1], rc = cp.v[2], xc = cp.v[3], yc = cp.v[4], xs = cp.v[5];
+    const double a = 0.204;
+    const double p1 = 1.0 / (g * Ms * Ms);
+    if (xg < xs) {
+      const double dx = xg - xc, dy = yg - yc;
+      const double rr = sqrt(dx * dx + dy * dy);
+      const double tau = rr / rc;
+      const double c1 = sqrt(g * p1 / 1.0);
+      const double ut = eps * c1 * tau * exp(a * (1.0 - tau * tau));
+      const double sn = rr > 0.0 ? dy / rr : 0.0, cs = rr > 0.0 ? dx / rr : 0.0;
+      const double T1 = p1 / 1.0;
+      const double T = T1 - (g - 1.0) * ((eps * c1) * (eps * c1)) / (4.0 * a * g) * exp(2.0 * a * (1.0 - tau * tau)) *
+                                (1.0 / 1.0);
+      rho = pow(T / T1, 1.0 / (g - 1.0));
+      u = 1.0 - ut * sn;
+      v = ut * cs;
+      p = p1 * pow(T / T1, g / (g - 1.0));
+    } else {
+      const double r21 = ((g + 1.0) * Ms * Ms) / ((g - 1.0) * Ms * Ms + 2.0);
+      const double p21 = 1.0 + 2.0 * g / (g + 1.0) * (Ms * Ms - 1.0);
+      rho = r21;
+      u = 1.0 / r21;
+      v = 0.0;
+      p = p1 * p21;
+    }
+  }
+  const long o = node_off(d, i, j, k), VOL = d.VOL;
+  q[o] = rho;
+  q[VOL + o] = rho * u;
+  q[2 * VOL + o] = rho * v;
+  q[3 * VOL + o] = rho * w;
+  q[4 * VOL + o] = p / (g - 1.0) + 0.5 * rho * (u * u + v * v + w * w);
+}
+
 inline unsigned nb(long n) { return (unsigned)((n + 255) / 256); }
 
 }  // namespace
@@ -229,6 +328,14 @@ cudaError_t launch_ic(const Dims& d, double* const prim[6], double angle_deg, do
   const double PI = 3.14159265358979323846;
   const double AoA = angle_deg * PI / 180.0;
   ic_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, P, cos(AoA), sin(AoA), p_inf, viscous);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_case_ic(const Dims& d, const double* x, const double* y, const double* z, int kind,
+                           const double* prm, int nprm, double gamma, double* q, cudaStream_t s) {
+  CaseParams cp;
+  for (int m = 0; m < 8; ++m) cp.v[m] = m < nprm ? prm[m] : 0.0;
+  case_ic_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, x, y, z, kind, cp, gamma, q);
   return cudaGetLastError();
 }
 

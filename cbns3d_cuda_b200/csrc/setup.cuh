@@ -2,6 +2,7 @@
 #pragma once
 
 #include "cbns_common.cuh"
+#include "../../include/cbns_b200.h"
 
 namespace cbns {
 
@@ -11,6 +12,10 @@ cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, cons
                            double* const area[10], float* const area32[6], cudaStream_t s);
 cudaError_t launch_ic(const Dims& d, double* const prim[6], double angle_deg, double p_inf, int viscous,
                       cudaStream_t s);
+// Case initial states on the ghosted box (kind CBNS_CASE_*, prm as in
+// cbns_init_case) from the grid coordinates x, y, z (device, IM*JM*KM).
+cudaError_t launch_case_ic(const Dims& d, const double* x, const double* y, const double* z, int kind,
+                           const double* prm, int nprm, double gamma, double* q, cudaStream_t s);
 cudaError_t launch_conservative(const Dims& d, double* const prim[6], double* q, double gam1, cudaStream_t s);
 cudaError_t launch_primitive(const Dims& d, const double* q, double* const prim[6], double gam1, double gM2,
                              cudaStream_t s);

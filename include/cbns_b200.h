@@ -78,6 +78,18 @@ extern "C" {
 #define CBNS_BC_REFERENCE 0
 #define CBNS_BC_FARFIELD  1
 
+/* cbns_init_case kinds (no counterpart in the reference) and their parameters:
+ *   VORTEX        Mach, strength beta, centre x, centre y, radius R, stream
+ *                 direction (dx, dy): isentropic vortex in a free stream
+ *   BLAST         r2_in, p_in, p_out: pressure p_in where x^2+y^2+z^2 < r2_in,
+ *                 p_out elsewhere, unit density, at rest
+ *   SHOCK_VORTEX  shock Mach Ms, vortex strength eps, radius rc, centre x,
+ *                 centre y, shock position x_s: stationary normal shock with a
+ *                 vortex in the upstream flow */
+#define CBNS_CASE_VORTEX       0
+#define CBNS_CASE_BLAST        1
+#define CBNS_CASE_SHOCK_VORTEX 2
+
 /* Run parameters: the fields of Block3dInfo that Block3d::read_input fills
  * (src/Block3d.cpp:33-138, include/Block3d_cuda.h:32-78) plus build-time
  * switches of the reference that are run-time options here.  The derived
@@ -117,6 +129,15 @@ int cbns_get_metrics(cbns_ctx* ctx, double* xi_x, double* xi_y, double* xi_z,
 int cbns_initial_condition(cbns_ctx* ctx);
 int cbns_calc_conservative(cbns_ctx* ctx, int which);
 int cbns_set_conservative(cbns_ctx* ctx, const double* Q_host);
+/* Initial state of a configuration case (CBNS_CASE_*, nprm <= 8 parameters
+ * as listed above) formed on the device from the grid coordinates (host,
+ * IM*JM*KM each, as cbns_calc_metrics), the coordinates extended into the
+ * ghost layers by odd reflection (k, then j, then i); the state of Q (and
+ * Q_p) on the whole ghosted box in the reference's units.  The same as
+ * forming it on the host and calling cbns_set_conservative, without the
+ * host work or the 5-field upload. */
+int cbns_init_case(cbns_ctx* ctx, int kind, const double* x, const double* y, const double* z, const double* prm,
+                   unsigned nprm);
 int cbns_get_conservative(cbns_ctx* ctx, int which, double* Q_host);
 /* Ghosted primitive arrays (IM_G*JM_G*KM_G each); T may be null. */
 int cbns_get_primitive(cbns_ctx* ctx, double* rho, double* u, double* v, double* w,

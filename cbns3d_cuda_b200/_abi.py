@@ -37,6 +37,7 @@ CASE_SHOCK_VORTEX = 2
 
 BC_REFERENCE = 0  # the reference's boundary conditions (parity contract)
 BC_FARFIELD = 1   # every boundary and ghost node holds the state it was set to
+BC_CHARACTERISTIC = 2  # Riemann-invariant far field against the free stream on every face
 
 
 class Params(C.Structure):

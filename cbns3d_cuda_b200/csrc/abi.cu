@@ -203,7 +203,11 @@ BCArgs bc_args(cbns_ctx* c, double* q, bool check_done, bool sigma) {
   a.st = c->st;
   a.check_done = check_done;
   a.sigma = sigma;
-  a.farfield = c->prm.bc_mode == CBNS_BC_FARFIELD;
+  a.farfield = c->prm.bc_mode == CBNS_BC_FARFIELD || c->prm.bc_mode == CBNS_BC_CHARACTERISTIC;
+  a.characteristic = c->prm.bc_mode == CBNS_BC_CHARACTERISTIC;
+  const double aoa = c->ph.angle_attack * 3.14159265358979323846 / 180.0;
+  a.u_inf = std::cos(aoa);
+  a.v_inf = std::sin(aoa);
   return a;
 }
 
@@ -691,7 +695,8 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   if (p->viscous != 0 && p->viscous != 1) return CBNS_ERR_ARG;
   if (p->precision < CBNS_PREC_FP64 || p->precision > CBNS_PREC_HYBRID) return CBNS_ERR_ARG;
   if (p->vis_divergence != CBNS_VISDIV_REFERENCE && p->vis_divergence != CBNS_VISDIV_CENTERED) return CBNS_ERR_ARG;
-  if (p->bc_mode != CBNS_BC_REFERENCE && p->bc_mode != CBNS_BC_FARFIELD) return CBNS_ERR_ARG;
+  if (p->bc_mode != CBNS_BC_REFERENCE && p->bc_mode != CBNS_BC_FARFIELD && p->bc_mode != CBNS_BC_CHARACTERISTIC)
+    return CBNS_ERR_ARG;
   for (int r : p->reserved)
     if (r != 0) return CBNS_ERR_ARG;
   const double ng = ((double)p->IM + 4) * ((double)p->JM + 4) * ((double)p->KM + 4);

@@ -13,7 +13,9 @@
 //            next time step (the boundary half of src/time_step_kernel.cu).
 // With CBNS_BC_FARFIELD (no counterpart in the reference) one kernel replaces
 // the three: boundary and ghost nodes keep their Q (a free-stream far field on
-// every face), only their primitives and spectral radii are formed.
+// every face), only their primitives and spectral radii are formed; with
+// CBNS_BC_CHARACTERISTIC three launches (i, j, k faces) first set every
+// boundary node and its ghosts to a characteristic far-field state.
 // The reference runs these as __syncthreads-separated phases of one kernel, so
 // its cross-CTA reads (wake mirror, k-face copies of j-face results) are races;
 // separate launches give the program-order result, which is what the reference
@@ -285,6 +287,80 @@ __global__ void bc_farfield(const BCArgs a) {
   if (!a.viscous && a.sigma) warp_sigma_max(a, sg, has);
 }
 
+// CBNS_BC_CHARACTERISTIC, one face direction per launch (dir 0 = i, 1 = j,
+// 2 = k; launched in that order).  Boundary node b, its inward neighbour e,
+// outward unit normal n = -+grad(xi_dir)/|grad(xi_dir)| at b.  Subsonic: the
+// outgoing invariant R+ = qn_e + 2c_e/(g-1) from e, the incoming
+// R- = qn_inf - 2c_inf/(g-1) from the free stream, qn_b = (R+ + R-)/2,
+// c_b = (g-1)(R+ - R-)/4; entropy p/rho^g and tangential velocity from e when
+// qn_b >= 0, from the free stream otherwise.  Supersonic (|qn_e| >= c_e):
+// outflow copies e, inflow takes the free stream.  b's two ghosts along dir
+// take b's state.  Dims of at least 4 keep e off the other face.
+__global__ void bc_characteristic(const BCArgs a, int dir) {
+  if (a.check_done && a.st->done) return;
+  const Dims& d = a.d;
+  const int n0 = dir == 0 ? d.JM : d.IM;
+  const int n1 = dir == 2 ? d.JM : d.KM;
+  const int nf = dir == 0 ? d.IM : dir == 1 ? d.JM : d.KM;
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 2L * n0 * n1) return;
+  const int side = (int)(t / ((long)n0 * n1));
+  const long r = t % ((long)n0 * n1);
+  const int f0 = (int)(r % n0), f1 = (int)(r / n0);
+  const int lb = side ? nf - 1 : 0;
+  const int i = dir == 0 ? lb : f0;
+  const int j = dir == 0 ? f0 : dir == 1 ? lb : f1;
+  const int k = dir == 2 ? lb : f1;
+  const long stride = dir == 0 ? 1L : dir == 1 ? d.PX : d.PL;
+  const long out = side ? stride : -stride;  // offset of the next node outward
+  const long ob = node_off(d, i, j, k), oe = ob - out;
+  const long VOL = d.VOL;
+  double* q = a.q;
+  const double mx = a.met[3 * dir][ob], my = a.met[3 * dir + 1][ob], mz = a.met[3 * dir + 2][ob];
+  const double sgn = side ? 1.0 : -1.0;
+  const double mn = sgn / sqrt(mx * mx + my * my + mz * mz);
+  const double nx = mx * mn, ny = my * mn, nz = mz * mn;
+  const PrimV se = prim_of(q, oe, VOL, a.gam1);
+  const double ce = sqrt(a.gamma * se.p / se.r);
+  const double qne = se.u * nx + se.v * ny + se.w * nz;
+  double qb[5];
+  if (fabs(qne) >= ce && qne >= 0.0) {
+#pragma unroll
+    for (int m = 0; m < 5; ++m) qb[m] = q[m * VOL + oe];
+  } else {
+    double r_b, u_b, v_b, w_b, p_b;
+    const double ci = sqrt(a.gamma * a.p_inf);  // rho_inf = 1
+    const double qni = a.u_inf * nx + a.v_inf * ny;
+    if (fabs(qne) >= ce) {
+      r_b = 1.0; u_b = a.u_inf; v_b = a.v_inf; w_b = 0.0; p_b = a.p_inf;
+    } else {
+      const double rp = qne + 2.0 * ce / a.gam1, rm = qni - 2.0 * ci / a.gam1;
+      const double qnb = 0.5 * (rp + rm), cb = 0.25 * a.gam1 * (rp - rm);
+      double s, dq;
+      if (qnb >= 0.0) {
+        s = se.p / pow(se.r, a.gamma);
+        dq = qnb - qne;
+        u_b = se.u + dq * nx; v_b = se.v + dq * ny; w_b = se.w + dq * nz;
+      } else {
+        s = a.p_inf;
+        dq = qnb - qni;
+        u_b = a.u_inf + dq * nx; v_b = a.v_inf + dq * ny; w_b = dq * nz;
+      }
+      r_b = pow(cb * cb / (a.gamma * s), 1.0 / a.gam1);
+      p_b = r_b * cb * cb / a.gamma;
+    }
+    qb[0] = r_b;
+    qb[1] = r_b * u_b;
+    qb[2] = r_b * v_b;
+    qb[3] = r_b * w_b;
+    qb[4] = p_b / a.gam1 + 0.5 * r_b * (u_b * u_b + v_b * v_b + w_b * w_b);
+  }
+#pragma unroll
+  for (int l = 0; l <= NG; ++l)
+#pragma unroll
+    for (int m = 0; m < 5; ++m) q[m * VOL + ob + l * out] = qb[m];
+}
+
 // Interior primitives (rho,u,v,w,p,T) from Q, the first part of
 // primitive_bc_kernel (:59-79); needed when the primitive arrays do not yet
 // describe the buffer the boundary conditions act on.
@@ -313,6 +389,12 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
     ++nl;
   }
   if (a.farfield) {
+    if (a.characteristic) {
+      bc_characteristic<<<nblk(2L * d.JM * d.KM, B), B, 0, s>>>(a, 0);
+      bc_characteristic<<<nblk(2L * d.IM * d.KM, B), B, 0, s>>>(a, 1);
+      bc_characteristic<<<nblk(2L * d.IM * d.JM, B), B, 0, s>>>(a, 2);
+      nl += 3;
+    }
     if (a.viscous || a.sigma) {
       bc_farfield<<<nblk((long)d.IG * d.JG * d.KG, B), B, 0, s>>>(a);
       ++nl;

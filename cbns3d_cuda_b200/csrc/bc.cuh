@@ -16,7 +16,10 @@ struct BCArgs {
   StepState* st;
   int check_done;        // return at once when st->done is set (graph-replayed steps)
   int sigma;             // inviscid: accumulate boundary-node spectral radii
-  int farfield;          // CBNS_BC_FARFIELD: boundary and ghost nodes hold their state
+  int farfield;          // boundary and ghost nodes hold their state (FARFIELD), or take the
+                         // characteristic far-field state (CHARACTERISTIC); primitives from Q
+  int characteristic;    // CBNS_BC_CHARACTERISTIC
+  double u_inf, v_inf;   // free-stream velocity (cos, sin of the angle of attack)
 };
 
 // interior_prims: also recompute interior primitives (viscous runs), when the

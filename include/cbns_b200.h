@@ -77,6 +77,15 @@ extern "C" {
  * radii are recomputed. */
 #define CBNS_BC_REFERENCE 0
 #define CBNS_BC_FARFIELD  1
+/* CHARACTERISTIC (no counterpart in the reference): a characteristic far field
+ * on all six faces against the free stream (rho 1, velocity (cos a, sin a, 0)
+ * at the angle of attack a, p_inf): per boundary node, Riemann invariants
+ * along the outward unit normal from the node one step inward and from the
+ * free stream; entropy and tangential velocity from the interior at outflow,
+ * from the free stream at inflow; supersonic inflow takes the free stream,
+ * supersonic outflow the interior node.  i faces, then j faces (all i), then
+ * k faces (all i, j), each node's two ghosts set to its state. */
+#define CBNS_BC_CHARACTERISTIC 2
 
 /* cbns_init_case kinds (no counterpart in the reference) and their parameters:
  *   VORTEX        Mach, strength beta, centre x, centre y, radius R, stream

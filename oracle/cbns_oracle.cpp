@@ -363,6 +363,68 @@ struct Oracle {
   }
 
   // ---------------------------------------------------------------------------
+  // CBNS_BC_CHARACTERISTIC (no counterpart in the reference), one face
+  // direction: every node of the dir = 0 / IM-1 (resp. JM-1, KM-1) faces takes
+  // the Riemann-invariant far-field state built from its inward neighbour and
+  // the free stream along the outward unit normal; its two ghosts copy it.
+  void bc_characteristic(std::vector<double>& Q, int dir) {
+    const double gamma = P.gamma, gam1 = D.gam1, p_inf = D.p_inf;
+    const double AoA = P.angle_attack * PI / 180.0;
+    const double u_inf = std::cos(AoA), v_inf = std::sin(AoA);
+    const long n0 = dir == 0 ? JM : IM, n1 = dir == 2 ? JM : KM, nf = dir == 0 ? IM : dir == 1 ? JM : KM;
+    for (int side = 0; side < 2; ++side)
+#pragma omp parallel for schedule(static)
+      for (long f1 = 0; f1 < n1; ++f1)
+        for (long f0 = 0; f0 < n0; ++f0) {
+          const long lb = side ? nf - 1 : 0, st = side ? 1 : -1;
+          long ijk[3] = {dir == 0 ? lb : f0, dir == 0 ? f0 : dir == 1 ? lb : f1, dir == 2 ? lb : f1};
+          const long tb = g(ijk[0], ijk[1], ijk[2]);
+          ijk[dir] -= st;
+          const long te = g(ijk[0], ijk[1], ijk[2]);
+          const double mx = met[3 * dir][tb], my = met[3 * dir + 1][tb], mz = met[3 * dir + 2][tb];
+          const double mn = (side ? 1.0 : -1.0) / std::sqrt(mx * mx + my * my + mz * mz);
+          const double nx = mx * mn, ny = my * mn, nz = mz * mn;
+          const Prim se = to_prim(&Q[5 * te], gam1);
+          const double ce = std::sqrt(gamma * se.p / se.r);
+          const double qne = se.u * nx + se.v * ny + se.w * nz;
+          double qb[5];
+          if (std::fabs(qne) >= ce && qne >= 0.0) {  // supersonic outflow
+            for (int m = 0; m < 5; ++m) qb[m] = Q[5 * te + m];
+          } else {
+            Prim b;
+            if (std::fabs(qne) >= ce) {  // supersonic inflow
+              b.r = 1.0; b.u = u_inf; b.v = v_inf; b.w = 0.0; b.p = p_inf;
+            } else {
+              const double ci = std::sqrt(gamma * p_inf);
+              const double qni = u_inf * nx + v_inf * ny;
+              const double rp = qne + 2.0 * ce / gam1, rm = qni - 2.0 * ci / gam1;
+              const double qnb = 0.5 * (rp + rm), cb = 0.25 * gam1 * (rp - rm);
+              double s;
+              if (qnb >= 0.0) {
+                s = se.p / std::pow(se.r, gamma);
+                const double dq = qnb - qne;
+                b.u = se.u + dq * nx; b.v = se.v + dq * ny; b.w = se.w + dq * nz;
+              } else {
+                s = p_inf;
+                const double dq = qnb - qni;
+                b.u = u_inf + dq * nx; b.v = v_inf + dq * ny; b.w = dq * nz;
+              }
+              b.r = std::pow(cb * cb / (gamma * s), 1.0 / gam1);
+              b.p = b.r * cb * cb / gamma;
+            }
+            qb[0] = b.r; qb[1] = b.r * b.u; qb[2] = b.r * b.v; qb[3] = b.r * b.w;
+            qb[4] = b.p / gam1 + 0.5 * b.r * (b.u * b.u + b.v * b.v + b.w * b.w);
+          }
+          ijk[dir] += st;
+          for (long l = 0; l <= NG; ++l) {
+            const long t = g(ijk[0], ijk[1], ijk[2]);
+            for (int m = 0; m < 5; ++m) Q[5 * t + m] = qb[m];
+            ijk[dir] += st;
+          }
+        }
+  }
+
+  // ---------------------------------------------------------------------------
   // set_bc_calc_primitive: src/primitive_bc_kernel.cu:13-494.  The kernel's
   // three __syncthreads-separated phases run here in order over the whole grid:
   //   1. interior primitives; i=0 and i=IM-1 faces (pressure reset to p_inf)
@@ -377,9 +439,11 @@ struct Oracle {
     for (long k = 1; k < KM - 1; ++k)
       for (long j = 1; j < JM - 1; ++j)
         for (long i = 1; i < IM - 1; ++i) put_prim(g(i, j, k), to_prim(&Q[5 * g(i, j, k)], gam1));
-    if (P.bc_mode == CBNS_BC_FARFIELD) {
-      // no counterpart in the reference: boundary and ghost nodes keep their Q,
-      // their primitives follow from it
+    if (P.bc_mode == CBNS_BC_FARFIELD || P.bc_mode == CBNS_BC_CHARACTERISTIC) {
+      // no counterpart in the reference: boundary and ghost nodes keep their Q
+      // (or first take the characteristic state), their primitives follow from it
+      if (P.bc_mode == CBNS_BC_CHARACTERISTIC)
+        for (int dir = 0; dir < 3; ++dir) bc_characteristic(Q, dir);
 #pragma omp parallel for schedule(static)
       for (long k = -NG; k < KM + NG; ++k)
         for (long j = -NG; j < JM + NG; ++j)

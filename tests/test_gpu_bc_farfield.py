@@ -6,12 +6,14 @@ vortex and batched-block configurations ask for and the reference lacks:
 * the CUDA path matches the CPU oracle's far-field mode to the plain path's
   1e-10 after 20 steps, inviscid and viscous;
 * the mode changes the solution near the boundaries (it is not the
-  reference's boundary conditions).
+  reference's boundary conditions);
+* the characteristic far field (BC_CHARACTERISTIC) matches the oracle's to
+  1e-10 after 20 steps, graph and per-call paths, inviscid and viscous.
 """
 import numpy as np
 import pytest
 
-from cbns3d_cuda_b200 import BC_FARFIELD, cases
+from cbns3d_cuda_b200 import BC_CHARACTERISTIC, BC_FARFIELD, cases
 from tests.helpers import per_var_rel_linf
 from tests.test_gpu_parity import pair
 
@@ -59,3 +61,26 @@ def test_farfield_differs_from_reference_mode():
         assert x.run(20) == 20
     assert not np.array_equal(a.get_conservative(), b.get_conservative())
     assert np.all(np.isfinite(a.get_conservative()))
+
+
+@pytest.mark.parametrize("viscous", [False, True])
+@pytest.mark.parametrize("graph", [False, True])
+def test_characteristic_matches_oracle(viscous, graph):
+    c = cases.case_vortex(24, 16, 10)
+    over = dict(bc_mode=BC_CHARACTERISTIC)
+    if viscous:
+        over.update(viscous=True, Re=500.0)
+    g, o = pair(c, **over)
+    n = 20
+    if graph:
+        g.set_time(0.0)
+        assert g.run(n) == n
+    else:
+        t = 0.0
+        for _ in range(n):
+            t = g.step_like_reference(t, 1.0e30)
+    rc, _, no = o.solve(n, 1.0e30)
+    assert rc == 0 and no == n
+    q = g.get_conservative()
+    assert np.all(np.isfinite(q))
+    assert max(per_var_rel_linf(q, o.get_conservative())) <= 1e-10

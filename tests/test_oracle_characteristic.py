@@ -1,0 +1,104 @@
+"""The oracle's characteristic far-field mode (BC_CHARACTERISTIC), checked
+through properties of the Riemann-invariant state it sets on the i faces of a
+Cartesian box (outward normals -x and +x):
+
+* subsonic outflow face: the outgoing invariant qn + 2c/(g-1) and the entropy
+  p/rho^g equal the inward neighbour's, the incoming qn - 2c/(g-1) the free
+  stream's, the tangential velocity is the neighbour's;
+* subsonic inflow face: outgoing invariant from the neighbour, incoming one,
+  entropy and tangential velocity from the free stream;
+* supersonic: the inflow face takes the free stream, the outflow face copies
+  the neighbour bit for bit; ghosts copy their boundary node;
+* a uniform free stream stays uniform over steps.
+"""
+import numpy as np
+
+from cbns3d_cuda_b200 import BC_CHARACTERISTIC, CBNS_Q, cases, make_params
+from oracle import oracle as orc
+
+
+def _box(IM=20, JM=14, KM=10, Mach=0.5):
+    c = cases.case_vortex(IM, JM, KM, Mach=Mach)
+    c.x, c.y, c.z = cases.perturbed_box(IM, JM, KM, amp=0.0)
+    return c
+
+
+def _apply(c, Q):
+    o = orc.OracleBlock(make_params(*c.shape, **c.params, bc_mode=BC_CHARACTERISTIC))
+    o.calc_metrics(c.x, c.y, c.z)
+    o.set_conservative(Q.reshape(-1))
+    o.set_bc_calc_primitive(CBNS_Q)
+    return o
+
+
+def _prims(q, g):
+    r = q[..., 0]
+    u, v, w = q[..., 1] / r, q[..., 2] / r, q[..., 3] / r
+    p = (g - 1.0) * (q[..., 4] - 0.5 * r * (u * u + v * v + w * w))
+    return r, u, v, w, p
+
+
+def test_subsonic_faces_follow_the_invariants(oracle_lib):
+    c = _box()
+    IM, JM, KM = c.shape
+    g = c.params["gamma"]
+    g1 = g - 1.0
+    p_inf = 1.0 / (g * c.params["Mach"] ** 2)
+    c_inf = np.sqrt(g * p_inf)
+    q = _apply(c, c.Q0).get_conservative().reshape(KM + 4, JM + 4, IM + 4, 5)
+    inner = (slice(3, KM + 1), slice(3, JM + 1))  # j, k away from the other faces
+    for ib, ie, sgn in ((2, 3, -1.0), (IM + 1, IM, 1.0)):
+        rb, ub, vb, wb, pb = _prims(q[inner + (ib,)], g)
+        re, ue, ve, we, pe = _prims(q[inner + (ie,)], g)
+        cb, ce = np.sqrt(g * pb / rb), np.sqrt(g * pe / re)
+        qnb, qne, qni = sgn * ub, sgn * ue, sgn * 1.0
+        assert np.all(np.abs(qne) < ce)
+        np.testing.assert_allclose(qnb + 2 * cb / g1, qne + 2 * ce / g1, rtol=0, atol=1e-12)
+        np.testing.assert_allclose(qnb - 2 * cb / g1, qni - 2 * c_inf / g1, rtol=0, atol=1e-12)
+        if sgn > 0:  # outflow: entropy and tangential velocity of the neighbour
+            assert np.all(qnb >= 0)
+            np.testing.assert_allclose(pb / rb ** g, pe / re ** g, rtol=1e-12)
+            np.testing.assert_allclose(vb, ve, rtol=0, atol=1e-13)
+            np.testing.assert_allclose(wb, we, rtol=0, atol=1e-13)
+        else:  # inflow: entropy and tangential velocity of the free stream
+            assert np.all(qnb < 0)
+            np.testing.assert_allclose(pb / rb ** g, p_inf, rtol=1e-12)
+            np.testing.assert_allclose(vb, 0.0, rtol=0, atol=1e-13)
+            np.testing.assert_allclose(wb, 0.0, rtol=0, atol=1e-13)
+        for l in (1, 2):  # ghosts copy the boundary node
+            gi = ib - l if sgn < 0 else ib + l
+            assert np.array_equal(q[inner + (gi,)], q[inner + (ib,)])
+
+
+def test_supersonic_faces(oracle_lib):
+    c = _box(Mach=2.0)
+    IM, JM, KM = c.shape
+    g = c.params["gamma"]
+    p_inf = 1.0 / (g * 4.0)
+    Q = np.zeros((KM + 4, JM + 4, IM + 4, 5))
+    rng = np.random.default_rng(3)
+    Q[..., 0] = 1.0 + 0.05 * rng.random(Q.shape[:3])
+    Q[..., 1] = Q[..., 0] * 1.0
+    Q[..., 4] = p_inf / (g - 1.0) + 0.5 * Q[..., 0]
+    q = _apply(c, Q).get_conservative().reshape(Q.shape)
+    inner = (slice(3, KM + 1), slice(3, JM + 1))
+    free = np.array([1.0, 1.0, 0.0, 0.0, p_inf / (g - 1.0) + 0.5])
+    for i in (0, 1, 2):  # inflow face and its ghosts
+        np.testing.assert_allclose(q[inner + (i,)], np.broadcast_to(free, q[inner + (i,)].shape), rtol=1e-15, atol=1e-15)
+    for i in (IM + 1, IM + 2, IM + 3):  # outflow face and ghosts copy i = IM-2
+        assert np.array_equal(q[inner + (i,)], Q[inner + (IM,)])
+
+
+def test_free_stream_stays_uniform(oracle_lib):
+    c = _box()
+    IM, JM, KM = c.shape
+    g = c.params["gamma"]
+    p_inf = 1.0 / (g * c.params["Mach"] ** 2)
+    Q = np.zeros((KM + 4, JM + 4, IM + 4, 5))
+    Q[..., 0] = 1.0
+    Q[..., 1] = 1.0
+    Q[..., 4] = p_inf / (g - 1.0) + 0.5
+    o = _apply(c, Q)
+    rc, _, n = o.solve(5, 1.0e30)
+    assert rc == 0 and n == 5
+    assert np.max(np.abs(o.get_conservative() - Q.reshape(-1))) <= 1e-8

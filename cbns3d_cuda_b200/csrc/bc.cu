@@ -295,12 +295,16 @@ __global__ void bc_farfield(const BCArgs a) {
 // c_b = (g-1)(R+ - R-)/4; entropy p/rho^g and tangential velocity from e when
 // qn_b >= 0, from the free stream otherwise.  Supersonic (|qn_e| >= c_e):
 // outflow copies e, inflow takes the free stream.  b's two ghosts along dir
-// take b's state.  Dims of at least 4 keep e off the other face.
+// take b's state.  The i faces cover j, k interior, the j faces every i and
+// k interior, the k faces every (i, j): every e is an interior node or a
+// face node set earlier in the same call, so the state depends on the
+// buffer's interior only (not on its history).  Ghosts off those lines keep
+// their state.  Dims of at least 4 keep e off the other face.
 __global__ void bc_characteristic(const BCArgs a, int dir) {
   if (a.check_done && a.st->done) return;
   const Dims& d = a.d;
-  const int n0 = dir == 0 ? d.JM : d.IM;
-  const int n1 = dir == 2 ? d.JM : d.KM;
+  const int n0 = dir == 0 ? d.JM - 2 : d.IM;
+  const int n1 = dir == 2 ? d.JM : d.KM - 2;
   const int nf = dir == 0 ? d.IM : dir == 1 ? d.JM : d.KM;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (t >= 2L * n0 * n1) return;
@@ -309,8 +313,8 @@ __global__ void bc_characteristic(const BCArgs a, int dir) {
   const int f0 = (int)(r % n0), f1 = (int)(r / n0);
   const int lb = side ? nf - 1 : 0;
   const int i = dir == 0 ? lb : f0;
-  const int j = dir == 0 ? f0 : dir == 1 ? lb : f1;
-  const int k = dir == 2 ? lb : f1;
+  const int j = dir == 0 ? f0 + 1 : dir == 1 ? lb : f1;
+  const int k = dir == 2 ? lb : f1 + 1;
   const long stride = dir == 0 ? 1L : dir == 1 ? d.PX : d.PL;
   const long out = side ? stride : -stride;  // offset of the next node outward
   const long ob = node_off(d, i, j, k), oe = ob - out;
@@ -390,8 +394,8 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
   }
   if (a.farfield) {
     if (a.characteristic) {
-      bc_characteristic<<<nblk(2L * d.JM * d.KM, B), B, 0, s>>>(a, 0);
-      bc_characteristic<<<nblk(2L * d.IM * d.KM, B), B, 0, s>>>(a, 1);
+      bc_characteristic<<<nblk(2L * (d.JM - 2) * (d.KM - 2), B), B, 0, s>>>(a, 0);
+      bc_characteristic<<<nblk(2L * d.IM * (d.KM - 2), B), B, 0, s>>>(a, 1);
       bc_characteristic<<<nblk(2L * d.IM * d.JM, B), B, 0, s>>>(a, 2);
       nl += 3;
     }

@@ -50,6 +50,7 @@ cbns_params params_of(const Block3dInfo* b) {
   p.viscous = b->is_viscous;
   p.precision = b->precision;
   p.vis_divergence = b->vis_divergence;
+  p.bc_mode = b->bc_mode;
   return p;
 }
 

@@ -61,6 +61,7 @@ void Block3d::read_input() {
   info_.is_viscous = opt_.viscous;
   info_.precision = opt_.precision;
   info_.vis_divergence = opt_.vis_divergence;
+  info_.bc_mode = opt_.bc_mode;
   info_.sensor_weights = opt_.sensor.empty() ? nullptr : opt_.sensor.c_str();
 }
 

@@ -17,6 +17,7 @@ class Block3d {
     bool graph = false;      // whole steps from a CUDA graph (dt stays on the device)
     int precision = CBNS_PREC_FP64;
     int vis_divergence = CBNS_VISDIV_REFERENCE;
+    int bc_mode = CBNS_BC_REFERENCE;
     int viscous = CBNS_SHIM_VISCOUS_DEFAULT;
     std::string input = "input.txt";
     std::string sensor = "";  // learned-sensor weights (precision hybrid)

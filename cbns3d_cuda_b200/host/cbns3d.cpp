@@ -8,6 +8,7 @@
 //                    trained weights shipped beside this executable,
 //                    ../data/sensor_weights.bin)
 //   --visdiv D       reference (default) | centered
+//   --bc B           reference (default) | farfield | characteristic
 //   --inviscid / --viscous   override the build-time default
 //   --input FILE     parameter file (default input.txt)
 //   --vtk-binary     output.vtk in legacy VTK BINARY (same data set as the
@@ -44,6 +45,15 @@ int main(int argc, char** argv) {
       o.precision = v == "split" ? CBNS_PREC_SPLIT : (v == "hybrid" ? CBNS_PREC_HYBRID : CBNS_PREC_FP64);
     } else if (s == "--sensor") {
       o.sensor = next();
+    } else if (s == "--bc") {
+      const std::string v = next();
+      if (v == "reference") o.bc_mode = CBNS_BC_REFERENCE;
+      else if (v == "farfield") o.bc_mode = CBNS_BC_FARFIELD;
+      else if (v == "characteristic") o.bc_mode = CBNS_BC_CHARACTERISTIC;
+      else {
+        std::cerr << "unknown boundary mode " << v << "\n";
+        return 2;
+      }
     } else if (s == "--visdiv") {
       o.vis_divergence = next() == "centered" ? CBNS_VISDIV_CENTERED : CBNS_VISDIV_REFERENCE;
     } else {

@@ -90,6 +90,7 @@ struct Block3dInfo {
   int is_viscous = CBNS_SHIM_VISCOUS_DEFAULT;
   int precision = CBNS_PREC_FP64;
   int vis_divergence = CBNS_VISDIV_REFERENCE;
+  int bc_mode = CBNS_BC_REFERENCE;  /* CBNS_BC_*: the reference's boundaries by default */
   /* weights file of the learned sensor (cbns_sensor_load_file), required when
    * precision is CBNS_PREC_HYBRID */
   const char* sensor_weights = nullptr;

@@ -83,8 +83,9 @@ extern "C" {
  * along the outward unit normal from the node one step inward and from the
  * free stream; entropy and tangential velocity from the interior at outflow,
  * from the free stream at inflow; supersonic inflow takes the free stream,
- * supersonic outflow the interior node.  i faces, then j faces (all i), then
- * k faces (all i, j), each node's two ghosts set to its state. */
+ * supersonic outflow the inward node.  i faces (j, k interior), then j faces
+ * (all i, k interior), then k faces (all i, j), each node's two ghosts set to
+ * its state; the state depends on the buffer's interior only. */
 #define CBNS_BC_CHARACTERISTIC 2
 
 /* cbns_init_case kinds (no counterpart in the reference) and their parameters:

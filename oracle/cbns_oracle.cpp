@@ -367,17 +367,19 @@ struct Oracle {
   // direction: every node of the dir = 0 / IM-1 (resp. JM-1, KM-1) faces takes
   // the Riemann-invariant far-field state built from its inward neighbour and
   // the free stream along the outward unit normal; its two ghosts copy it.
+  // i faces over j, k interior, j faces over all i and k interior, k faces
+  // over all (i, j), so each neighbour is interior or set earlier in the call.
   void bc_characteristic(std::vector<double>& Q, int dir) {
     const double gamma = P.gamma, gam1 = D.gam1, p_inf = D.p_inf;
     const double AoA = P.angle_attack * PI / 180.0;
     const double u_inf = std::cos(AoA), v_inf = std::sin(AoA);
-    const long n0 = dir == 0 ? JM : IM, n1 = dir == 2 ? JM : KM, nf = dir == 0 ? IM : dir == 1 ? JM : KM;
+    const long n0 = dir == 0 ? JM - 2 : IM, n1 = dir == 2 ? JM : KM - 2, nf = dir == 0 ? IM : dir == 1 ? JM : KM;
     for (int side = 0; side < 2; ++side)
 #pragma omp parallel for schedule(static)
       for (long f1 = 0; f1 < n1; ++f1)
         for (long f0 = 0; f0 < n0; ++f0) {
           const long lb = side ? nf - 1 : 0, st = side ? 1 : -1;
-          long ijk[3] = {dir == 0 ? lb : f0, dir == 0 ? f0 : dir == 1 ? lb : f1, dir == 2 ? lb : f1};
+          long ijk[3] = {dir == 0 ? lb : f0, dir == 0 ? f0 + 1 : dir == 1 ? lb : f1, dir == 2 ? lb : f1 + 1};
           const long tb = g(ijk[0], ijk[1], ijk[2]);
           ijk[dir] -= st;
           const long te = g(ijk[0], ijk[1], ijk[2]);

@@ -5,7 +5,9 @@
   (to the ASCII file's 7 significant digits);
 * --plot3d writes output.xyz / output.q in binary Plot3D: the input grid and
   the final conservative state, equal bit for bit to the grid file and the
-  checkpoint's interior.
+  checkpoint's interior;
+* --bc characteristic runs the characteristic far-field mode: the checkpoint
+  matches the library's own run of that mode.
 """
 import subprocess
 from pathlib import Path
@@ -13,7 +15,9 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from cbns3d_cuda_b200 import cases
+from cbns3d_cuda_b200 import BC_CHARACTERISTIC, cases
+from tests.helpers import per_var_rel_linf
+from tests.test_gpu_parity import pair
 
 pytestmark = pytest.mark.gpu
 
@@ -46,3 +50,14 @@ def test_binary_vtk_and_plot3d(tmp_path):
     t_ck, Q = cases.read_checkpoint(db / "checkpoint.dat")
     assert t == t_ck and mach == c.params["Mach"]
     assert np.array_equal(q, np.moveaxis(Q[2:-2, 2:-2, 2:-2, :], -1, 0))
+
+
+def test_bc_option(tmp_path):
+    c = cases.case_vortex(20, 14, 10)
+    d = c.write(tmp_path / "char", nsteps=5, checkpoint_freq=5)
+    _run(d, "--bc", "characteristic")
+    _, Q = cases.read_checkpoint(d / "checkpoint.dat")
+    g, _ = pair(c, bc_mode=BC_CHARACTERISTIC)
+    g.set_time(0.0)
+    assert g.run(5) == 5
+    assert max(per_var_rel_linf(Q.reshape(-1), g.get_conservative())) <= 1e-12

@@ -12,11 +12,12 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from ._abi import (BC_CHARACTERISTIC, BC_FARFIELD, BC_REFERENCE, CBNS_Q, CBNS_QP, PREC_FP64, PREC_HYBRID, PREC_SPLIT,  # noqa: F401
+from ._abi import (BC_CHARACTERISTIC, BC_FARFIELD, BC_OGRID, BC_REFERENCE, OGRID_WRAP, CBNS_Q, CBNS_QP, PREC_FP64, PREC_HYBRID, PREC_SPLIT,  # noqa: F401
                    VISDIV_CENTERED, VISDIV_REFERENCE, CbnsError, Params)
 
 __all__ = ["Block", "Batch", "Params", "CbnsError", "CBNS_Q", "CBNS_QP", "PREC_FP64", "PREC_SPLIT", "PREC_HYBRID",
-           "VISDIV_REFERENCE", "VISDIV_CENTERED", "BC_REFERENCE", "BC_FARFIELD", "BC_CHARACTERISTIC", "make_params"]
+           "VISDIV_REFERENCE", "VISDIV_CENTERED", "BC_REFERENCE", "BC_FARFIELD", "BC_CHARACTERISTIC", "BC_OGRID", "OGRID_WRAP",
+           "make_params"]
 
 NG = 2
 NEQ = 5

@@ -38,6 +38,8 @@ CASE_SHOCK_VORTEX = 2
 BC_REFERENCE = 0  # the reference's boundary conditions (parity contract)
 BC_FARFIELD = 1   # every boundary and ghost node holds the state it was set to
 BC_CHARACTERISTIC = 2  # Riemann-invariant far field against the free stream on every face
+BC_OGRID = 3      # i wraps around (OGRID_WRAP copied points either side), wall j = 0, characteristic j = JM-1
+OGRID_WRAP = 4
 
 
 class Params(C.Structure):

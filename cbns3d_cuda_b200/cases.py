@@ -278,6 +278,13 @@ def naca0012_ogrid(IM, JM, KM, first=1.0e-5, far=20.0, span=0.1):
     return x, y, z, r
 
 
+def ogrid_wrap(a, wrap=4):
+    """The block layout of the O-grid boundary mode (bc_mode = 3): the
+    periodic line of P points along i (last axis) stored with `wrap` copies of
+    the points across the seam on either side, P + 2*wrap points in all."""
+    return np.concatenate([a[..., -wrap:], a, a[..., :wrap]], axis=-1)
+
+
 # ---------------------------------------------------------------- initial states
 def isentropic_vortex(xg, yg, Mach, beta, xc, yc, R, gamma=1.4, u_dir=(1.0, 0.0)):
     """Isentropic vortex of strength beta (in units of the free-stream sound
@@ -320,6 +327,19 @@ def case_naca(IM=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5):
     params = dict(CFL=CFL, Mach=0.8, angle_attack=1.25, Re=5.0e4, Pr=0.72, Pr_t=0.9, T_inf=288.15, gamma=1.4,
                   i_begin=1, i_end=IM, viscous=True)
     return Case("naca", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)
+
+
+def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, viscous=True):
+    """configs[1] with its own boundaries (bc_mode = 3, BC_OGRID): the NACA 0012
+    O-grid of P points around the profile, wrapped periodically in i (stored
+    with 4 copied points either side, IM = P + 8), adiabatic no-slip wall on
+    j = 0 (slip when inviscid), characteristic far field on j = JM-1; M 0.8,
+    AoA 1.25 deg, Re 5e4, free-stream start."""
+    x, y, z, _ = naca0012_ogrid(P, JM, KM, first=first)
+    x, y, z = (ogrid_wrap(a) for a in (x, y, z))
+    params = dict(CFL=CFL, Mach=0.8, angle_attack=1.25, Re=5.0e4, Pr=0.72, Pr_t=0.9, T_inf=288.15, gamma=1.4,
+                  i_begin=1, i_end=P + 8, viscous=viscous, bc_mode=3)
+    return Case("naca_ogrid", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)
 
 
 def case_blast(IM=384, JM=384, KM=384, t_end=0.05, CFL=0.5):

@@ -205,6 +205,7 @@ BCArgs bc_args(cbns_ctx* c, double* q, bool check_done, bool sigma) {
   a.sigma = sigma;
   a.farfield = c->prm.bc_mode == CBNS_BC_FARFIELD || c->prm.bc_mode == CBNS_BC_CHARACTERISTIC;
   a.characteristic = c->prm.bc_mode == CBNS_BC_CHARACTERISTIC;
+  a.wrap = c->prm.bc_mode == CBNS_BC_OGRID ? CBNS_OGRID_WRAP : 0;
   const double aoa = c->ph.angle_attack * 3.14159265358979323846 / 180.0;
   a.u_inf = std::cos(aoa);
   a.v_inf = std::sin(aoa);
@@ -406,6 +407,7 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step
 }
 
 bool hybrid(const cbns_ctx* c) { return c->ph.precision == CBNS_PREC_HYBRID; }
+bool ogrid(const cbns_ctx* c) { return c->prm.bc_mode == CBNS_BC_OGRID; }
 
 // One SSP-RK3 step on the fixed buffer roles P0 = Q, P1 = spare, P2 = Q_p.
 int enqueue_step(cbns_ctx* c) {
@@ -425,8 +427,12 @@ int enqueue_step(cbns_ctx* c) {
   } s[3] = {{P0, P0, P0, P1}, {P1, P0, P1, P2}, {P2, P0, P2, P0}};
   for (int k = 0; k < 3; ++k) {
     const bool last = k == 2;
-    RET(stage_launch(c, stage_args(c, s[k].src, s[k].q0, s[k].qp, s[k].out, last && !visc), k + 1));
-    RET(bc_launch(c, bc_args(c, s[k].out, true, last && !visc), false));
+    // O-grid: the wrap copy rewrites nodes stage 3 updated, so the spectral
+    // radius is swept after the boundary pass
+    const bool fuse = last && !visc && !ogrid(c);
+    RET(stage_launch(c, stage_args(c, s[k].src, s[k].q0, s[k].qp, s[k].out, fuse), k + 1));
+    RET(bc_launch(c, bc_args(c, s[k].out, true, fuse), false));
+    if (last && !visc && ogrid(c)) RET(sigma_launch(c));
     if (visc) RET(visc_launch(c, visc_args(c, true, last)));
   }
   return CBNS_OK;
@@ -695,8 +701,11 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   if (p->viscous != 0 && p->viscous != 1) return CBNS_ERR_ARG;
   if (p->precision < CBNS_PREC_FP64 || p->precision > CBNS_PREC_HYBRID) return CBNS_ERR_ARG;
   if (p->vis_divergence != CBNS_VISDIV_REFERENCE && p->vis_divergence != CBNS_VISDIV_CENTERED) return CBNS_ERR_ARG;
-  if (p->bc_mode != CBNS_BC_REFERENCE && p->bc_mode != CBNS_BC_FARFIELD && p->bc_mode != CBNS_BC_CHARACTERISTIC)
+  if (p->bc_mode < CBNS_BC_REFERENCE || p->bc_mode > CBNS_BC_OGRID) return CBNS_ERR_ARG;
+  if (p->bc_mode == CBNS_BC_OGRID && p->IM - 2 * CBNS_OGRID_WRAP < 6) {
+    g_last = "an O-grid block needs IM - 2*CBNS_OGRID_WRAP >= 6";
     return CBNS_ERR_ARG;
+  }
   for (int r : p->reserved)
     if (r != 0) return CBNS_ERR_ARG;
   const double ng = ((double)p->IM + 4) * ((double)p->JM + 4) * ((double)p->KM + 4);
@@ -859,9 +868,10 @@ int cbns_calc_metrics(cbns_ctx* c, const double* x, const double* y, const doubl
   CK(cudaMemcpyAsync(sx, x, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(sx + N, y, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(sx + 2 * N, z, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const int wrap = ogrid(c) ? CBNS_OGRID_WRAP : 0;
   CK(launch_metrics(c->d, sx, sx + N, sx + 2 * N, c->f.met, c->f.area,
-                    c->f.area32[0] ? c->f.area32 : nullptr, c->stream));
-  c->launches += 3;
+                    c->f.area32[0] ? c->f.area32 : nullptr, wrap, c->stream));
+  c->launches += wrap ? 4 : 3;
   RET(sync(c));
   c->have_metrics = true;
   c->sigma_valid = false;
@@ -1039,7 +1049,7 @@ int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
   // inviscid stage 3 accumulates the spectral radius of the interior nodes it
   // updates; set_bc_calc_primitive(Q) adds the boundary nodes, and the next
   // cbns_calc_dt reads the maximum instead of sweeping the grid again
-  const bool sigma = stage == 3 && !c->ph.viscous;
+  const bool sigma = stage == 3 && !c->ph.viscous && !ogrid(c);
   if (sigma) CK(cudaMemsetAsync(&c->st->sigma_bits, 0, sizeof(unsigned long long), c->stream));
   const StageArgs a = stage_args(c, c->qb[src], c->qb[c->lq], c->qb[c->lp], c->qb[out], sigma);
   RET(stage_launch(c, a, (int)stage));
@@ -1409,6 +1419,10 @@ int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, c
     RET(check_flux_ready(blocks[i]));
     if (blocks[i]->ph.viscous != blocks[0]->ph.viscous || blocks[i]->ph.precision != blocks[0]->ph.precision) {
       g_last = "the blocks of a batch share the precision and the viscous flag";
+      return CBNS_ERR_ARG;
+    }
+    if (ogrid(blocks[i])) {
+      g_last = "O-grid blocks (CBNS_BC_OGRID) cannot join a batch";
       return CBNS_ERR_ARG;
     }
   }

@@ -15,7 +15,9 @@
 // the three: boundary and ghost nodes keep their Q (a free-stream far field on
 // every face), only their primitives and spectral radii are formed; with
 // CBNS_BC_CHARACTERISTIC three launches (i, j, k faces) first set every
-// boundary node and its ghosts to a characteristic far-field state.
+// boundary node and its ghosts to a characteristic far-field state.  With
+// CBNS_BC_OGRID: phase 2 with the wall on every i, the characteristic state on
+// j = JM-1, phase 3, then the copies across the periodic seam in i.
 // The reference runs these as __syncthreads-separated phases of one kernel, so
 // its cross-CTA reads (wake mirror, k-face copies of j-face results) are races;
 // separate launches give the program-order result, which is what the reference
@@ -300,15 +302,15 @@ __global__ void bc_farfield(const BCArgs a) {
 // face node set earlier in the same call, so the state depends on the
 // buffer's interior only (not on its history).  Ghosts off those lines keep
 // their state.  Dims of at least 4 keep e off the other face.
-__global__ void bc_characteristic(const BCArgs a, int dir) {
+__global__ void bc_characteristic(const BCArgs a, int dir, int side0, int nsides) {
   if (a.check_done && a.st->done) return;
   const Dims& d = a.d;
   const int n0 = dir == 0 ? d.JM - 2 : d.IM;
   const int n1 = dir == 2 ? d.JM : d.KM - 2;
   const int nf = dir == 0 ? d.IM : dir == 1 ? d.JM : d.KM;
   const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= 2L * n0 * n1) return;
-  const int side = (int)(t / ((long)n0 * n1));
+  if (t >= (long)nsides * n0 * n1) return;
+  const int side = side0 + (int)(t / ((long)n0 * n1));
   const long r = t % ((long)n0 * n1);
   const int f0 = (int)(r % n0), f1 = (int)(r / n0);
   const int lb = side ? nf - 1 : 0;
@@ -365,6 +367,32 @@ __global__ void bc_characteristic(const BCArgs a, int dir) {
     for (int m = 0; m < 5; ++m) q[m * VOL + ob + l * out] = qb[m];
 }
 
+// CBNS_BC_OGRID, last pass: every node with i < wrap or i >= IM - wrap, the
+// i ghosts included, over the whole ghosted (j, k) box, takes Q (and in
+// viscous runs the primitives) of the node P = IM - 2*wrap away, which lies
+// on the stored periodic line and is final by now.
+__global__ void bc_wrap(const BCArgs a) {
+  if (a.check_done && a.st->done) return;
+  const Dims& d = a.d;
+  const int W = a.wrap + NG;  // copied positions either side
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= 2L * W * d.JG * d.KG) return;
+  const int u = (int)(t % (2 * W));
+  const long r = t / (2 * W);
+  const int j = (int)(r % d.JG) - NG, k = (int)(r / d.JG) - NG;
+  const int P = d.IM - 2 * a.wrap;
+  const int i = u < W ? u - NG : d.IM - a.wrap + (u - W);
+  const int src = u < W ? i + P : i - P;
+  const long o = node_off(d, i, j, k), os = node_off(d, src, j, k);
+  const long VOL = d.VOL;
+#pragma unroll
+  for (int c = 0; c < NEQ; ++c) a.q[c * VOL + o] = a.q[c * VOL + os];
+  if (a.viscous) {
+#pragma unroll
+    for (int m = 0; m < 6; ++m) a.prim[m][o] = a.prim[m][os];
+  }
+}
+
 // Interior primitives (rho,u,v,w,p,T) from Q, the first part of
 // primitive_bc_kernel (:59-79); needed when the primitive arrays do not yet
 // describe the buffer the boundary conditions act on.
@@ -392,11 +420,27 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
     bc_interior_prims<<<nblk((long)(d.IM - 2) * (d.JM - 2) * (d.KM - 2), B), B, 0, s>>>(a);
     ++nl;
   }
+  const long n3 = (long)d.IM * (d.KM - 2) + (long)(d.JM - 2) * (d.KM - 2) + (long)d.IM * d.JM;
+  if (a.wrap) {
+    // O-grid: wall on every i of j = 0, characteristic far field on j = JM-1,
+    // the reference's k faces, then the copies across the seam
+    BCArgs w = a;
+    w.i_begin = 1u;
+    w.i_end = (unsigned)d.IM;
+    w.sigma = 0;
+    bc_phase2<<<nblk((long)d.IM * (d.KM - 2), B), B, 0, s>>>(w);
+    bc_characteristic<<<nblk((long)d.IM * (d.KM - 2), B), B, 0, s>>>(w, 1, 1, 1);
+    bc_phase3<<<nblk(n3, B), B, 0, s>>>(w);
+    bc_wrap<<<nblk(2L * (a.wrap + NG) * d.JG * d.KG, B), B, 0, s>>>(w);
+    nl += 4;
+    if (launches) *launches += nl;
+    return cudaGetLastError();
+  }
   if (a.farfield) {
     if (a.characteristic) {
-      bc_characteristic<<<nblk(2L * (d.JM - 2) * (d.KM - 2), B), B, 0, s>>>(a, 0);
-      bc_characteristic<<<nblk(2L * d.IM * (d.KM - 2), B), B, 0, s>>>(a, 1);
-      bc_characteristic<<<nblk(2L * d.IM * d.JM, B), B, 0, s>>>(a, 2);
+      bc_characteristic<<<nblk(2L * (d.JM - 2) * (d.KM - 2), B), B, 0, s>>>(a, 0, 0, 2);
+      bc_characteristic<<<nblk(2L * d.IM * (d.KM - 2), B), B, 0, s>>>(a, 1, 0, 2);
+      bc_characteristic<<<nblk(2L * d.IM * d.JM, B), B, 0, s>>>(a, 2, 0, 2);
       nl += 3;
     }
     if (a.viscous || a.sigma) {
@@ -415,7 +459,6 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
     bc_phase2<<<nblk((long)d.IM * (d.KM - 2), B), B, 0, s>>>(a);
     ++nl;
   }
-  const long n3 = (long)d.IM * (d.KM - 2) + (long)(d.JM - 2) * (d.KM - 2) + (long)d.IM * d.JM;
   bc_phase3<<<nblk(n3, B), B, 0, s>>>(a);
   ++nl;
   if (launches) *launches += nl;

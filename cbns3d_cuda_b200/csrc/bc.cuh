@@ -20,6 +20,7 @@ struct BCArgs {
                          // characteristic far-field state (CHARACTERISTIC); primitives from Q
   int characteristic;    // CBNS_BC_CHARACTERISTIC
   double u_inf, v_inf;   // free-stream velocity (cos, sin of the angle of attack)
+  int wrap;              // CBNS_BC_OGRID: number of copied points either side of the seam, else 0
 };
 
 // interior_prims: also recompute interior primitives (viscous runs), when the

@@ -60,6 +60,23 @@ __global__ void metrics_nodes(Dims d, const double* x, const double* y, const do
   M.m[8][o] = (-xe * yx + xx * ye) / J;
 }
 
+// O-grid: the stored copies of the points across the seam (i < wrap and
+// i >= IM - wrap) take the metrics of the points they copy, P = IM - 2*wrap
+// away, whose stencils all lie on the stored periodic line.
+__global__ void metrics_wrap(Dims d, Met M, int wrap) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= 2L * wrap * d.JM * d.KM) return;
+  const int t = (int)(e % (2 * wrap));
+  const long r = e / (2 * wrap);
+  const int j = (int)(r % d.JM), k = (int)(r / d.JM);
+  const int P = d.IM - 2 * wrap;
+  const int i = t < wrap ? t : d.IM - 2 * wrap + t;
+  const int src = t < wrap ? i + P : i - P;
+  const long o = node_off(d, i, j, k), c = node_off(d, src, j, k);
+#pragma unroll
+  for (int m = 0; m < 10; ++m) M.m[m][o] = M.m[m][c];
+}
+
 // Ghost faces, edges and corners take the value of the nearest boundary node
 // (the clamped index), which is what metrics_kernel.cu:72-560 writes.
 __global__ void metrics_ghosts(Dims d, Met M) {
@@ -307,7 +324,7 @@ inline unsigned nb(long n) { return (unsigned)((n + 255) / 256); }
 }  // namespace
 
 cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, const double* z, double* const met[10],
-                           double* const area[10], float* const area32[6], cudaStream_t s) {
+                           double* const area[10], float* const area32[6], int wrap, cudaStream_t s) {
   Met M, A;
   Area32 A32;
   for (int m = 0; m < 10; ++m) {
@@ -316,6 +333,7 @@ cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, cons
   }
   for (int m = 0; m < 6; ++m) A32.m[m] = area32 ? area32[m] : nullptr;
   metrics_nodes<<<nb((long)d.IM * d.JM * d.KM), 256, 0, s>>>(d, x, y, z, M);
+  if (wrap > 0) metrics_wrap<<<nb(2L * wrap * d.JM * d.KM), 256, 0, s>>>(d, M, wrap);
   metrics_ghosts<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M);
   area_kernel<<<nb((long)d.IG * d.JG * d.KG), 256, 0, s>>>(d, M, A, A32);
   return cudaGetLastError();

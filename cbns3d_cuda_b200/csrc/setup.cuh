@@ -7,9 +7,11 @@
 namespace cbns {
 
 // metrics, their ghost extension, and the node area vectors / 1/J (area32,
-// may be null: FP32 copies of the xi and eta area vectors)
+// may be null: FP32 copies of the xi and eta area vectors).  wrap > 0 (O-grid):
+// the nodes i < wrap and i >= IM - wrap take the metrics of the nodes
+// IM - 2*wrap away, before the ghost extension.
 cudaError_t launch_metrics(const Dims& d, const double* x, const double* y, const double* z, double* const met[10],
-                           double* const area[10], float* const area32[6], cudaStream_t s);
+                           double* const area[10], float* const area32[6], int wrap, cudaStream_t s);
 cudaError_t launch_ic(const Dims& d, double* const prim[6], double angle_deg, double p_inf, int viscous,
                       cudaStream_t s);
 // Case initial states on the ghosted box (kind CBNS_CASE_*, prm as in

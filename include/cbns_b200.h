@@ -87,6 +87,22 @@ extern "C" {
  * (all i, k interior), then k faces (all i, j), each node's two ghosts set to
  * its state; the state depends on the buffer's interior only. */
 #define CBNS_BC_CHARACTERISTIC 2
+/* OGRID (no counterpart in the reference; the NACA 0012 O-grid configuration):
+ * i wraps around, j = 0 is the wall (adiabatic no-slip in viscous runs, slip
+ * in inviscid ones, on every i: the reference's wall branch with i_begin = 1,
+ * i_end = IM whatever the parameters say), j = JM-1 the characteristic far
+ * field above, the k faces the reference's zero-gradient copy.  The block
+ * stores the periodic line of P = IM - 2*CBNS_OGRID_WRAP points at
+ * i = CBNS_OGRID_WRAP .. IM-CBNS_OGRID_WRAP-1, with CBNS_OGRID_WRAP copies of
+ * the points across the seam on either side (i < W holds point i + P,
+ * i >= IM - W point i - P; the grid passed to cbns_calc_metrics must hold
+ * them).  After every boundary pass those nodes and the i ghosts are copies of
+ * the nodes P away (Q and primitives), and their metrics are copies too, so
+ * every stencil of a stored point sees the periodic line.  Needs P >= 6.
+ * Inviscid runs sweep the spectral radius after the boundary pass instead of
+ * fusing it into stage 3; blocks in this mode cannot join a batch. */
+#define CBNS_BC_OGRID 3
+#define CBNS_OGRID_WRAP 4
 
 /* cbns_init_case kinds (no counterpart in the reference) and their parameters:
  *   VORTEX        Mach, strength beta, centre x, centre y, radius R, stream

@@ -305,6 +305,18 @@ struct Oracle {
           met[7][t] = (xe * zx - xx * ze) / J;
           met[8][t] = (-xe * yx + xx * ye) / J;
         }
+    // CBNS_BC_OGRID (no counterpart in the reference): the stored copies of
+    // the points across the seam take the metrics of the points they copy.
+    if (P.bc_mode == CBNS_BC_OGRID) {
+      const long W = CBNS_OGRID_WRAP, Pw = IM - 2 * W;
+      for (long k = 0; k < KM; ++k)
+        for (long j = 0; j < JM; ++j)
+          for (long i = 0; i < IM; ++i) {
+            if (i >= W && i < IM - W) continue;
+            const long src = i < W ? i + Pw : i - Pw;
+            for (auto& m : met) m[g(i, j, k)] = m[g(src, j, k)];
+          }
+    }
     // Ghost faces, edges and corners take the value of the nearest boundary
     // node (metrics_kernel.cu:72-560 writes exactly the clamped-index copy).
 #pragma omp parallel for schedule(static)
@@ -369,12 +381,12 @@ struct Oracle {
   // the free stream along the outward unit normal; its two ghosts copy it.
   // i faces over j, k interior, j faces over all i and k interior, k faces
   // over all (i, j), so each neighbour is interior or set earlier in the call.
-  void bc_characteristic(std::vector<double>& Q, int dir) {
+  void bc_characteristic(std::vector<double>& Q, int dir, int side0 = 0, int nsides = 2) {
     const double gamma = P.gamma, gam1 = D.gam1, p_inf = D.p_inf;
     const double AoA = P.angle_attack * PI / 180.0;
     const double u_inf = std::cos(AoA), v_inf = std::sin(AoA);
     const long n0 = dir == 0 ? JM - 2 : IM, n1 = dir == 2 ? JM : KM - 2, nf = dir == 0 ? IM : dir == 1 ? JM : KM;
-    for (int side = 0; side < 2; ++side)
+    for (int side = side0; side < side0 + nsides; ++side)
 #pragma omp parallel for schedule(static)
       for (long f1 = 0; f1 < n1; ++f1)
         for (long f0 = 0; f0 < n0; ++f0) {
@@ -455,9 +467,14 @@ struct Oracle {
           }
       return;
     }
+    // CBNS_BC_OGRID (no counterpart in the reference): no i-face pass, the
+    // wall on every i of j = 0, the characteristic far field on j = JM-1, and
+    // after phase 3 the copies across the periodic seam
+    const bool og = P.bc_mode == CBNS_BC_OGRID;
+    const long k1b = og ? 1 : KM - 1;
     // phase 1b: i faces (:84-186)
 #pragma omp parallel for schedule(static)
-    for (long k = 1; k < KM - 1; ++k)
+    for (long k = 1; k < k1b; ++k)
       for (long j = 1; j < JM - 1; ++j) {
         for (int side = 0; side < 2; ++side) {
           const long src = side == 0 ? 1 : IM - 2;
@@ -478,7 +495,8 @@ struct Oracle {
         }
       }
     // phase 2a: j = 0 face, Q part (:190-352)
-    const unsigned ib1 = P.i_begin - 1u;  // unsigned, as in the reference
+    const unsigned ib1 = og ? 0u : P.i_begin - 1u;  // unsigned, as in the reference
+    const unsigned iend = og ? (unsigned)IM : (unsigned)P.i_end;
 #pragma omp parallel for schedule(static)
     for (long k = 1; k < KM - 1; ++k)
       for (long i = 0; i < IM; ++i) {
@@ -497,7 +515,7 @@ struct Oracle {
             std::memcpy(&Q[5 * g(i, -l, k)], &Q[5 * g(m, l, k)], 5 * sizeof(double));
             std::memcpy(&Q[5 * g(m, -l, k)], &Q[5 * g(i, l, k)], 5 * sizeof(double));
           }
-        } else if ((unsigned)P.i_end > ui) {
+        } else if (iend > ui) {
           if (P.viscous) {  // adiabatic no-slip wall (:263-295)
             const double* q = &Q[5 * g(i, 1, k)];
             const double r = q[0], ru = q[1], rv = q[2], rw = q[3], rE = q[4];
@@ -535,6 +553,7 @@ struct Oracle {
           }
         }
       }
+    if (og) bc_characteristic(Q, 1, 1, 1);
     // phase 2b: primitives on the j faces (:354-413)
 #pragma omp parallel for schedule(static)
     for (long k = 1; k < KM - 1; ++k)
@@ -558,6 +577,19 @@ struct Oracle {
           for (long l = 0; l <= NG; ++l) put_prim(g(i, j, base + dir * l), s);
         }
       }
+    if (og) {  // i < W and i >= IM - W, ghosts included, over the ghosted (j, k) box
+      const long W = CBNS_OGRID_WRAP, Pw = IM - 2 * W;
+#pragma omp parallel for schedule(static)
+      for (long k = -NG; k < KM + NG; ++k)
+        for (long j = -NG; j < JM + NG; ++j)
+          for (long i = -NG; i < IM + NG; ++i) {
+            if (i >= W && i < IM - W) continue;
+            const long t = g(i, j, k), ts = g(i < W ? i + Pw : i - Pw, j, k);
+            std::memcpy(&Q[5 * t], &Q[5 * ts], 5 * sizeof(double));
+            rho[t] = rho[ts]; u[t] = u[ts]; v[t] = v[ts]; w[t] = w[ts]; p[t] = p[ts];
+            if (P.viscous) T[t] = T[ts];
+          }
+    }
   }
 
   // ---------------------------------------------------------------------------

@@ -278,6 +278,39 @@ def naca0012_ogrid(IM, JM, KM, first=1.0e-5, far=20.0, span=0.1):
     return x, y, z, r
 
 
+def naca0012_ogrid_blend(P, JM, KM, first=1.0e-5, far=20.0, span=0.1):
+    """Periodic O-grid around the closed-trailing-edge NACA 0012 for the
+    wrap-around boundary mode: P points around the profile at the parameter
+    angles of naca0012_ogrid, each j line running straight from the surface
+    point to the point at the same angle on the circle of radius `far` about
+    mid-chord, with the geometric spacing of naca0012_ogrid (first cell
+    `first` of the line length).  Unlike surface normals, which turn by almost
+    180 degrees between the last and the first point at the trailing edge,
+    these lines stay nearly parallel across the seam, so the cells there are as
+    regular as elsewhere."""
+    dth = 2.0 * np.pi / P
+    th = np.linspace(0.5 * dth, 2.0 * np.pi - 0.5 * dth, P)
+    xs = 0.5 * (1.0 + np.cos(th))
+    yt = 5 * 0.12 * (0.2969 * np.sqrt(xs) - 0.1260 * xs - 0.3516 * xs ** 2 + 0.2843 * xs ** 3 - 0.1036 * xs ** 4)
+    ys = np.where(th <= np.pi, -yt, yt)
+    xf, yf = 0.5 + far * np.cos(th), -far * np.sin(th)
+    lo, hi = 1.0 + 1e-9, 2.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if first * (r ** (JM - 1) - 1) / (r - 1) > far:
+            hi = r
+        else:
+            lo = r
+    f = (r ** np.arange(JM) - 1) / (r ** (JM - 1) - 1)
+    x2 = xs[None, :] + f[:, None] * (xf - xs)[None, :]
+    y2 = ys[None, :] + f[:, None] * (yf - ys)[None, :]
+    zk = np.linspace(0.0, span, KM)
+    x = np.broadcast_to(x2, (KM, JM, P)).copy()
+    y = np.broadcast_to(y2, (KM, JM, P)).copy()
+    z = np.broadcast_to(zk[:, None, None], (KM, JM, P)).copy()
+    return x, y, z
+
+
 def ogrid_wrap(a, wrap=4):
     """The block layout of the O-grid boundary mode (bc_mode = 3): the
     periodic line of P points along i (last axis) stored with `wrap` copies of
@@ -331,12 +364,11 @@ def case_naca(IM=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5):
 
 def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, viscous=True):
     """configs[1] with its own boundaries (bc_mode = 3, BC_OGRID): the NACA 0012
-    O-grid of P points around the profile, wrapped periodically in i (stored
+    O-grid of P points around the profile (naca0012_ogrid_blend), wrapped periodically in i (stored
     with 4 copied points either side, IM = P + 8), adiabatic no-slip wall on
     j = 0 (slip when inviscid), characteristic far field on j = JM-1; M 0.8,
     AoA 1.25 deg, Re 5e4, free-stream start."""
-    x, y, z, _ = naca0012_ogrid(P, JM, KM, first=first)
-    x, y, z = (ogrid_wrap(a) for a in (x, y, z))
+    x, y, z = (ogrid_wrap(a) for a in naca0012_ogrid_blend(P, JM, KM, first=first))
     params = dict(CFL=CFL, Mach=0.8, angle_attack=1.25, Re=5.0e4, Pr=0.72, Pr_t=0.9, T_inf=288.15, gamma=1.4,
                   i_begin=1, i_end=P + 8, viscous=viscous, bc_mode=3)
     return Case("naca_ogrid", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)

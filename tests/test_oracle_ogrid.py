@@ -6,6 +6,10 @@
   (the same grid, its periodic line rolled) gives, after some steps, the same
   state rolled by s, bit for bit, inviscid and viscous;
 * the wall holds: zero velocity on j = 0 in viscous runs.
+
+The grid is naca0012_ogrid_blend: on the surface-normal O-grid the single
+cell across a sharp trailing edge turns by almost 180 degrees, and a run
+wrapped across it loses positivity within ten steps.
 """
 import numpy as np
 import pytest
@@ -58,9 +62,10 @@ def test_seam_is_invisible(oracle_lib, viscous):
     a, b = _case(viscous), _case(viscous, seam_shift=s)
     oa, ob = _oracle(a), _oracle(b)
     for o in (oa, ob):
-        rc, _, n = o.solve(6, 1.0e30)
-        assert rc == 0 and n == 6
+        rc, _, n = o.solve(20, 1.0e30)
+        assert rc == 0 and n == 20
     qa, qb = _q(oa, a), _q(ob, b)
+    assert np.all(np.isfinite(qa)) and np.all(np.isfinite(qb))
     IM = a.shape[0]
     ca = qa[:, :, 2 + W:IM + 2 - W]
     cb = qb[:, :, 2 + W:IM + 2 - W]

@@ -8,7 +8,8 @@
 //                    trained weights shipped beside this executable,
 //                    ../data/sensor_weights.bin)
 //   --visdiv D       reference (default) | centered
-//   --bc B           reference (default) | farfield | characteristic
+//   --bc B           reference (default) | farfield | characteristic | ogrid
+//                    (ogrid: the grid file stores the wrap copies of CBNS_BC_OGRID)
 //   --inviscid / --viscous   override the build-time default
 //   --input FILE     parameter file (default input.txt)
 //   --vtk-binary     output.vtk in legacy VTK BINARY (same data set as the
@@ -50,6 +51,7 @@ int main(int argc, char** argv) {
       if (v == "reference") o.bc_mode = CBNS_BC_REFERENCE;
       else if (v == "farfield") o.bc_mode = CBNS_BC_FARFIELD;
       else if (v == "characteristic") o.bc_mode = CBNS_BC_CHARACTERISTIC;
+      else if (v == "ogrid") o.bc_mode = CBNS_BC_OGRID;
       else {
         std::cerr << "unknown boundary mode " << v << "\n";
         return 2;

@@ -2,7 +2,8 @@
 characteristic far field on j = JM-1) on a small NACA 0012 O-grid:
 
 * the CUDA path matches the oracle's O-grid mode to the plain path's 1e-10
-  after 20 steps, graph and per-call paths, inviscid and viscous;
+  after 20 steps, graph and per-call paths, inviscid and viscous (rho w,
+  zero up to rounding in the inviscid runs, against the state's scale);
 * the copied nodes either side of the seam equal the nodes they copy, bit for
   bit;
 * moving the seam around the profile gives the same state, rolled;
@@ -47,8 +48,14 @@ def test_ogrid_matches_oracle(viscous, graph):
     rc, _, no = o.solve(n, 1.0e30)
     assert rc == 0 and no == n
     q = g.get_conservative()
+    ref = o.get_conservative()
     assert np.all(np.isfinite(q))
-    assert max(per_var_rel_linf(q, o.get_conservative())) <= 1e-10
+    # rho w of the extruded 2-D flow is zero up to rounding in inviscid runs
+    # (~4e-17: the characteristic projection's round trip), so its difference is
+    # held to 1e-10 of the state's scale, the other variables to 1e-10 of their own
+    err = per_var_rel_linf(q, ref)
+    assert max(err[:3] + err[4:]) <= 1e-10
+    assert np.max(np.abs(q.reshape(-1, 5)[:, 3] - ref.reshape(-1, 5)[:, 3])) <= 1e-10 * np.max(np.abs(ref))
     IM, JM, KM = c.shape
     q = q.reshape(KM + 4, JM + 4, IM + 4, 5)
     P = IM - 2 * W

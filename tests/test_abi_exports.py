@@ -67,3 +67,28 @@ def test_bad_params_rejected_without_gpu(built):
     p = make_params(10, 10, 10, precision=7)
     assert lib.cbns_create(C.byref(p), C.byref(h)) == _abi.CBNS_ERR_ARG
     assert lib.cbns_create(None, C.byref(h)) == _abi.CBNS_ERR_ARG
+
+
+def test_bad_boundary_modes_rejected_without_gpu(built):
+    import ctypes as C
+    from cbns3d_cuda_b200 import _abi, make_params
+    lib = _abi.load()
+    h = C.c_void_p()
+    p = make_params(20, 10, 10, bc_mode=4)
+    assert lib.cbns_create(C.byref(p), C.byref(h)) == _abi.CBNS_ERR_ARG
+    p = make_params(2 * _abi.OGRID_WRAP + 5, 10, 10, bc_mode=_abi.BC_OGRID)  # periodic line of 5 < 6 points
+    assert lib.cbns_create(C.byref(p), C.byref(h)) == _abi.CBNS_ERR_ARG
+
+
+def test_header_constants_match_the_binding():
+    import re
+    from pathlib import Path
+    from cbns3d_cuda_b200 import _abi
+    hdr = (Path(__file__).resolve().parents[1] / "include" / "cbns_b200.h").read_text()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+CBNS_(\w+)\s+(-?\d+)\b", hdr)}
+    for name in ("BC_REFERENCE", "BC_FARFIELD", "BC_CHARACTERISTIC", "BC_OGRID", "OGRID_WRAP", "PREC_FP64",
+                 "PREC_SPLIT", "PREC_HYBRID", "VISDIV_REFERENCE", "VISDIV_CENTERED", "ERR_ARG", "ERR_NAN_DT"):
+        py = getattr(_abi, name, None)
+        if py is None:
+            py = getattr(_abi, "CBNS_" + name)
+        assert defs[name] == py, name

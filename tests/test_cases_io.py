@@ -76,6 +76,28 @@ def test_naca_grid_spacing():
     assert 1.0 < r < 2.0
 
 
+def test_naca_blend_grid_and_wrap(oracle_lib):
+    """The O-grid of the wrap-around mode: right-handed with its wrap copies
+    (metrics of the O-grid mode), wall spacing `first` of each line's length,
+    outer points on the 20-chord circle, and the seam cells no larger than
+    their neighbours around the profile."""
+    P, JM, KM = 64, 32, 4
+    x, y, z = cases.naca0012_ogrid_blend(P, JM, KM, first=1e-5)
+    L = np.hypot(x[0, -1] - x[0, 0], y[0, -1] - y[0, 0])
+    d1 = np.hypot(x[0, 1] - x[0, 0], y[0, 1] - y[0, 0])
+    assert np.allclose(d1, 1e-5 * L / 20.0, rtol=1e-6)  # first / far of the line's length L
+    assert np.allclose(np.hypot(x[0, -1] - 0.5, y[0, -1]), 20.0)
+    ds = np.hypot(np.diff(x[0, 8], append=x[0, 8, :1]), np.diff(y[0, 8], append=y[0, 8, :1]))
+    assert ds[-1] <= 1.5 * max(ds[-2], ds[0])  # the cell across the trailing edge
+    c = cases.case_naca_ogrid(P, JM, KM)
+    assert c.shape == (P + 8, JM, KM)
+    assert np.array_equal(c.x[..., :4], x[..., -4:]) and np.array_equal(c.x[..., -4:], x[..., :4])
+    o = orc.OracleBlock(make_params(*c.shape, **c.params))
+    o.calc_metrics(c.x, c.y, c.z)
+    J = o.get_metrics()[9]
+    assert (J > 0).all()
+
+
 def _write_vtk(path, dims, pts, fields, binary):
     """The driver's legacy VTK layout (Block3d::output_vtk / output_vtk_binary)."""
     n = pts.shape[0]

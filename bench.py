@@ -65,7 +65,7 @@ def args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--case", default="shock_vortex", choices=["shock_vortex", "blast", "vortex", "batch"])
-    ap.add_argument("--blocks", type=int, default=64, help="--case batch: number of blocks (configs[4]: 64)")
+    ap.add_argument("--blocks", type=int, default=64, help="--case batch: number of blocks (64 in the batched-blocks workload)")
     ap.add_argument("--size", default=None, help="IMxJMxKM (default: the case's config size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -77,12 +77,12 @@ def make_case(name, size):
     from cbns3d_cuda_b200 import cases
     if name == "shock_vortex":
         IM, JM, KM = size or (256, 256, 128)
-        return cases.case_shock_vortex(IM, JM, KM), f"shock-vortex {IM}x{JM}x{KM} (configs[3] grid), inviscid"
+        return cases.case_shock_vortex(IM, JM, KM), f"shock-vortex {IM}x{JM}x{KM}, inviscid"
     if name == "blast":
         IM, JM, KM = size or (384, 384, 384)
-        return cases.case_blast(IM, JM, KM), f"spherical blast {IM}x{JM}x{KM} (configs[2]), inviscid"
+        return cases.case_blast(IM, JM, KM), f"spherical blast {IM}x{JM}x{KM}, inviscid"
     IM, JM, KM = size or (64, 32, 16)
-    return cases.case_vortex(IM, JM, KM), f"isentropic vortex {IM}x{JM}x{KM} (configs[0]), inviscid"
+    return cases.case_vortex(IM, JM, KM), f"isentropic vortex {IM}x{JM}x{KM}, inviscid"
 
 
 class Clocks:
@@ -435,7 +435,7 @@ def run_reference(a):
 
 
 def run_batch(a):
-    """independent viscous blocks of uneven size (seeded draw),
+    """Batched-blocks workload: independent viscous blocks of uneven size (seeded draw),
     learned-sensor hybrid, advanced by one persistent work-queue launch of the
     stage kernel per RK stage (cbns_batch_run) with per-block dt; beside it the
     same blocks stepped one after the other on the same stream (one CUDA graph
@@ -502,7 +502,7 @@ def run_batch(a):
         "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": K, "warmup": W,
         "ms_per_step": ms_batch / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 flux / f64 state", "data": "synthetic",
-        "config": {"workload": f"configs[4]: {len(cs)} viscous blocks, sizes 32^3..128x64x64 (seed 0), "
+        "config": {"workload": f"batched blocks: {len(cs)} viscous blocks, sizes 32^3..128x64x64 (seed 0), "
                                "Mach U[0.3,2], Re U[1e3,1e5], far-field boundaries, learned-sensor hybrid, per-block dt",
                    "cell_updates_per_step": N, "blocks": len(cs),
                    "shapes": [d["shape"] for d in draw]},

@@ -336,7 +336,7 @@ def isentropic_vortex(xg, yg, Mach, beta, xc, yc, R, gamma=1.4, u_dir=(1.0, 0.0)
 
 
 def case_vortex(IM=64, JM=32, KM=16, nsteps=100, CFL=0.5, Mach=0.5):
-    """isentropic vortex (strength 5, centre (3, 2.5), radius 1) at
+    """Isentropic vortex case: isentropic vortex (strength 5, centre (3, 2.5), radius 1) at
     Mach 0.5 on the perturbed 10 x 5 x 2.5 box; 100 steps at CFL 0.5.  Reference
     boundary mode: i faces pressure-reset extrapolation, j faces held at the
     initial state (i_begin = 1, i_end = 0), k faces zero-gradient."""
@@ -350,7 +350,7 @@ def case_vortex(IM=64, JM=32, KM=16, nsteps=100, CFL=0.5, Mach=0.5):
 
 
 def case_naca(IM=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5):
-    """viscous NACA 0012 O-grid, M 0.8, AoA 1.25 deg, Re 5e4, Pr 0.72,
+    """NACA 0012 case: viscous NACA 0012 O-grid, M 0.8, AoA 1.25 deg, Re 5e4, Pr 0.72,
     Sutherland with T_inf = 288.15 K, free-stream start.  Reference boundary
     mode: wall on the whole j = 0 face (i_begin = 1, i_end = IM).  Small test
     grids use a larger first cell: with 1e-5 chords and few points around the
@@ -363,7 +363,7 @@ def case_naca(IM=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5):
 
 
 def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, viscous=True):
-    """configs[1] with its own boundaries (bc_mode = 3, BC_OGRID): the NACA 0012
+    """NACA 0012 case with its own boundaries (bc_mode = 3, BC_OGRID): the NACA 0012
     O-grid of P points around the profile (naca0012_ogrid_blend), wrapped periodically in i (stored
     with 4 copied points either side, IM = P + 8), adiabatic no-slip wall on
     j = 0 (slip when inviscid), characteristic far field on j = JM-1; M 0.8,
@@ -375,7 +375,7 @@ def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, vis
 
 
 def case_blast(IM=384, JM=384, KM=384, t_end=0.05, CFL=0.5):
-    """spherical blast (p = 10 inside r < 0.1, 0.1 outside, rho = 1,
+    """Blast case: spherical blast (p = 10 inside r < 0.1, 0.1 outside, rho = 1,
     at rest) on the centre-clustered (stretch 1.5), 5%-skewed [-1,1]^3 box.
     Mach is chosen so that p_inf = 1/(gamma M^2) = 0.1, the ambient pressure
     the i-face boundary resets to."""
@@ -393,7 +393,7 @@ def case_blast(IM=384, JM=384, KM=384, t_end=0.05, CFL=0.5):
 
 
 def case_batch(nblocks=64, seed=0, size_lo=(32, 32, 32), size_hi=(128, 64, 64), viscous=True, CFL=0.5):
-    """independent blocks for the batched form.  Per block (seeded
+    """Batched-blocks case: independent blocks for the batched form.  Per block (seeded
     draw): grid points uniform in size_lo..size_hi per dimension, free-stream
     Mach uniform in [0.3, 2.0], Reynolds number uniform in [1e3, 1e5], an
     isentropic vortex of strength uniform in [1, 5] at a random position of
@@ -421,7 +421,7 @@ def case_batch(nblocks=64, seed=0, size_lo=(32, 32, 32), size_hi=(128, 64, 64), 
 
 
 def case_shock_vortex(IM=256, JM=256, KM=128, nsteps=100, CFL=0.5, Ms=1.2, eps=0.3, rc=0.075):
-    """a stationary Mach 1.2 normal shock at x = 0.5 of the 5%-skewed
+    """Shock/vortex case: a stationary Mach 1.2 normal shock at x = 0.5 of the 5%-skewed
     [0,1]x[0,1]x[0,0.5] box, with an isentropic vortex (strength 0.3, radius
     0.075, centre (0.25, 0.5)) in the upstream flow moving into it."""
     x, y, z = skewed_channel(IM, JM, KM)

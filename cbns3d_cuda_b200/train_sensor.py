@@ -17,7 +17,7 @@ cross-entropy (cbns_mlp_grad and cbns_mlp_adam) over 90 % of the faces; the
 held-out 10 % give recall and WENO5 fraction.
 
 Threshold: the decision threshold tau is calibrated in closed loop, with
-WENO5 as the judge: on a shock / vortex grid not used for training (192 x 192
+WENO5 as the arbiter: on a shock / vortex grid not used for training (192 x 192
 x 96), 100 steps of the hybrid flux (tcgen05 inference, as deployed) are
 compared with 100 steps of the FP64 WENO5 path for each candidate tau, and the
 largest tau whose density L2 error stays at or below --l2-bound is kept.  Everything runs on the GPU; the script prints one line per stage and a

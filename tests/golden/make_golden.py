@@ -7,7 +7,9 @@ initial checkpoint or the free-stream flag, parameters), the per-step dt the
 reference printed, and the checkpoint it wrote after the last step.
 
 Cases avoid the reference's racy boundary branches: no wake cut
-(i_begin = 1) and KM % 4 != 1 ("Reference races").
+(i_begin = 1), whose mirror reads cross thread blocks, and KM % 4 != 1, so
+that the k = KM-1 copy and its source k = KM-2 fall in the same 4-deep block
+of the reference's boundary kernel.
 
 Usage:  python tests/golden/make_golden.py [OUTDIR]   (default: tests/golden)
 """

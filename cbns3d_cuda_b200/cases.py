@@ -311,6 +311,89 @@ def naca0012_ogrid_blend(P, JM, KM, first=1.0e-5, far=20.0, span=0.1):
     return x, y, z
 
 
+def _naca_half_thickness(x):
+    return 5 * 0.12 * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x ** 2 + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+
+
+def _naca_half_thickness_dx(x):
+    return 5 * 0.12 * (0.14845 / np.sqrt(x) - 0.1260 - 0.7032 * x + 0.8529 * x ** 2 - 0.4144 * x ** 3)
+
+
+def naca0012_rounded_surface(P, te_radius=2.0e-3, cluster=0.9):
+    """P points around the NACA 0012 whose sharp trailing edge is replaced by
+    the circular arc of radius te_radius tangent to both surfaces (centre on
+    the chord line, tangent where yt * sqrt(1 + yt'^2) = te_radius).  Point 0
+    sits on the rounded edge; the points run along the lower surface to the
+    leading edge and back along the upper one, spaced in arc length s(u) =
+    S (u - cluster sin(4 pi u) / (4 pi)), u = i/P, so the spacing at both
+    edges is 1 - cluster of the mean."""
+    lo, hi = 0.9, 1.0 - 1e-12
+    for _ in range(200):  # tangency abscissa
+        m = 0.5 * (lo + hi)
+        if _naca_half_thickness(m) * np.sqrt(1 + _naca_half_thickness_dx(m) ** 2) > te_radius:
+            lo = m
+        else:
+            hi = m
+    xt = lo
+    xc = xt + _naca_half_thickness(xt) * _naca_half_thickness_dx(xt)
+    phi = np.arctan2(_naca_half_thickness(xt), xt - xc)
+    beta = np.linspace(0.0, np.pi, 20001)
+    xs = 0.5 * (1.0 - np.cos(beta)) * xt
+    arc = np.linspace(0.0, phi, 400)
+    lower_arc = np.stack([xc + te_radius * np.cos(arc), -te_radius * np.sin(arc)], 1)
+    lower = np.stack([xs[::-1][1:], -_naca_half_thickness(xs[::-1][1:])], 1)
+    upper = np.stack([xs[1:], _naca_half_thickness(xs[1:])], 1)
+    upper_arc = np.stack([xc + te_radius * np.cos(arc[::-1][1:]), te_radius * np.sin(arc[::-1][1:])], 1)
+    closed = np.vstack([lower_arc, lower, upper, upper_arc])  # ends back on the edge point
+    s = np.concatenate([[0.0], np.cumsum(np.hypot(*np.diff(closed, axis=0).T))])
+    u = np.arange(P) / P
+    st = s[-1] * (u - cluster * np.sin(4 * np.pi * u) / (4 * np.pi))
+    return np.interp(st, s, closed[:, 0]), np.interp(st, s, closed[:, 1])
+
+
+def naca0012_ogrid_marched(P, JM, KM, first=1.0e-5, far=20.0, span=0.1, te_radius=2.0e-3, smooth=0.3):
+    """Periodic O-grid around the NACA 0012 with a rounded trailing edge
+    (naca0012_rounded_surface), marched outward layer by layer: each layer
+    steps along its own unit normals (central differences around the closed
+    line), smoothed along the layer by 2 + 2j Jacobi sweeps of weight
+    `smooth`, with the geometric spacing of naca0012_ogrid (first cell
+    `first`, `far` chords in all).  The lines leave the wall within a few
+    degrees of its normal; outward the smoothing fans them out evenly around
+    the trailing edge, so
+    the Jacobian stays positive at the full 384 x 128 size, where straight
+    normal lines from the rounded edge give negative Jacobians in the wake
+    fan."""
+    x0, y0 = naca0012_rounded_surface(P, te_radius)
+    lo, hi = 1.0 + 1e-9, 2.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if first * (r ** (JM - 1) - 1) / (r - 1) > far:
+            hi = r
+        else:
+            lo = r
+    d = first * (r ** np.arange(JM) - 1) / (r - 1)
+    X = np.zeros((JM, P))
+    Y = np.zeros((JM, P))
+    X[0], Y[0] = x0, y0
+    for j in range(JM - 1):
+        tx = np.roll(X[j], -1) - np.roll(X[j], 1)
+        ty = np.roll(Y[j], -1) - np.roll(Y[j], 1)
+        n = np.hypot(tx, ty)
+        nx, ny = -ty / n, tx / n
+        for _ in range(2 + 2 * j):
+            nx = nx + smooth * (np.roll(nx, 1) + np.roll(nx, -1) - 2 * nx)
+            ny = ny + smooth * (np.roll(ny, 1) + np.roll(ny, -1) - 2 * ny)
+            n = np.hypot(nx, ny)
+            nx, ny = nx / n, ny / n
+        X[j + 1] = X[j] + (d[j + 1] - d[j]) * nx
+        Y[j + 1] = Y[j] + (d[j + 1] - d[j]) * ny
+    zk = np.linspace(0.0, span, KM)
+    x = np.broadcast_to(X, (KM, JM, P)).copy()
+    y = np.broadcast_to(Y, (KM, JM, P)).copy()
+    z = np.broadcast_to(zk[:, None, None], (KM, JM, P)).copy()
+    return x, y, z
+
+
 def ogrid_wrap(a, wrap=4):
     """The block layout of the O-grid boundary mode (bc_mode = 3): the
     periodic line of P points along i (last axis) stored with `wrap` copies of
@@ -362,13 +445,18 @@ def case_naca(IM=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5):
     return Case("naca", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)
 
 
-def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, viscous=True):
-    """NACA 0012 case with its own boundaries (bc_mode = 3, BC_OGRID): the NACA 0012
-    O-grid of P points around the profile (naca0012_ogrid_blend), wrapped periodically in i (stored
+def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, viscous=True, grid="blend"):
+    """NACA 0012 case with its own boundaries (bc_mode = 3, BC_OGRID): an
+    O-grid of P points around the profile, wrapped periodically in i (stored
     with 4 copied points either side, IM = P + 8), adiabatic no-slip wall on
     j = 0 (slip when inviscid), characteristic far field on j = JM-1; M 0.8,
-    AoA 1.25 deg, Re 5e4, free-stream start."""
-    x, y, z = (ogrid_wrap(a) for a in naca0012_ogrid_blend(P, JM, KM, first=first))
+    AoA 1.25 deg, Re 5e4, free-stream start.  grid "blend":
+    naca0012_ogrid_blend (sharp edge, straight lines to a far circle; regular
+    on small grids with a coarse first cell), "marched":
+    naca0012_ogrid_marched (rounded edge, wall-normal marched lines; valid at
+    the full 384 x 128 size with a 1e-5 first cell)."""
+    gen = {"blend": naca0012_ogrid_blend, "marched": naca0012_ogrid_marched}[grid]
+    x, y, z = (ogrid_wrap(a) for a in gen(P, JM, KM, first=first))
     params = dict(CFL=CFL, Mach=0.8, angle_attack=1.25, Re=5.0e4, Pr=0.72, Pr_t=0.9, T_inf=288.15, gamma=1.4,
                   i_begin=1, i_end=P + 8, viscous=viscous, bc_mode=3)
     return Case("naca_ogrid", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)

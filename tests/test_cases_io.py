@@ -134,3 +134,21 @@ def test_read_vtk_ascii_and_binary(tmp_path):
         assert np.max(np.abs(p - pts)) <= tol * np.max(np.abs(pts))
         for k in fields:
             assert np.max(np.abs(f[k] - fields[k])) <= tol * np.max(np.abs(fields[k]))
+
+
+def test_naca_marched_grid_full_size(oracle_lib):
+    """The marched O-grid at the NACA configuration's size: positive Jacobian
+    everywhere (O-grid metrics), first cell 1e-5, lines leaving the wall within
+    a few degrees of its normal, outer boundary about 20 chords out."""
+    c = cases.case_naca_ogrid(384, 128, 4, grid="marched")
+    x, y = c.x[0, :, 4:-4], c.y[0, :, 4:-4]
+    d1 = np.hypot(x[1] - x[0], y[1] - y[0])
+    assert np.allclose(d1, 1e-5, rtol=1e-9)
+    tx, ty = np.roll(x[0], -1) - np.roll(x[0], 1), np.roll(y[0], -1) - np.roll(y[0], 1)
+    cosang = ((x[1] - x[0]) * tx + (y[1] - y[0]) * ty) / (d1 * np.hypot(tx, ty))
+    assert np.max(np.abs(cosang)) < 0.1  # within ~6 degrees of the wall normal
+    r = np.hypot(x[-1] - 0.5, y[-1])
+    assert 19.0 < r.min() and r.max() < 21.0
+    o = orc.OracleBlock(make_params(*c.shape, **c.params))
+    o.calc_metrics(c.x, c.y, c.z)
+    assert (np.asarray(o.get_metrics()[9]) > 0).all()

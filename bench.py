@@ -18,9 +18,17 @@ step; N_upd = (IM-2)(JM-2)(KM-2).
   e2e     the reference-style host-driven solve of the hybrid through the C
           ABI (block3d_cuda call sequence: dt read back every step, dt passed
           per stage), with the state uploaded from pinned host memory before
-          and downloaded after the K steps inside the timed region.
-  roofline  HBM roofline of the dominant kernel (the fused stage kernel).
-  cpu_baseline  the FP64 CPU oracle (OpenMP, all host cores) on a bounded sample.
+          and downloaded after the K steps inside the timed region; the same
+          for the plain FP64 path under paths.fp64.e2e (the precision-matched
+          end-to-end figure).
+  plain_vs_reference_linf  the plain FP64 path's state after the W + K steps
+          against the reference's own CUDA build run on the same files for the
+          same steps (largest relative L-inf over the five variables).
+  roofline  HBM roofline of the dominant kernel (the fused stage kernel); the
+          plain path's stage kernel also against the FP64 rate of a cuBLAS
+          DGEMM measured in the same run.
+  cpu_baseline  the FP64 CPU oracle (OpenMP, all host cores) on a bounded
+          sample, with the host's CPU model.
 
 --impl reference runs the reference's own build (oracle/_ref, compiled from its
 sources) on the same case through its own executable and times it from its
@@ -49,13 +57,20 @@ sys.path.insert(0, str(ROOT))
 # bytes per cell-update the kernel must move: per stage the stage input (40 B),
 # the metrics (80 B) and the output (40 B), plus the RK base in stages 2 and 3
 ALG_BYTES_PER_UPDATE = 560.0
-# FP64 FLOP the plain path executes per cell-update (dadd + dmul + 2 dfma, ncu
-# counters of a stage-2 launch: 4,660 per node, times three stages;
-# profiles/stage_kernel_128x128x64.md), and the B200's FP64 peak: 64 DFMA lanes
-# per SM x 148 SMs x 2 FLOP x 1.965 GHz (ncu's peak_sustained of
-# sm__sass_thread_inst_executed_op_dfma_pred_on, at the maximum SM clock)
+# FP64 FLOP the plain path executes per cell-update: dadd + dmul + 2 dfma
+# counted by ncu over a stage-2 launch of the plain stage kernel (4,660 per
+# node), times three stages
 FP64_FLOP_PER_UPDATE = 13980.0
-FP64_PEAK_TFLOPS = 64 * 148 * 2 * 1.965e9 / 1e12
+# nominal FP64 peak for context: 64 DFMA lanes per SM x 148 SMs x 2 FLOP x
+# 1.965 GHz; the fraction is taken against the DGEMM rate measured in the run
+FP64_NOMINAL_TFLOPS = 64 * 148 * 2 * 1.965e9 / 1e12
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per interior node
+# of one stage-2 launch of the stage kernel, from single ncu captures on the
+# shock-vortex case: plain FP64 kernel at 128x128x64, hybrid kernel at
+# 192x192x96 (inputs larger than L2 in both); traffic grows with the nodes of
+# a launch, so the figures scale to the bench grid
+FP64_STAGE_DRAM_BYTES_PER_NODE = 240.0
+HYBRID_STAGE_DRAM_BYTES_PER_NODE = 237.8
 
 
 def args():
@@ -69,6 +84,8 @@ def args():
     ap.add_argument("--size", default=None, help="IMxJMxKM (default: the case's config size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-reference-check", action="store_true",
+                    help="skip the plain path's comparison with the reference build")
     ap.add_argument("--sensor", default=str(ROOT / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz"))
     return ap.parse_args()
 
@@ -167,7 +184,7 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def device_pass(case, precision, K, W, torch, dist, clocks=None):
+def device_pass(case, precision, K, W, torch, dist, clocks=None, keep_state=False):
     """W untimed steps, K steps replayed from the CUDA graph and timed with
     events on the launch stream (optionally with clock sampling), the state
     read back, then K more steps with events around every kernel for the
@@ -199,7 +216,10 @@ def device_pass(case, precision, K, W, torch, dist, clocks=None):
     out["ms"] = e0.elapsed_time(e1)
     out["launches"] = b.launch_count() - l0
     IM, JM, KM = case.shape
-    out["rho"] = b.get_conservative().reshape(KM + 4, JM + 4, IM + 4, 5)[2:-2, 2:-2, 2:-2, 0].copy()
+    q = b.get_conservative().reshape(KM + 4, JM + 4, IM + 4, 5)
+    out["rho"] = q[2:-2, 2:-2, 2:-2, 0].copy()
+    if keep_state:
+        out["q"] = q
     out["stats"] = b.sensor_stats() if precision == PREC_HYBRID else None
     b.prof_enable(True)
     b.prof_reset()
@@ -210,10 +230,12 @@ def device_pass(case, precision, K, W, torch, dist, clocks=None):
     return out
 
 
-def e2e_pass(case, K, torch):
-    """Host-driven solve of the hybrid through the C ABI with host buffers (pinned)."""
-    from cbns3d_cuda_b200 import CBNS_Q, PREC_HYBRID, _abi
-    b = init_block(case, PREC_HYBRID)
+def e2e_pass(case, K, torch, precision):
+    """Host-driven solve through the C ABI with host buffers (pinned): the
+    state uploaded, K steps of the reference's time loop (dt read back every
+    step), the state downloaded, all inside the timed region."""
+    from cbns3d_cuda_b200 import CBNS_Q, _abi
+    b = init_block(case, precision)
     stream = torch.cuda.Stream()
     b.set_stream(stream.cuda_stream)
     n = case.Q0.size
@@ -240,6 +262,51 @@ def e2e_pass(case, K, torch):
     return ms, {"h2d_bytes_per_step": state_bytes / K + 3 * 8, "d2h_bytes_per_step": state_bytes / K + 8}
 
 
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def fp64_peak_tflops(torch):
+    """FP64 rate of a cuBLAS DGEMM (torch.matmul, 8192^3, best of 5, CUDA events)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = None
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = ms if best is None else min(best, ms)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best / 1e3) / 1e12
+
+
+def reference_state(case, nsteps, timeout=1800):
+    """The reference build's conservative state (ghosted AoS, as its checkpoint
+    stores it) after nsteps steps of the case, or None when it was not built."""
+    exe = ROOT / "oracle" / "_ref" / "cbns3d_ref_inv"
+    if not exe.exists():
+        return None
+    from cbns3d_cuda_b200 import cases
+    with tempfile.TemporaryDirectory() as td:
+        d = case.write(Path(td) / "run", nsteps=nsteps, checkpoint_freq=nsteps)
+        r = subprocess.run([str(exe)], cwd=d, capture_output=True, text=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference run failed: {r.stdout[-300:]}")
+        return cases.read_checkpoint(d / "checkpoint.dat")[1]
+
+
 def cpu_baseline(case, budget_s=15.0):
     from cbns3d_cuda_b200 import make_params
     from oracle import oracle as orc
@@ -257,6 +324,7 @@ def cpu_baseline(case, budget_s=15.0):
             break
     o.close()
     return {"value": n_updates(case) * steps / el, "unit": "cell-updates/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
+            "nproc": cores, "cpu_model": cpu_model(),
             "kind": "port", "sample": f"{steps} RK3 step(s) of the same {case.shape} case, FP64 oracle "
                                       f"(C++/OpenMP restatement of the reference kernels), {el:.1f} s"}
 
@@ -286,7 +354,7 @@ def run_ours(a):
 
     # plain FP64 path, the split path without the sensor, then the
     # learned-sensor hybrid (headline) with clocks sampled during its timed region
-    p64 = device_pass(case, PREC_FP64, K, W, torch, dist)
+    p64 = device_pass(case, PREC_FP64, K, W, torch, dist, keep_state=not a.no_reference_check)
     p32 = device_pass(case, PREC_SPLIT, K, W, torch, dist)
     clk = Clocks(local)
     ph = device_pass(case, PREC_HYBRID, K, W, torch, dist, clocks=clk)
@@ -316,30 +384,40 @@ def run_ours(a):
     value32 = world * N * K / (ms32 / 1e3)
     value64 = world * N * K / (ms64 / 1e3)
 
-    e2e = None
+    e2e = e2e64 = None
     if not a.no_e2e:
-        ems, eb = e2e_pass(case, K, torch)
+        ems, eb = e2e_pass(case, K, torch, PREC_HYBRID)
         ems = reduce_max(ems)
         e2e = {"value": world * N * K / (ems / 1e3), "unit": "cell-updates/s", **eb}
+        ems, eb = e2e_pass(case, K, torch, PREC_FP64)
+        ems = reduce_max(ems)
+        e2e64 = {"value": world * N * K / (ems / 1e3), "unit": "cell-updates/s", **eb}
 
     peak, peak_kind = measured_peaks()
+    fp64_peak = fp64_peak_tflops(torch)
     # the per-kernel events come from a second run of K steps (same work per step)
     st_ms, st_n = kernh[0]
     alg_per_launch = ALG_BYTES_PER_UPDATE / 3.0 * N
     achieved = alg_per_launch / (st_ms / st_n / 1e3) / 1e9 if st_n else None
-    traffic = traffic64 = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        t = json.loads(tf.read_text())
-        if "hybrid_stage_bytes_per_update" in t:
-            traffic = t["hybrid_stage_bytes_per_update"] / 3.0 * N
-        if "fp64_stage_bytes_per_update" in t:
-            traffic64 = t["fp64_stage_bytes_per_update"] / 3.0 * N
+    traffic = HYBRID_STAGE_DRAM_BYTES_PER_NODE * N
+    traffic64 = FP64_STAGE_DRAM_BYTES_PER_NODE * N
     # the plain path's stage kernel: HBM and FP64-pipe fractions
     st64_ms, st64_n = kern64[0]
     st64_launch_s = st64_ms / max(st64_n, 1) / 1e3
     ach64 = alg_per_launch / st64_launch_s / 1e9 if st64_n else None
     tfl64 = FP64_FLOP_PER_UPDATE / 3.0 * N / st64_launch_s / 1e12 if st64_n else None
+
+    # the plain path against the reference's own build after the same W + K
+    # steps of the same case: relative L-inf per conservative variable
+    ref_cmp = None
+    if not a.no_reference_check and rank == 0:
+        qr = reference_state(case, W + K)
+        if qr is not None:
+            q64 = p64["q"]
+            per = [float(np.max(np.abs(q64[..., n] - qr[..., n])) / np.max(np.abs(qr[..., n]))) for n in range(5)]
+            ref_cmp = {"linf_per_variable": per, "max": max(per), "steps": W + K,
+                       "what": "plain FP64 path vs the reference CUDA build (oracle/_ref/cbns3d_ref_inv), same "
+                               "grid file, initial checkpoint and input.txt; relative L-inf over the ghosted box"}
 
     def kern_ms(k):
         return {name: {"ms_per_step": k[i][0] / K, "launches_per_step": k[i][1] / K}
@@ -355,19 +433,23 @@ def run_ours(a):
             "dtype": "f32 flux / f64 state", "data": "synthetic",
             "config": {"workload": wl,
                        "path": "learned-sensor hybrid: per face WENO5-char or linear upwind-5 flux (FP32), "
-                               "FP64 state, metrics, dt; sensor MLP on tcgen05 (BF16) every step, audit on a "
-                               "rotating 1/97 sample of the linear faces",
+                               "FP64 state, metrics, dt; sensor MLP on tcgen05 (BF16) every 3rd step, decisions "
+                               "held and widened in between; audit every step on a rotating 1/97 sample of the "
+                               "linear faces",
                        "grid": list(case.shape), "cell_updates_per_step": N, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (3 state buffers + 10 metric arrays)",
                        "sensor": {"weights": os.path.relpath(a.sensor, ROOT), "tau": SENSOR[1]}},
             "rho_l2_vs_fp64": l2_h, "rho_linf_vs_fp64": linf_h,
+            "plain_vs_reference_linf": ref_cmp["max"] if ref_cmp else None,
             "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "kernels": kern_ms(kern64),
                                "roofline_hbm": {"achieved": ach64, "peak": peak, "unit": "GB/s",
                                                 "frac": (ach64 / peak) if ach64 else None, "traffic": traffic64},
-                               "roofline_fp64": {"achieved": tfl64, "peak": FP64_PEAK_TFLOPS, "unit": "TFLOP/s",
-                                                 "frac": (tfl64 / FP64_PEAK_TFLOPS) if tfl64 else None,
+                               "roofline_fp64": {"achieved": tfl64, "peak": fp64_peak, "unit": "TFLOP/s",
+                                                 "frac": (tfl64 / fp64_peak) if tfl64 else None,
                                                  "flop_per_update": FP64_FLOP_PER_UPDATE,
-                                                 "peak_kind": "nominal (ncu DFMA peak x max SM clock)"}},
+                                                 "peak_kind": "measured in this run: cuBLAS DGEMM 8192^3",
+                                                 "nominal": FP64_NOMINAL_TFLOPS},
+                               "e2e": e2e64, "plain_vs_reference": ref_cmp},
                       "split": {"value": value32, "ms_per_step": ms32 / K, "rho_l2_vs_fp64": l2_32,
                                 "rho_linf_vs_fp64": linf_32, "stage_variant": variant32,
                                 "kernels": kern_ms(kern32)},

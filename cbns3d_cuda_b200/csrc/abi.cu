@@ -96,6 +96,15 @@ thread_local std::string g_last;
     }                                                                               \
   } while (0)
 
+}  // namespace
+
+namespace cbns {
+// The last error text of this thread, for entry points in other files.
+void set_last_error(const char* what, cudaError_t e) { g_last = std::string(what) + ": " + cudaGetErrorString(e); }
+}  // namespace cbns
+
+namespace {
+
 int dalloc(cbns_ctx* c, double** p, size_t elems) {
   void* q = nullptr;
   if (cudaMalloc(&q, elems * sizeof(double)) != cudaSuccess) {

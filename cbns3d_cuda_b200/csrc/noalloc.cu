@@ -1,13 +1,14 @@
 // noalloc.cu - cbns_calc_gradient_noalloc: the 4th-order gradient of a host
 // field without any device allocation.
 //
-// Who needs it: callers that cannot call cudaMalloc -- code running while a
-// stream is being captured into a CUDA graph (allocation is not allowed there),
-// hosts whose device memory is fully owned by their own pool allocator or held
-// to a fixed budget, and latency-sensitive paths that cannot afford the
-// device-wide synchronisation cudaMalloc/cudaFree imply.  cbns_calc_gradient
-// allocates its device copies per call; this variant keeps them in a
-// file-scope __device__ array instead.
+// Who needs it: callers that cannot call cudaMalloc -- hosts whose device
+// memory is fully owned by their own pool allocator or held to a fixed budget
+// (a cudaMalloc outside the pool can fail or push the process over its
+// budget), and latency-sensitive paths that cannot afford the device-wide
+// synchronisation cudaMalloc/cudaFree imply.  cbns_calc_gradient allocates its
+// device copies per call; this variant keeps them in a file-scope __device__
+// array instead.  Like cbns_calc_gradient it is synchronous: blocking copies
+// on the legacy default stream.
 //
 // Limits and sharing:
 //   * at most CBNS_NOALLOC_MAX_POINTS grid points (IM*JM*KM); larger requests
@@ -21,13 +22,19 @@
 //     on the array and must be serialised by the caller;
 //   * the device address of the array is looked up once per device, on that
 //     device's first call (with the device current); make that first call
-//     before any stream capture begins.
+//     before any stream capture begins;
+//   * a failure returns CBNS_ERR_CUDA and records the CUDA error text for
+//     cbns_status_string, as the other entry points do.
 #include <cuda_runtime.h>
 
 #include <mutex>
 
 #include "../../include/cbns_b200.h"
 #include "setup.cuh"
+
+namespace cbns {
+void set_last_error(const char* what, cudaError_t e);  // abi.cu
+}
 
 namespace {
 
@@ -65,15 +72,22 @@ extern "C" int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM,
   const unsigned long long N = (unsigned long long)IM * JM * KM;
   if (N > kMaxPoints) return CBNS_ERR_TOO_LARGE;
   double* s = nullptr;
-  if (scratch_for_current_device(&s) != cudaSuccess) return CBNS_ERR_CUDA;
+  cudaError_t e = scratch_for_current_device(&s);
+  if (e != cudaSuccess) {
+    cbns::set_last_error("cudaGetSymbolAddress(g_noalloc_scratch)", e);
+    return CBNS_ERR_CUDA;
+  }
   const size_t bytes = N * sizeof(double);
-  if (cudaMemcpy(s, f, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return CBNS_ERR_CUDA;
-  if (cbns::launch_gradient_dense((int)IM, (int)JM, (int)KM, s, s + kMaxPoints, s + 2 * kMaxPoints,
-                                  s + 3 * kMaxPoints, 0) != cudaSuccess)
+  e = cudaMemcpy(s, f, bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cbns::launch_gradient_dense((int)IM, (int)JM, (int)KM, s, s + kMaxPoints, s + 2 * kMaxPoints,
+                                    s + 3 * kMaxPoints, 0);
+  if (e == cudaSuccess) e = cudaMemcpy(fx, s + kMaxPoints, bytes, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(fy, s + 2 * kMaxPoints, bytes, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(fz, s + 3 * kMaxPoints, bytes, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    cbns::set_last_error("cbns_calc_gradient_noalloc", e);
     return CBNS_ERR_CUDA;
-  if (cudaMemcpy(fx, s + kMaxPoints, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(fy, s + 2 * kMaxPoints, bytes, cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(fz, s + 3 * kMaxPoints, bytes, cudaMemcpyDeviceToHost) != cudaSuccess)
-    return CBNS_ERR_CUDA;
+  }
   return CBNS_OK;
 }

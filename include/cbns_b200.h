@@ -204,11 +204,11 @@ int cbns_eval_rhs(cbns_ctx* ctx, int which, double* rhs_host);
 int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f,
                        double* fx, double* fy, double* fz);
 
-/* The same gradient for callers that cannot allocate device memory: code
- * running while a stream is captured into a CUDA graph, hosts whose device
- * memory belongs to their own pool allocator or a fixed budget, and paths that
- * cannot take the device-wide synchronisation of cudaMalloc/cudaFree.  It
- * calls no allocator; its device working copies live in one fixed array of
+/* The same gradient for callers that cannot allocate device memory: hosts
+ * whose device memory belongs to their own pool allocator or a fixed budget,
+ * and paths that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree.  Synchronous, like cbns_calc_gradient.  It calls no
+ * allocator; its device working copies live in one fixed array of
  * 4 x CBNS_NOALLOC_MAX_POINTS doubles (8 MiB) that every GPU loading this
  * library holds until the process exits.  IM*JM*KM above
  * CBNS_NOALLOC_MAX_POINTS returns CBNS_ERR_TOO_LARGE.  All calls on a device
@@ -216,7 +216,8 @@ int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f,
  * reads it first writes), so calls overlapping on the GPU race and must be
  * serialised by the caller.  The first call on each device looks up the
  * array's device address (with that device current); make it before any
- * stream capture begins.  No counterpart in the reference. */
+ * stream capture begins.  A CUDA failure returns CBNS_ERR_CUDA with its text
+ * in cbns_status_string.  No counterpart in the reference. */
 #define CBNS_NOALLOC_MAX_POINTS 262144u
 int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM, const double* f,
                                double* fx, double* fy, double* fz);

@@ -1,9 +1,10 @@
 """cbns_calc_gradient_noalloc, the gradient entry point for callers that cannot
-allocate device memory (inside a stream capture, under a foreign pool
-allocator or a fixed memory budget, or where cudaMalloc's device-wide
+allocate device memory (hosts whose device memory belongs to their own pool
+allocator or a fixed budget, or paths where cudaMalloc's device-wide
 synchronisation is not acceptable).  It must give what the allocating
 cbns_calc_gradient gives, on consecutive calls that reuse its one fixed
-device array, and refuse sizes above CBNS_NOALLOC_MAX_POINTS.
+device array, leave the device's free memory unchanged, and refuse sizes
+above CBNS_NOALLOC_MAX_POINTS.
 
 Collected last on purpose: a run that stops at the first failure has run
 every other test before this one.
@@ -51,6 +52,24 @@ def test_noalloc_gradient_matches_allocating_entry_point_on_consecutive_calls():
         for a, b in zip(got, ref):
             scale = np.max(np.abs(b))
             assert np.max(np.abs(a - b)) <= 1e-12 * scale
+
+
+def test_noalloc_gradient_allocates_nothing():
+    """Free device memory is the same before and after warmed-up calls."""
+    import torch
+
+    lib = _lib()
+    f = np.ascontiguousarray(np.random.default_rng(3).standard_normal((32, 48, 40)))
+    rc, _ = _grad(lib.cbns_calc_gradient_noalloc, f)  # warm-up: address lookup, module load
+    assert rc == _abi.CBNS_OK
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        rc, _ = _grad(lib.cbns_calc_gradient_noalloc, f)
+        assert rc == _abi.CBNS_OK
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0
 
 
 def test_noalloc_gradient_rejects_oversize_request():

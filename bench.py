@@ -79,11 +79,15 @@ def args():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--case", default="shock_vortex", choices=["shock_vortex", "blast", "vortex", "batch"])
+    ap.add_argument("--case", default="shock_vortex", choices=["shock_vortex", "blast", "vortex", "batch", "naca"])
     ap.add_argument("--blocks", type=int, default=64, help="--case batch: number of blocks (64 in the batched-blocks workload)")
     ap.add_argument("--size", default=None, help="IMxJMxKM (default: the case's config size)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--to-tend", action="store_true",
+                    help="run each path from the initial state to the case's end time (precision-form runs)")
+    ap.add_argument("--t-end", type=float, default=None, help="--to-tend: end time (default: the case's)")
+    ap.add_argument("--max-steps", type=int, default=100000, help="--to-tend: step limit")
     ap.add_argument("--no-reference-check", action="store_true",
                     help="skip the plain path's comparison with the reference build")
     ap.add_argument("--sensor", default=str(ROOT / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz"))
@@ -98,6 +102,11 @@ def make_case(name, size):
     if name == "blast":
         IM, JM, KM = size or (384, 384, 384)
         return cases.case_blast(IM, JM, KM), f"spherical blast {IM}x{JM}x{KM}, inviscid"
+    if name == "naca":
+        P, JM, KM = size or (384, 128, 4)
+        c = cases.case_naca_ogrid(P, JM, KM, grid="marched", start="potential")
+        return c, (f"NACA 0012 O-grid {P}x{JM}x{KM} (+{2 * 4} wrap points), viscous, M 0.8, AoA 1.25, Re 5e4, "
+                   f"first cell 1e-5, CFL 0.8, potential-flow start")
     IM, JM, KM = size or (64, 32, 16)
     return cases.case_vortex(IM, JM, KM), f"isentropic vortex {IM}x{JM}x{KM}, inviscid"
 
@@ -164,8 +173,16 @@ def init_block(case, precision):
     p["precision"] = precision
     b = Block(make_params(*case.shape, **p))
     b.calc_metrics(case.x, case.y, case.z)
-    b.set_conservative(case.Q0)
+    if case.Q0 is None:
+        b.initial_condition()
+        b.calc_conservative(CBNS_Q)
+    else:
+        b.set_conservative(case.Q0)
+        if p.get("viscous"):
+            b.calc_primitive(CBNS_Q)
     b.set_bc_calc_primitive(CBNS_Q)
+    if p.get("viscous"):
+        b.calc_viscous_terms()
     if precision == PREC_HYBRID:
         b.sensor_load(*SENSOR)
     return b
@@ -516,6 +533,147 @@ def run_reference(a):
     }))
 
 
+def run_to_tend(a):
+    """A case run from its initial state to its end time on each path (plain
+    FP64, split, learned-sensor hybrid), as the precision-form configuration
+    asks: density L2 / L-inf of the FP32-flux paths against the FP64 run at
+    the same end time, and each path's throughput over the whole run (CUDA
+    events on the launch stream, steps enqueued from the graph in chunks,
+    host reads of the step counter between chunks inside the timed region)."""
+    import torch
+    from cbns3d_cuda_b200 import PREC_FP64, PREC_HYBRID, PREC_SPLIT
+    torch.cuda.set_device(0)
+    load_sensor(a.sensor)
+    size = tuple(int(v) for v in a.size.split("x")) if a.size else None
+    case, wl = make_case(a.case, size)
+    N = n_updates(case)
+    t_end = case.t_end if a.t_end is None else a.t_end
+    chunk = 50
+    res = {}
+    clocks = None
+    for name, prec in (("fp64", PREC_FP64), ("split", PREC_SPLIT), ("hybrid", PREC_HYBRID)):
+        b = init_block(case, prec)
+        stream = torch.cuda.Stream()
+        b.set_stream(stream.cuda_stream)
+        variant = b.autotune()
+        b.set_time(0.0)
+        if prec == PREC_HYBRID:
+            b.sensor_stats_reset()
+        clk = Clocks(0) if prec == PREC_HYBRID else None
+        torch.cuda.synchronize()
+        if clk:
+            clk.__enter__()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        steps = 0
+        while True:
+            n = b.run(chunk, t_end)
+            steps += n
+            if n < chunk or steps >= a.max_steps:
+                break
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if clk:
+            clk.__exit__(None, None, None)
+            clocks = clk.summary()
+        ms = e0.elapsed_time(e1)
+        t_fin, dt_last = b.get_time()
+        IM, JM, KM = case.shape
+        rho = b.get_conservative().reshape(KM + 4, JM + 4, IM + 4, 5)[2:-2, 2:-2, 2:-2, 0].copy()
+        stats = b.sensor_stats() if prec == PREC_HYBRID else None
+        b.close()
+        res[name] = {"value": N * steps / (ms / 1e3), "ms_per_step": ms / steps, "steps": steps, "t_final": t_fin,
+                     "stage_variant": variant, "rho": rho, "stats": stats}
+        del b
+    r64 = res["fp64"]["rho"]
+    out_paths = {}
+    for name, r in res.items():
+        d = {k: v for k, v in r.items() if k not in ("rho", "stats")}
+        if name != "fp64":
+            rr = r["rho"]
+            d["rho_l2_vs_fp64"] = float(np.sqrt(np.mean((rr - r64) ** 2) / np.mean(r64 ** 2)))
+            d["rho_linf_vs_fp64"] = float(np.max(np.abs(rr - r64)) / np.max(np.abs(r64)))
+        if r["stats"]:
+            st = r["stats"]
+            d["weno_face_fraction"] = st["weno_faces"] / max(1, r["steps"] * st["faces_per_step"])
+            d["audit_rejected_steps"] = st["audit_fail_steps"]
+            d["sensor_timeouts"] = st["sensor_fail"]
+        out_paths[name] = d
+    h = out_paths["hybrid"]
+    print(json.dumps({
+        "metric": "cell-updates/s: learned-hybrid FP32 vs plain FP64 WENO5, same B200, rho-L2<=1e-5",
+        "value": h["value"], "unit": "cell-updates/s", "n_gpus": 1, "steps": h["steps"], "warmup": 0,
+        "ms_per_step": h["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 flux / f64 state", "data": "synthetic",
+        "config": {"workload": f"{wl}, from the initial state to t = {t_end}", "grid": list(case.shape),
+                   "cell_updates_per_step": N, "t_end": t_end,
+                   "l2": "inputs larger than L2"},
+        "rho_l2_vs_fp64": h["rho_l2_vs_fp64"], "rho_linf_vs_fp64": h["rho_linf_vs_fp64"],
+        "paths": out_paths, "hybrid_over_fp64": h["value"] / out_paths["fp64"]["value"],
+        "split_over_fp64": out_paths["split"]["value"] / out_paths["fp64"]["value"],
+        "clocks": clocks}))
+
+
+def run_naca(a):
+    """The viscous NACA 0012 O-grid configuration on the plain FP64 path: K
+    steps from the started flow (graph replays in chunks of 500, each timed
+    with CUDA events on the launch stream), the state checked for positivity
+    after every chunk (outside the timed region), and the per-kernel times of
+    one more chunk."""
+    import torch
+    from cbns3d_cuda_b200 import PREC_FP64
+    torch.cuda.set_device(0)
+    size = tuple(int(v) for v in a.size.split("x")) if a.size else None
+    case, wl = make_case("naca", size)
+    IM, JM, KM = case.shape
+    N = n_updates(case)
+    b = init_block(case, PREC_FP64)
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    b.set_time(0.0)
+    K = a.steps
+    chunk = min(500, K)
+    ms_total, done, history = 0.0, 0, []
+    clk = Clocks(0)
+    clk.__enter__()
+    while done < K:
+        n = min(chunk, K - done)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        b.run_async(n)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_total += e0.elapsed_time(e1)
+        done += n
+        q = b.get_conservative().reshape(KM + 4, JM + 4, IM + 4, 5)[2:-2, 2:-2, 2:-2]
+        r = q[..., 0]
+        pr = 0.4 * (q[..., 4] - 0.5 * (q[..., 1] ** 2 + q[..., 2] ** 2 + q[..., 3] ** 2) / r)
+        t, dt = b.get_time()
+        history.append({"steps": done, "t": t, "dt": dt, "rho_min": float(np.min(r)), "p_min": float(np.min(pr)),
+                        "p_max": float(np.max(pr)), "finite": bool(np.isfinite(q).all())})
+        if not history[-1]["finite"] or history[-1]["p_min"] <= 0 or history[-1]["rho_min"] <= 0:
+            break
+    clk.__exit__(None, None, None)
+    b.prof_enable(True)
+    b.prof_reset()
+    b.run(100)
+    kern = {name: {"ms_per_step": b.prof_read(i)[0] / 100, "launches_per_step": b.prof_read(i)[1] / 100}
+            for i, name in enumerate(["stage", "bc", "viscous", "dt", "sensor", "audit", "weno_faces"])
+            if b.prof_read(i)[1]}
+    b.close()
+    ok = all(h["finite"] and h["p_min"] > 0 and h["rho_min"] > 0 for h in history)
+    print(json.dumps({
+        "metric": "cell-updates/s: learned-hybrid FP32 vs plain FP64 WENO5, same B200, rho-L2<=1e-5",
+        "value": N * done / (ms_total / 1e3), "unit": "cell-updates/s", "n_gpus": 1, "steps": done, "warmup": 0,
+        "ms_per_step": ms_total / done, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": wl, "path": "plain FP64 (viscous divergence at the node, full viscous dt limit, "
+                                           "O-grid boundary mode)", "grid": list(case.shape),
+                   "cell_updates_per_step": N},
+        "stable": ok, "history": history, "kernels": kern, "clocks": clk.summary()}))
+
+
 def run_batch(a):
     """Batched-blocks workload: independent viscous blocks of uneven size (seeded draw),
     learned-sensor hybrid, advanced by one persistent work-queue launch of the
@@ -601,5 +759,9 @@ if __name__ == "__main__":
         run_reference(a)
     elif a.case == "batch":
         run_batch(a)
+    elif a.case == "naca":
+        run_naca(a)
+    elif a.to_tend:
+        run_to_tend(a)
     else:
         run_ours(a)

@@ -12,11 +12,13 @@ import ctypes as C
 import numpy as np
 
 from . import _abi
-from ._abi import (BC_CHARACTERISTIC, BC_FARFIELD, BC_OGRID, BC_REFERENCE, OGRID_WRAP, CBNS_Q, CBNS_QP, PREC_FP64, PREC_HYBRID, PREC_SPLIT,  # noqa: F401
+from ._abi import (BC_CHARACTERISTIC, BC_FARFIELD, BC_OGRID, BC_REFERENCE, DTV_FULL, DTV_REFERENCE, OGRID_WRAP,  # noqa: F401
+                   CBNS_Q, CBNS_QP, PREC_FP64, PREC_HYBRID, PREC_SPLIT,
                    VISDIV_CENTERED, VISDIV_REFERENCE, CbnsError, Params)
 
 __all__ = ["Block", "Batch", "Params", "CbnsError", "CBNS_Q", "CBNS_QP", "PREC_FP64", "PREC_SPLIT", "PREC_HYBRID",
            "VISDIV_REFERENCE", "VISDIV_CENTERED", "BC_REFERENCE", "BC_FARFIELD", "BC_CHARACTERISTIC", "BC_OGRID", "OGRID_WRAP",
+           "DTV_REFERENCE", "DTV_FULL",
            "make_params"]
 
 NG = 2
@@ -25,7 +27,7 @@ NEQ = 5
 
 def make_params(IM, JM, KM, *, CFL=0.5, angle_attack=0.0, i_begin=1, i_end=0, Mach=0.5, Re=1.0e4, gamma=1.4,
                 Pr=0.72, Pr_t=0.9, T_inf=288.15, viscous=False, precision=PREC_FP64,
-                vis_divergence=VISDIV_REFERENCE, bc_mode=BC_REFERENCE) -> Params:
+                vis_divergence=VISDIV_REFERENCE, bc_mode=BC_REFERENCE, dt_viscous=DTV_REFERENCE) -> Params:
     p = Params()
     p.IM, p.JM, p.KM = IM, JM, KM
     p.CFL, p.angle_attack = CFL, angle_attack
@@ -33,6 +35,7 @@ def make_params(IM, JM, KM, *, CFL=0.5, angle_attack=0.0, i_begin=1, i_end=0, Ma
     p.Mach, p.Re, p.gamma, p.Pr, p.Pr_t, p.T_inf = Mach, Re, gamma, Pr, Pr_t, T_inf
     p.viscous, p.precision, p.vis_divergence = int(viscous), int(precision), int(vis_divergence)
     p.bc_mode = int(bc_mode)
+    p.dt_viscous = int(dt_viscous)
     return p
 
 

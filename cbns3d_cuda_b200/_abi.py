@@ -40,6 +40,8 @@ BC_FARFIELD = 1   # every boundary and ghost node holds the state it was set to
 BC_CHARACTERISTIC = 2  # Riemann-invariant far field against the free stream on every face
 BC_OGRID = 3      # i wraps around (OGRID_WRAP copied points either side), wall j = 0, characteristic j = JM-1
 OGRID_WRAP = 4
+DTV_REFERENCE = 0  # viscous dt term scaled by the local |u|/c, as the reference
+DTV_FULL = 1       # viscous dt term without that factor (wall-resolved grids)
 
 
 class Params(C.Structure):
@@ -52,7 +54,7 @@ class Params(C.Structure):
         ("Mach", C.c_double), ("Re", C.c_double), ("gamma", C.c_double),
         ("Pr", C.c_double), ("Pr_t", C.c_double), ("T_inf", C.c_double),
         ("viscous", C.c_int), ("precision", C.c_int), ("vis_divergence", C.c_int),
-        ("bc_mode", C.c_int), ("reserved", C.c_int * 4),
+        ("bc_mode", C.c_int), ("dt_viscous", C.c_int), ("reserved", C.c_int * 3),
     ]
 
 

@@ -445,21 +445,36 @@ def case_naca(IM=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5):
     return Case("naca", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)
 
 
-def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, viscous=True, grid="blend"):
+def case_naca_ogrid(P=384, JM=128, KM=4, nsteps=2000, CFL=0.8, first=1.0e-5, viscous=True, grid="blend",
+                    start="freestream"):
     """NACA 0012 case with its own boundaries (bc_mode = 3, BC_OGRID): an
     O-grid of P points around the profile, wrapped periodically in i (stored
     with 4 copied points either side, IM = P + 8), adiabatic no-slip wall on
     j = 0 (slip when inviscid), characteristic far field on j = JM-1; M 0.8,
-    AoA 1.25 deg, Re 5e4, free-stream start.  grid "blend":
-    naca0012_ogrid_blend (sharp edge, straight lines to a far circle; regular
-    on small grids with a coarse first cell), "marched":
-    naca0012_ogrid_marched (rounded edge, wall-normal marched lines; valid at
-    the full 384 x 128 size with a 1e-5 first cell)."""
+    AoA 1.25 deg, Re 5e4.  grid "blend": naca0012_ogrid_blend (sharp edge,
+    straight lines to a far circle; regular on small grids with a coarse first
+    cell), "marched": naca0012_ogrid_marched (rounded edge, wall-normal
+    marched lines; valid at the full 384 x 128 size with a 1e-5 first cell).
+    start "freestream": the reference's impulsive start (Q0 None: the free
+    stream everywhere); "potential": the started flow of naca_started_state,
+    with the viscous divergence taken at the node (vis_divergence 1) and the
+    full viscous time-step limit (dt_viscous 1).  On the wall-resolved grid the
+    impulsive start expands to vacuum round the rounded trailing edge within
+    ~15 steps, the reference's shifted divergence placement grows a
+    grid-scale oscillation along the wall within ~40, and the reference's
+    viscous time-step term vanishes where the flow is at rest."""
     gen = {"blend": naca0012_ogrid_blend, "marched": naca0012_ogrid_marched}[grid]
     x, y, z = (ogrid_wrap(a) for a in gen(P, JM, KM, first=first))
     params = dict(CFL=CFL, Mach=0.8, angle_attack=1.25, Re=5.0e4, Pr=0.72, Pr_t=0.9, T_inf=288.15, gamma=1.4,
                   i_begin=1, i_end=P + 8, viscous=viscous, bc_mode=3)
-    return Case("naca_ogrid", x, y, z, params, None, t_end=1.0e6, nsteps=nsteps)
+    Q0 = None
+    if start == "potential":
+        Q0 = naca_started_state(x, y, params["Mach"], params["angle_attack"], params["gamma"])
+        if viscous:
+            params.update(vis_divergence=1, dt_viscous=1)
+    elif start != "freestream":
+        raise ValueError(f"unknown start {start!r}")
+    return Case("naca_ogrid", x, y, z, params, Q0, t_end=1.0e6, nsteps=nsteps)
 
 
 def case_blast(IM=384, JM=384, KM=384, t_end=0.05, CFL=0.5):
@@ -544,3 +559,109 @@ def case_shock_vortex(IM=256, JM=256, KM=128, nsteps=100, CFL=0.5, Ms=1.2, eps=0
     Q = conservative(rho, u, v, w, p, g)
     params = dict(CFL=CFL, Mach=Ms, gamma=g, i_begin=1, i_end=0)
     return Case("shock_vortex", x, y, z, params, Q, t_end=1.0e6, nsteps=nsteps)
+
+
+# ---------------------------------------------------------------- started flow
+def panel_flow(xs, ys, alpha_deg):
+    """Incompressible potential flow of unit free-stream speed at angle
+    alpha_deg past the closed polygon (xs, ys) (points in clockwise order, the
+    trailing edge at point 0), by the Hess-Smith panel method: a constant
+    source density per panel and one vortex density shared by all panels,
+    fixed by zero normal velocity at the panel midpoints and the Kutta
+    condition (equal and opposite tangential velocity on the two panels that
+    meet at the trailing edge).  Returns a function (x, y) -> (u, v) for points
+    off the surface."""
+    P = len(xs)
+    x0, y0 = np.asarray(xs, float), np.asarray(ys, float)
+    x1, y1 = np.roll(x0, -1), np.roll(y0, -1)
+    th = np.arctan2(y1 - y0, x1 - x0)
+    ct, st = np.cos(th), np.sin(th)
+    xm, ym = 0.5 * (x0 + x1), 0.5 * (y0 + y1)
+    al = np.deg2rad(alpha_deg)
+    ua, va = np.cos(al), np.sin(al)
+
+    def unit(px, py):
+        """Velocities at points (px, py) (shape (n,)) induced by unit source
+        and unit vortex density on every panel: (us, vs, uv, vv), each (n, P)."""
+        rsx, rsy = x0[None, :] - px[:, None], y0[None, :] - py[:, None]
+        rex, rey = x1[None, :] - px[:, None], y1[None, :] - py[:, None]
+        beta = np.arctan2(rsx * rey - rsy * rex, rsx * rex + rsy * rey)
+        lg = 0.5 * np.log((rsx * rsx + rsy * rsy) / (rex * rex + rey * rey))
+        # panel frame: source (lg, beta)/(2 pi), vortex (beta, -lg)/(2 pi) rotated
+        # by +90 degrees from it (clockwise circulation positive)
+        sl, sn = lg / (2 * np.pi), beta / (2 * np.pi)
+        us, vs = sl * ct - sn * st, sl * st + sn * ct
+        uv, vv = sn * ct + sl * st, sn * st - sl * ct
+        return us, vs, uv, vv
+
+    us, vs, uv, vv = unit(xm, ym)
+    idx = np.arange(P)
+    # self-influence at a panel's own midpoint, outer side: beta = pi
+    us[idx, idx], vs[idx, idx] = -0.5 * st, 0.5 * ct
+    uv[idx, idx], vv[idx, idx] = 0.5 * ct, 0.5 * st
+    nx, ny = -st, ct
+    A = np.zeros((P + 1, P + 1))
+    A[:P, :P] = us * nx[:, None] + vs * ny[:, None]
+    A[:P, P] = (uv * nx[:, None] + vv * ny[:, None]).sum(1)
+    b = np.zeros(P + 1)
+    b[:P] = -(ua * nx + va * ny)
+    for i in (0, P - 1):  # Kutta: tangential velocities on panels 0 and P-1 sum to zero
+        A[P, :P] += us[i] * ct[i] + vs[i] * st[i]
+        A[P, P] += (uv[i] * ct[i] + vv[i] * st[i]).sum()
+        b[P] -= ua * ct[i] + va * st[i]
+    sol = np.linalg.solve(A, b)
+    q, g = sol[:P], sol[P]
+
+    def velocity(px, py):
+        px, py = np.asarray(px, float).ravel(), np.asarray(py, float).ravel()
+        u = np.empty_like(px)
+        v = np.empty_like(px)
+        for s in range(0, px.size, 4096):
+            e = slice(s, s + 4096)
+            a, bb, c, d = unit(px[e], py[e])
+            u[e] = ua + a @ q + g * c.sum(1)
+            v[e] = va + bb @ q + g * d.sum(1)
+        return u, v
+
+    return velocity
+
+
+def naca_started_state(x, y, Mach, alpha_deg, gamma=1.4, wrap=4):
+    """Started-flow initial state of the wrapped NACA O-grid block (x, y of
+    shape (KM, JM, P + 2 wrap), j = 0 the wall): the compressible free stream
+    replaced by the incompressible potential flow past the profile with the
+    Kutta condition (panel_flow over the j = 0 line), density and pressure from
+    the isentropic relations of the local speed (T / T_inf = 1 + (gamma-1)/2
+    M^2 (1 - |u|^2), floored at 0.5).  Nodes closer to the wall than half the
+    local surface spacing take the tangential velocity of the first node along
+    their j line that is not; the wall nodes take zero (the no-slip boundary
+    condition sets them anyway).  Returns the ghosted AoS state (ghost layers
+    copied from the nearest node; every boundary mode rewrites them)."""
+    xs, ys = x[0, 0, wrap:-wrap], y[0, 0, wrap:-wrap]
+    vel = panel_flow(xs, ys, alpha_deg)
+    X, Y = x[0], y[0]
+    JM, IM = X.shape
+    u, v = vel(X[1:], Y[1:])
+    u, v = u.reshape(JM - 1, IM), v.reshape(JM - 1, IM)
+    # surface spacing at each i and the first usable node of each j line
+    sx, sy = X[0], Y[0]
+    ds = 0.5 * (np.hypot(np.roll(sx, -1) - sx, np.roll(sy, -1) - sy) +
+                np.hypot(sx - np.roll(sx, 1), sy - np.roll(sy, 1)))
+    d = np.hypot(X - sx[None, :], Y - sy[None, :])
+    tx, ty = np.roll(sx, -1) - np.roll(sx, 1), np.roll(sy, -1) - np.roll(sy, 1)
+    tn = np.hypot(tx, ty)
+    tx, ty = tx / tn, ty / tn
+    for i in range(IM):
+        jf = int(np.argmax(d[1:, i] >= 0.5 * ds[i]))  # index into rows 1..JM-1
+        ut = u[jf, i] * tx[i] + v[jf, i] * ty[i]
+        u[:jf, i], v[:jf, i] = ut * tx[i], ut * ty[i]
+    U = np.zeros((JM, IM))
+    V = np.zeros((JM, IM))
+    U[1:], V[1:] = u, v
+    T = np.maximum(1.0 + 0.5 * (gamma - 1.0) * Mach ** 2 * (1.0 - (U * U + V * V)), 0.5)
+    rho = T ** (1.0 / (gamma - 1.0))
+    p = T ** (gamma / (gamma - 1.0)) / (gamma * Mach ** 2)
+    KM = x.shape[0]
+    f = [np.broadcast_to(a, (KM, JM, IM)) for a in (rho, U, V, np.zeros_like(U), p)]
+    Q = conservative(*f, gamma)
+    return np.pad(Q, ((NG, NG), (NG, NG), (NG, NG), (0, 0)), mode="edge")

@@ -228,6 +228,7 @@ ViscArgs visc_args(cbns_ctx* c, bool check_done, bool sigma) {
   a.Re_inv = c->ph.Re_inv;
   a.C_T_inf = c->ph.C_T_inf;
   a.C_dt_v = c->ph.C_dt_v;
+  a.dt_full = c->prm.dt_viscous == CBNS_DTV_FULL;
   a.qc = -c->ph.Pr_inv * c->ph.gam1_inv / c->ph.Mach2;
   for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
   fill_met(c, a.met);
@@ -301,6 +302,7 @@ int sigma_launch(cbns_ctx* c) {
   a.gamma = c->ph.gamma;
   a.gam1 = c->ph.gam1;
   a.C_dt_v = c->ph.C_dt_v;
+  a.dt_full = c->prm.dt_viscous == CBNS_DTV_FULL;
   a.viscous = c->ph.viscous;
   a.q = c->qb[c->lq];
   for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
@@ -715,6 +717,7 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
     g_last = "an O-grid block needs IM - 2*CBNS_OGRID_WRAP >= 6";
     return CBNS_ERR_ARG;
   }
+  if (p->dt_viscous != CBNS_DTV_REFERENCE && p->dt_viscous != CBNS_DTV_FULL) return CBNS_ERR_ARG;
   for (int r : p->reserved)
     if (r != 0) return CBNS_ERR_ARG;
   const double ng = ((double)p->IM + 4) * ((double)p->JM + 4) * ((double)p->KM + 4);

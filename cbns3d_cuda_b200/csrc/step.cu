@@ -43,7 +43,9 @@ __global__ void sigma_nodes(const SigmaArgs a) {
     }
     const double c = sqrt(a.gamma * pp / rr);
     double fv = 0.0;
-    if (a.viscous) fv = 2.0 * a.mu[o] * a.C_dt_v * sqrt(uu * uu + vv * vv + ww * ww) / c / rr;
+    if (a.viscous)
+      fv = a.dt_full ? 2.0 * a.mu[o] * a.C_dt_v / rr
+                     : 2.0 * a.mu[o] * a.C_dt_v * sqrt(uu * uu + vv * vv + ww * ww) / c / rr;
     double s = 0.0;
 #pragma unroll
     for (int dd = 0; dd < 3; ++dd) {

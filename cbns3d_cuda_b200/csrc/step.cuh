@@ -9,6 +9,7 @@ struct SigmaArgs {
   Dims d;
   double gamma, gam1, C_dt_v;
   int viscous;
+  int dt_full;            // viscous spectral radius without the |u|/c factor (CBNS_DTV_FULL)
   const double* q;        // inviscid: primitives recomputed from this buffer
   const double* prim[6];  // viscous: rho,u,v,w,p,T
   const double* mu;       // viscous

@@ -89,7 +89,8 @@ __global__ void __launch_bounds__(128) visc_node_kernel(const ViscArgs a) {
     if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && k >= 0 && k < d.KM) {
       const double rr = a.prim[0][o], pp = a.prim[4][o];
       const double c = sqrt(a.gamma * pp / rr);
-      const double fv = 2.0 * mu * a.C_dt_v * sqrt(uu * uu + vv * vv + ww * ww) / c / rr;
+      const double fv = a.dt_full ? 2.0 * mu * a.C_dt_v / rr
+                                  : 2.0 * mu * a.C_dt_v * sqrt(uu * uu + vv * vv + ww * ww) / c / rr;
       double s = 0.0;
 #pragma unroll
       for (int dd = 0; dd < 3; ++dd) {

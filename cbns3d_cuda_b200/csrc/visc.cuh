@@ -8,6 +8,7 @@ namespace cbns {
 struct ViscArgs {
   Dims d;
   double gamma, Re_inv, C_T_inf, C_dt_v;
+  int dt_full;               // viscous spectral radius without the |u|/c factor (CBNS_DTV_FULL)
   double qc;                 // -1/(Pr (gamma-1) M^2): heat-flux factor before mu/Re
   const double* prim[6];     // rho,u,v,w,p,T
   const double* met[10];

@@ -104,6 +104,16 @@ extern "C" {
 #define CBNS_BC_OGRID 3
 #define CBNS_OGRID_WRAP 4
 
+/* cbns_params.dt_viscous: the viscous part of the spectral radius behind the
+ * CFL time step.  REFERENCE: |grad xi|^2 * 2 mu C_dt_v |u| / (c rho) per
+ * direction, as src/time_step_kernel.cu:54 (the local Mach number |u|/c scales
+ * it, so it vanishes where the flow is at rest, e.g. at a no-slip wall).
+ * FULL (no counterpart in the reference): |grad xi|^2 * 2 mu C_dt_v / rho, the
+ * explicit diffusion limit without that factor, which the boundary layer of a
+ * wall-resolved grid needs (first cells of 1e-5 chords). */
+#define CBNS_DTV_REFERENCE 0
+#define CBNS_DTV_FULL      1
+
 /* cbns_init_case kinds (no counterpart in the reference) and their parameters:
  *   VORTEX        Mach, strength beta, centre x, centre y, radius R, stream
  *                 direction (dx, dy): isentropic vortex in a free stream
@@ -133,7 +143,8 @@ typedef struct cbns_params {
   int      precision;       /* CBNS_PREC_*                                         */
   int      vis_divergence;  /* CBNS_VISDIV_*                                       */
   int      bc_mode;         /* CBNS_BC_*                                           */
-  int      reserved[4];     /* must be zero                                        */
+  int      dt_viscous;      /* CBNS_DTV_*                                          */
+  int      reserved[3];     /* must be zero                                        */
 } cbns_params;
 
 typedef struct cbns_ctx cbns_ctx;

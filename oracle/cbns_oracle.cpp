@@ -718,7 +718,10 @@ struct Oracle {
           const double r = rho[t], uu = u[t], vv = v[t], ww = w[t], pp = p[t];
           const double c = std::sqrt(P.gamma * pp / r);
           double fv = 0.0;
-          if (P.viscous) fv = 2.0 * mu[t] * D.C_dt_v * std::sqrt(uu * uu + vv * vv + ww * ww) / c / r;
+          // dt_viscous = 1 (CBNS_DTV_FULL) drops the local-Mach factor |u|/c
+          if (P.viscous)
+            fv = P.dt_viscous == 1 ? 2.0 * mu[t] * D.C_dt_v / r
+                                   : 2.0 * mu[t] * D.C_dt_v * std::sqrt(uu * uu + vv * vv + ww * ww) / c / r;
           double s = 0.0;
           for (int d = 0; d < 3; ++d) {
             const double nx = met[3 * d][t], ny = met[3 * d + 1][t], nz = met[3 * d + 2][t];

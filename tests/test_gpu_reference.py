@@ -5,8 +5,10 @@ reference sources by `make -C oracle ref`) and this project's driver
 (cbns3d_cuda_b200/bin/cbns3d_b200, which calls the CUDA library through the
 block3d_cuda shims) read the same input.txt, Plot3D grid and checkpoint; the
 checkpoints they write must agree to relative L-infinity <= 1e-10 per
-variable after 100 steps (inviscid) / 50 steps (viscous), and the VTK files
-must have the same layout with values equal to their printed precision.
+variable after 100 steps (isentropic vortex, inviscid), 20 steps (the
+shock-vortex case of the throughput benchmark at 128 x 128 x 64, inviscid) and
+50 steps (NACA, viscous), and the VTK files must have the same layout with
+values equal to their printed precision.
 """
 import subprocess
 from pathlib import Path
@@ -48,6 +50,7 @@ def vtk_fields(path):
 CASES = {
     "vortex_c0": (lambda: cases.case_vortex(64, 32, 16), 100, "inv"),
     "naca_viscous": (lambda: cases.case_naca(64, 32, 6, first=1e-3), 50, "visc"),
+    "shock_vortex_mid": (lambda: cases.case_shock_vortex(128, 128, 64), 20, "inv"),
 }
 # the programs compared with the reference build on identical inputs
 VARIANTS = {

@@ -69,6 +69,10 @@ class Block:
         except Exception:
             pass
 
+    def synchronize(self):
+        """Wait for every call enqueued on the block's stream."""
+        _abi.check(self.lib.cbns_synchronize(self.h), "cbns_synchronize")
+
     def set_stream(self, stream_ptr: int | None):
         _abi.check(self.lib.cbns_set_stream(self.h, C.c_void_p(stream_ptr or 0)), "cbns_set_stream")
 
@@ -213,6 +217,13 @@ class Block:
         v = C.c_int()
         _abi.check(self.lib.cbns_autotune(self.h, C.byref(v)), "cbns_autotune")
         return v.value
+
+    def stage_variant(self, variant: int = -1) -> int:
+        """Select compiled stage-kernel variant `variant` (-1: only query);
+        returns the number of variants."""
+        n = C.c_int()
+        _abi.check(self.lib.cbns_stage_variant(self.h, int(variant), C.byref(n)), "cbns_stage_variant")
+        return n.value
 
     # timing -----------------------------------------------------------------
     def prof_enable(self, on=True):

@@ -98,6 +98,8 @@ SIGNATURES = [
     ("cbns_eval_rhs", C.c_int, [_V, C.c_int, _D]),
     ("cbns_calc_gradient", C.c_int, [C.c_uint, C.c_uint, C.c_uint, _D, _D, _D, _D]),
     ("cbns_autotune", C.c_int, [_V, C.POINTER(C.c_int)]),
+    ("cbns_stage_variant", C.c_int, [_V, C.c_int, C.POINTER(C.c_int)]),
+    ("cbns_synchronize", C.c_int, [_V]),
     ("cbns_sensor_sample", C.c_int,
      [_V, C.c_int, C.c_uint, C.c_uint, _V, _V, _V, _V, C.c_uint, C.POINTER(C.c_uint)]),
     ("cbns_mlp_grad", C.c_int, [_V, _V, _V, C.c_uint, C.c_float, _V, _V, _V]),

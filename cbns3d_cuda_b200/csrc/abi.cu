@@ -24,6 +24,7 @@
 #include "setup.cuh"
 #include "stage.cuh"
 #include "step.cuh"
+#include "tma.cuh"
 #include "visc.cuh"
 #include "sensor_kernels.cuh"
 
@@ -63,6 +64,7 @@ struct cbns_ctx {
   int ntile_i = 1, ntile_j = 1, kchunk = 1;
   int stage_variant = 0;  // compiled occupancy variant of the stage kernel (cbns_autotune)
   int nsm = 148;          // SMs of the device
+  StageMaps tm[3];        // FP32 precisions: TMA maps of the stage kernel, per state buffer
   // hybrid flux: the learned sensor's parameters and per-face decisions
   float* sensor_params = nullptr;  // device, CBNS_SENSOR_NPARAM floats
   unsigned char* mask = nullptr;   // device, one byte per face: the decisions the fluxes use
@@ -240,7 +242,16 @@ ViscArgs visc_args(cbns_ctx* c, bool check_done, bool sigma) {
   return a;
 }
 
-StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const double* qp, double* out, bool sigma) {
+// An inviscid block under the reference's boundary conditions with no wake cut
+// (i_begin = 1) and no wall (i_end = 0): its boundary conditions need only
+// the new state of the node next to each boundary node, so the stage kernel
+// applies them itself (fused_bc in stage.cu) in whole-step runs.
+bool bc_fusable(const cbns_ctx* c) {
+  return c->prm.bc_mode == CBNS_BC_REFERENCE && !c->ph.viscous && c->ph.i_begin == 1u && c->ph.i_end == 0u;
+}
+
+StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const double* qp, double* out, bool sigma,
+                     bool fuse_bc = false) {
   StageArgs a;
   a.d = c->d;
   a.gamma = c->ph.gamma;
@@ -263,8 +274,13 @@ StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const dou
   a.kchunk = c->kchunk;
   a.visdiv = c->ph.visdiv;
   a.sigma = sigma;
+  a.fuse_bc = fuse_bc && bc_fusable(c);
+  a.p_inf = c->ph.p_inf;
   a.mask = c->ph.precision == CBNS_PREC_HYBRID ? c->mask : nullptr;
   a.wflux = c->wflux;
+  a.tm = c->tm[0];  // src is always one of the three state buffers
+  for (int b = 0; b < 3; ++b)
+    if (src == c->qb[b]) a.tm = c->tm[b];
   for (int m = 0; m < 6; ++m) a.area32[m] = c->f.area32[m];
   return a;
 }
@@ -441,12 +457,25 @@ int enqueue_step(cbns_ctx* c) {
     // O-grid: the wrap copy rewrites nodes stage 3 updated, so the spectral
     // radius is swept after the boundary pass
     const bool fuse = last && !visc && !ogrid(c);
-    RET(stage_launch(c, stage_args(c, s[k].src, s[k].q0, s[k].qp, s[k].out, fuse), k + 1));
-    RET(bc_launch(c, bc_args(c, s[k].out, true, fuse), false));
+    RET(stage_launch(c, stage_args(c, s[k].src, s[k].q0, s[k].qp, s[k].out, fuse, true), k + 1));
+    // no boundary pass in the step when the stage kernel applied the boundary
+    // conditions (bc_fusable), or for a viscous far-field block, whose
+    // boundary and ghost nodes hold their Q, so that their primitives (formed
+    // at the start of the run) stand, the stage kernel recovering the interior
+    // primitives and the viscous node kernel the spectral radii
+    if (!bc_fusable(c) && !(visc && c->prm.bc_mode == CBNS_BC_FARFIELD))
+      RET(bc_launch(c, bc_args(c, s[k].out, true, fuse), false));
     if (last && !visc && ogrid(c)) RET(sigma_launch(c));
     if (visc) RET(visc_launch(c, visc_args(c, true, last)));
   }
   return CBNS_OK;
+}
+
+// A stage kernel whose TMA wait ran out left the state invalid.
+int stage_status(const StepState& h) {
+  if (!h.stage_fail) return CBNS_OK;
+  g_last = "a stage kernel's TMA wait timed out; the state is not valid";
+  return CBNS_ERR_CUDA;
 }
 
 int check_ready(cbns_ctx* c) {
@@ -479,7 +508,16 @@ int run_prepare(cbns_ctx* c, double t_end) {
   h.done = 0;
   h.nan_dt = 0;
   h.steps = 0;
+  h.sigma_fixed = 0ull;
   CK(cudaMemcpyAsync(c->st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
+  // viscous far field: the steps leave the boundary primitives as they are
+  // (enqueue_step); form them here from the state the run starts from
+  if (c->ph.viscous && c->prm.bc_mode == CBNS_BC_FARFIELD) RET(bc_launch(c, bc_args(c, c->qb[c->lq], false, false), false));
+  // fused boundary conditions: the held j-face rows' share of every step's dt
+  if (bc_fusable(c)) {
+    CK(launch_bc_fixed_sigma(bc_args(c, c->qb[c->lq], false, false), c->stream));
+    c->launches += 1;
+  }
   RET(sync(c));
   if (!c->sigma_valid) {
     RET(sigma_launch(c));
@@ -508,6 +546,19 @@ struct cbns_batch {
   int* start = nullptr;       // device: nblocks + 1
   unsigned* counter = nullptr;
   int total = 0;
+  // batched per-block kernels: the step prologues, and (every block in
+  // CBNS_BC_FARFIELD) the far-field boundary and viscous node kernels of all
+  // blocks in one launch per stage; device tables, block b owning CTAs
+  // cta[b] .. cta[b+1]-1
+  bool farfield = false;
+  void* tables = nullptr;            // one allocation holding the tables below
+  StepState** st_tab = nullptr;      // nblocks
+  double* cfl_tab = nullptr;         // nblocks
+  BCArgs* bc_tab = nullptr;          // 3 stages x nblocks
+  ViscArgs* visc_tab = nullptr;      // 3 stages x nblocks
+  int* bc_cta = nullptr;             // nblocks + 1
+  int* visc_cta = nullptr;           // nblocks + 1
+  int bc_total = 0, visc_total = 0;
   std::vector<int> roles;     // (lq, lp, ls) per block at capture
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -543,9 +594,9 @@ int batch_tables(cbns_batch* b) {
     double* P0 = c->qb[c->lq];
     double* P1 = c->qb[c->ls];
     double* P2 = c->qb[c->lp];
-    tab[0 * nb + i] = stage_args(c, P0, P0, P0, P1, false);
-    tab[1 * nb + i] = stage_args(c, P1, P0, P1, P2, false);
-    tab[2 * nb + i] = stage_args(c, P2, P0, P2, P0, !b->visc);
+    tab[0 * nb + i] = stage_args(c, P0, P0, P0, P1, false, true);
+    tab[1 * nb + i] = stage_args(c, P1, P0, P1, P2, false, true);
+    tab[2 * nb + i] = stage_args(c, P2, P0, P2, P0, !b->visc, true);
     start[i + 1] = start[i] + c->ntile_i * c->ntile_j * ((c->d.KM - 2 + c->kchunk - 1) / c->kchunk);
     b->roles.insert(b->roles.end(), {c->lq, c->lp, c->ls});
   }
@@ -553,6 +604,33 @@ int batch_tables(cbns_batch* b) {
   b->host_args = tab;
   CK(cudaMemcpyAsync(b->args, tab.data(), tab.size() * sizeof(StageArgs), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  // the batched per-block kernels' tables
+  std::vector<StepState*> sts(nb);
+  std::vector<double> cfl(nb);
+  std::vector<BCArgs> bct(3 * nb);
+  std::vector<ViscArgs> vt(3 * nb);
+  std::vector<int> bcc(nb + 1, 0), vc(nb + 1, 0);
+  for (int i = 0; i < nb; ++i) {
+    cbns_ctx* c = b->blk[i];
+    sts[i] = c->st;
+    cfl[i] = c->ph.CFL;
+    for (int k = 0; k < 3; ++k) {
+      double* out = k == 0 ? c->qb[c->ls] : (k == 1 ? c->qb[c->lp] : c->qb[c->lq]);
+      bct[k * nb + i] = bc_args(c, out, true, k == 2 && !b->visc);
+      if (b->visc) vt[k * nb + i] = visc_args(c, true, k == 2);
+    }
+    bcc[i + 1] = bcc[i] + bc_farfield_ctas(c->d);
+    vc[i + 1] = vc[i] + (b->visc ? visc_ctas(c->d) : 0);
+  }
+  b->bc_total = bcc[nb];
+  b->visc_total = vc[nb];
+  CK(cudaMemcpyAsync(b->st_tab, sts.data(), nb * sizeof(StepState*), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->cfl_tab, cfl.data(), nb * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->bc_tab, bct.data(), bct.size() * sizeof(BCArgs), cudaMemcpyHostToDevice, b->stream));
+  if (b->visc)
+    CK(cudaMemcpyAsync(b->visc_tab, vt.data(), vt.size() * sizeof(ViscArgs), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->bc_cta, bcc.data(), bcc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->visc_cta, vc.data(), vc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaStreamSynchronize(b->stream));
   return CBNS_OK;
 }
@@ -587,11 +665,12 @@ struct SideStreams {
 
 int batch_enqueue_body(cbns_batch* b) {
   const int nb = (int)b->blk.size();
+  // every block's prologue (own dt) in one launch
+  CK(launch_step_prologue_batched(b->st_tab, b->cfl_tab, nb, b->stream));
+  b->blk[0]->launches += 1;
   RET(batch_fork(b));
   for (int i = 0; i < nb; ++i) {
     cbns_ctx* c = b->blk[i];
-    CK(launch_step_prologue(c->st, c->ph.CFL, c->stream));
-    c->launches += 1;
     if (b->hyb) RET(sensor_launch(c, c->qb[c->lq], true));
   }
   for (int k = 0; k < 3; ++k) {
@@ -612,13 +691,29 @@ int batch_enqueue_body(cbns_batch* b) {
     bs.counter = b->counter;
     CK(launch_stage_batched(bs, k + 1, b->visc, b->fp32, b->hyb, b->stream));
     b->blk[0]->launches += 1;
+    if (b->farfield) {
+      // inviscid: all blocks' boundary spectral radii in stage 3 (a viscous
+      // far-field block's boundary primitives stand, see enqueue_step); then
+      // all blocks' viscous node fluxes
+      if (!b->visc && last) {
+        CK(launch_bc_farfield_batched(b->bc_tab + k * nb, b->bc_cta, nb, b->bc_total, b->stream));
+        b->blk[0]->launches += 1;
+      }
+      if (b->visc) {
+        CK(launch_visc_batched(b->visc_tab + k * nb, b->visc_cta, nb, b->visc_total, b->stream));
+        b->blk[0]->launches += 1;
+      }
+      if (!last) RET(batch_fork(b));
+      continue;
+    }
     RET(batch_fork(b));
     for (cbns_ctx* c : b->blk) {
       double* out = k == 0 ? c->qb[c->ls] : (k == 1 ? c->qb[c->lp] : c->qb[c->lq]);
-      RET(bc_launch(c, bc_args(c, out, true, last && !b->visc), false));
+      if (!bc_fusable(c)) RET(bc_launch(c, bc_args(c, out, true, last && !b->visc), false));
       if (b->visc) RET(visc_launch(c, visc_args(c, true, last)));
     }
   }
+  if (b->farfield) return CBNS_OK;  // the side streams were joined before the last stage
   RET(batch_join(b));
   return CBNS_OK;
 }
@@ -677,6 +772,7 @@ int batch_run(cbns_batch* b, unsigned nsteps, double t_end, bool wait, unsigned*
   for (cbns_ctx* c : b->blk) {
     StepState h;
     CK(cudaMemcpy(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost));
+    RET(stage_status(h));
     mn = std::min(mn, h.steps);
     if (h.nan_dt) {
       nan = true;
@@ -759,14 +855,21 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   int rc = CBNS_OK;
   for (int b = 0; b < 3 && rc == CBNS_OK; ++b) rc = dalloc(c, &c->qb[b], (size_t)NEQ * d.VOL);
   for (int m = 0; m < 10 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.met[m], d.VOL);
-  for (int m = 0; m < 10 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.area[m], d.VOL);
+  {
+    // one allocation, components VOL elements apart (one 4-D tensor map covers them)
+    double* tmp = nullptr;
+    rc = rc == CBNS_OK ? dalloc(c, &tmp, (size_t)10 * d.VOL) : rc;
+    if (rc == CBNS_OK)
+      for (int m = 0; m < 10; ++m) c->f.area[m] = tmp + (size_t)m * d.VOL;
+  }
   for (int m = 0; m < 6; ++m) c->f.area32[m] = nullptr;
-  if (p->precision != CBNS_PREC_FP64)
-    for (int m = 0; m < 6 && rc == CBNS_OK; ++m) {
-      double* tmp = nullptr;
-      rc = dalloc(c, &tmp, (size_t)(d.VOL + 1) / 2);
-      c->f.area32[m] = reinterpret_cast<float*>(tmp);
-    }
+  if (p->precision != CBNS_PREC_FP64) {
+    // one allocation, components VOL floats apart (one 4-D tensor map covers them)
+    double* tmp = nullptr;
+    rc = rc == CBNS_OK ? dalloc(c, &tmp, (size_t)3 * d.VOL) : rc;
+    if (rc == CBNS_OK)
+      for (int m = 0; m < 6; ++m) c->f.area32[m] = reinterpret_cast<float*>(tmp) + (size_t)m * d.VOL;
+  }
   for (int m = 0; m < 7 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.prim[m], d.VOL);
   for (int m = 0; m < 12; ++m) c->f.vflux[m] = nullptr;
   if (p->viscous)
@@ -818,6 +921,30 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
     return rc;
   }
   c->stream = c->own;
+  {
+    // the stage kernels' TMA boxes (stage.cu), per state buffer
+    bool ok = true;
+    const bool fp32 = p->precision != CBNS_PREC_FP64;
+    for (int b = 0; b < 3; ++b) {
+      StageMaps& m = c->tm[b];
+      if (fp32) {  // halo boxes of the state, FP32 area vectors
+        ok = ok && encode_node_map(&m.q_a, c->qb[b], 8, d.PX, d.JG, d.KG, d.VOL, NEQ, 4, 15, NEQ);
+        ok = ok && encode_node_map(&m.q_b, c->qb[b], 8, d.PX, d.JG, d.KG, d.VOL, NEQ, 16, 3, NEQ);
+        ok = ok && encode_node_map(&m.xi, c->f.area32[0], 4, d.PX, d.JG, d.KG, d.VOL, 6, 24, 15, 3);
+        ok = ok && encode_node_map(&m.eta, c->f.area32[0], 4, d.PX, d.JG, d.KG, d.VOL, 6, 16, 17, 3);
+      } else {  // ring column and plane boxes of the state, FP64 area vectors
+        ok = ok && encode_node_map(&m.q_a, c->qb[b], 8, d.PX, d.JG, d.KG, d.VOL, NEQ, 16, 15, NEQ);
+        ok = ok && encode_node_map(&m.q_b, c->qb[b], 8, d.PX, d.JG, d.KG, d.VOL, NEQ, 24, 21, NEQ);
+        ok = ok && encode_node_map(&m.xi, c->f.area[0], 8, d.PX, d.JG, d.KG, d.VOL, 10, 24, 15, 3);
+        ok = ok && encode_node_map(&m.eta, c->f.area[0], 8, d.PX, d.JG, d.KG, d.VOL, 10, 16, 17, 3);
+      }
+    }
+    if (!ok) {
+      g_last = "cuTensorMapEncodeTiled refused the stage kernel's tensor maps";
+      cbns_destroy(c);
+      return CBNS_ERR_CUDA;
+    }
+  }
   // zero everything once so padding never holds NaN garbage
   for (void* a : c->allocs) (void)a;
   for (int b = 0; b < 3; ++b) cudaMemsetAsync(c->qb[b], 0, (size_t)NEQ * d.VOL * sizeof(double), c->stream);
@@ -913,7 +1040,7 @@ int cbns_initial_condition(cbns_ctx* c) {
   CK(launch_ic(c->d, c->f.prim, c->ph.angle_attack, c->ph.p_inf, c->ph.viscous, c->stream));
   c->launches += 1;
   c->prims_of = -1;
-  return sync(c);
+  return CBNS_OK;  // stream-ordered: the host-reading calls wait
 }
 
 int cbns_calc_conservative(cbns_ctx* c, int which) {
@@ -926,7 +1053,7 @@ int cbns_calc_conservative(cbns_ctx* c, int which) {
   c->percall_hold = 0;  // a new state: the next per-call step evaluates the network
   c->percall_restart = true;
   c->prims_of = -1;
-  return sync(c);
+  return CBNS_OK;  // stream-ordered: the host-reading calls wait
 }
 
 int cbns_set_conservative(cbns_ctx* c, const double* Q) {
@@ -997,7 +1124,7 @@ int cbns_calc_primitive(cbns_ctx* c, int which) {
   CK(launch_primitive(c->d, buf(c, which), c->f.prim, c->ph.gam1, c->ph.gM2, c->stream));
   c->launches += 1;
   c->prims_of = phys(c, which);
-  return sync(c);
+  return CBNS_OK;  // stream-ordered: the host-reading calls wait
 }
 
 int cbns_set_bc_calc_primitive(cbns_ctx* c, int which) {
@@ -1011,7 +1138,7 @@ int cbns_set_bc_calc_primitive(cbns_ctx* c, int which) {
   if (c->ph.viscous) c->prims_of = pb;
   c->sigma_valid = sigma;
   c->sigma_pending = false;
-  return sync(c);
+  return CBNS_OK;  // stream-ordered: the host-reading calls wait
 }
 
 int cbns_calc_numerical_flux(cbns_ctx* c, int which) {
@@ -1032,7 +1159,7 @@ int cbns_calc_viscous_terms(cbns_ctx* c) {
   RET(check_ready(c));
   if (!c->ph.viscous) return CBNS_OK;  // the inviscid build compiles this to nothing
   RET(visc_launch(c, visc_args(c, false, false)));
-  return sync(c);
+  return CBNS_OK;  // stream-ordered: the host-reading calls wait
 }
 
 int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
@@ -1072,18 +1199,19 @@ int cbns_update_rk3(cbns_ctx* c, double dt, unsigned stage) {
   if (c->ph.viscous) c->prims_of = out;
   c->sigma_valid = false;
   c->sigma_pending = sigma;
-  return sync(c);
+  return CBNS_OK;  // stream-ordered: the host-reading calls wait
 }
 
 int cbns_calc_dt(cbns_ctx* c, double* dt) {
   RET(check_ready(c));
   if (!dt) return CBNS_ERR_ARG;
   if (!c->sigma_valid) RET(sigma_launch(c));
-  unsigned long long bits = 0;
-  CK(cudaMemcpyAsync(&bits, &c->st->sigma_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+  StepState h;
+  CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   RET(sync(c));
+  RET(stage_status(h));
   double smax;
-  std::memcpy(&smax, &bits, sizeof(smax));
+  std::memcpy(&smax, &h.sigma_bits, sizeof(smax));
   *dt = c->ph.CFL / smax;
   c->sigma_valid = true;
   if (std::isnan(*dt)) return CBNS_ERR_NAN_DT;
@@ -1145,6 +1273,7 @@ static int run_impl(cbns_ctx* c, unsigned nsteps, double t_end, bool wait, unsig
   CK(cudaMemcpyAsync(&h, c->st, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
   RET(sync(c));
   if (steps_done) *steps_done = h.steps;
+  RET(stage_status(h));
   if (h.nan_dt) {
     c->sigma_valid = false;
     return CBNS_ERR_NAN_DT;
@@ -1336,8 +1465,8 @@ int cbns_autotune(cbns_ctx* c, int* chosen) {
   int best = 0, best_kc = c->kchunk;
   float best_ms = 1e30f;
   for (int v = 0; v < nv; ++v) {
-    // variant v runs 2 + v CTAs per SM; each with its candidate k chunks
-    for (int kc : kchunk_candidates(c, 2 + v)) {
+    // FP32 variant v runs 2 + v CTAs per SM, the FP64 ones 2; each with its candidate k chunks
+    for (int kc : kchunk_candidates(c, fp32 ? 2 + v : 2)) {
       c->stage_variant = v;
       c->kchunk = kc;
       const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
@@ -1361,6 +1490,24 @@ int cbns_autotune(cbns_ctx* c, int* chosen) {
   c->kchunk = best_kc;
   drop_graph(c);
   if (chosen) *chosen = best;
+  return CBNS_OK;
+}
+
+int cbns_synchronize(cbns_ctx* c) {
+  if (!c) return CBNS_ERR_ARG;
+  return sync(c);
+}
+
+int cbns_stage_variant(cbns_ctx* c, int variant, int* count) {
+  if (!c) return CBNS_ERR_ARG;
+  const int nv = stage_variants(c->ph.precision != CBNS_PREC_FP64, hybrid(c));
+  if (count) *count = nv;
+  if (variant == -1) return CBNS_OK;
+  if (variant < 0 || variant >= nv) return CBNS_ERR_ARG;
+  if (variant != c->stage_variant) {
+    c->stage_variant = variant;
+    drop_graph(c);
+  }
   return CBNS_OK;
 }
 
@@ -1467,8 +1614,27 @@ int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, c
       return rc;
     }
   }
+  b->farfield = true;
+  for (cbns_ctx* c : b->blk) b->farfield = b->farfield && c->prm.bc_mode == CBNS_BC_FARFIELD;
   e = cudaMalloc(&b->args, 3 * nblocks * sizeof(StageArgs));
   if (e == cudaSuccess) e = cudaMalloc(&b->start, (nblocks + 1) * sizeof(int));
+  if (e == cudaSuccess) {
+    // tables of the batched per-block kernels, each on a 256-byte boundary
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t o1 = up(nblocks * sizeof(StepState*)), o2 = o1 + up(nblocks * sizeof(double)),
+                 o3 = o2 + up(3 * nblocks * sizeof(BCArgs)), o4 = o3 + up(3 * nblocks * sizeof(ViscArgs)),
+                 o5 = o4 + up((nblocks + 1) * sizeof(int)), o6 = o5 + up((nblocks + 1) * sizeof(int));
+    e = cudaMalloc(&b->tables, o6);
+    if (e == cudaSuccess) {
+      char* t = static_cast<char*>(b->tables);
+      b->st_tab = reinterpret_cast<StepState**>(t);
+      b->cfl_tab = reinterpret_cast<double*>(t + o1);
+      b->bc_tab = reinterpret_cast<BCArgs*>(t + o2);
+      b->visc_tab = reinterpret_cast<ViscArgs*>(t + o3);
+      b->bc_cta = reinterpret_cast<int*>(t + o4);
+      b->visc_cta = reinterpret_cast<int*>(t + o5);
+    }
+  }
   if (e == cudaSuccess) e = cudaMalloc(&b->counter, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
   for (unsigned i = 0; i < std::min(nblocks, 16u) && e == cudaSuccess; ++i) {
@@ -1484,6 +1650,7 @@ int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, c
     cudaFree(b->args);
     cudaFree(b->start);
     cudaFree(b->counter);
+    cudaFree(b->tables);
     batch_release_side(b);
     for (size_t i = 0; i < b->blk.size(); ++i) cbns_set_stream(b->blk[i], b->saved[i]);
     if (b->own_stream) cudaStreamDestroy(b->stream);
@@ -1504,6 +1671,7 @@ int cbns_batch_destroy(cbns_batch* b) {
   cudaFree(b->args);
   cudaFree(b->start);
   cudaFree(b->counter);
+  cudaFree(b->tables);
   batch_release_side(b);
   if (b->own_stream) cudaStreamDestroy(b->stream);
   delete b;

@@ -261,32 +261,78 @@ __global__ void bc_phase3(const BCArgs a) {
   if (!a.viscous && a.sigma) warp_sigma_max(a, sg, has);
 }
 
+// Nodes of the ghosted box outside the interior (i, j, k in 1 .. N-2): the
+// six k planes of the outer slabs, then per interior k the six outer j rows,
+// then per interior (j, k) the six outer i nodes (x fastest where it can be).
+__host__ __device__ inline long shell_nodes(const Dims& d) {
+  return 6L * d.IG * d.JG + (long)(d.KM - 2) * 6 * d.IG + (long)(d.KM - 2) * (d.JM - 2) * 6;
+}
+__device__ __forceinline__ void shell_node(const Dims& d, long e, int& i, int& j, int& k) {
+  const long A = 6L * d.IG * d.JG, B = (long)(d.KM - 2) * 6 * d.IG;
+  if (e < A) {
+    const int s = (int)(e / ((long)d.IG * d.JG));
+    const long r = e % ((long)d.IG * d.JG);
+    i = (int)(r % d.IG) - NG;
+    j = (int)(r / d.IG) - NG;
+    k = s < 3 ? s - NG : d.KM - 1 + (s - 3);
+  } else if (e < A + B) {
+    const long e2 = e - A;
+    k = 1 + (int)(e2 / (6L * d.IG));
+    const int r = (int)(e2 % (6L * d.IG));
+    const int s = r / d.IG;
+    i = r % d.IG - NG;
+    j = s < 3 ? s - NG : d.JM - 1 + (s - 3);
+  } else {
+    const long e3 = e - A - B;
+    const long kj = e3 / 6;
+    const int s = (int)(e3 % 6);
+    k = 1 + (int)(kj / (d.JM - 2));
+    j = 1 + (int)(kj % (d.JM - 2));
+    i = s < 3 ? s - NG : d.IM - 1 + (s - 3);
+  }
+}
+
 // CBNS_BC_FARFIELD: every node of the ghosted box outside the interior keeps
 // its Q; its primitives (viscous runs) follow from that Q, and in inviscid
 // runs the grid's boundary nodes add their spectral radii for the next dt.
-__global__ void bc_farfield(const BCArgs a) {
-  if (a.check_done && a.st->done) return;
+// e: the thread's shell node (shell_node); every lane of the warp calls this.
+__device__ __forceinline__ void farfield_body(const BCArgs& a, long e) {
   const Dims& d = a.d;
-  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double sg = 0.0;
   bool has = false;
-  if (e < (long)d.IG * d.JG * d.KG) {
-    const int i = (int)(e % d.IG) - NG;
-    const long r = e / d.IG;
-    const int j = (int)(r % d.JG) - NG, k = (int)(r / d.JG) - NG;
-    const bool interior = i >= 1 && i <= d.IM - 2 && j >= 1 && j <= d.JM - 2 && k >= 1 && k <= d.KM - 2;
-    if (!interior) {
-      const long o = node_off(d, i, j, k);
-      const PrimV s = prim_of(a.q, o, d.VOL, a.gam1);
-      if (a.viscous) {
-        put_prim(a, o, s);
-      } else if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && k >= 0 && k < d.KM) {
-        sg = sigma_inv(a, o, s);
-        has = true;
-      }
+  if (e < shell_nodes(d)) {
+    int i, j, k;
+    shell_node(d, e, i, j, k);
+    const long o = node_off(d, i, j, k);
+    const PrimV s = prim_of(a.q, o, d.VOL, a.gam1);
+    if (a.viscous) {
+      put_prim(a, o, s);
+    } else if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && k >= 0 && k < d.KM) {
+      sg = sigma_inv(a, o, s);
+      has = true;
     }
   }
   if (!a.viscous && a.sigma) warp_sigma_max(a, sg, has);
+}
+
+__global__ void bc_farfield(const BCArgs a) {
+  if (a.check_done && a.st->done) return;
+  farfield_body(a, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
+// The same for many blocks in one launch: block b owns CTAs cta[b] ..
+// cta[b+1]-1 (so a warp's spectral-radius maximum stays within one block);
+// args[b] are its BCArgs.
+__global__ void bc_farfield_batched(const BCArgs* args, const int* cta, int nblocks) {
+  int lo = 0, hi = nblocks - 1;  // the last b with cta[b] <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(cta + mid) <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const BCArgs& a = args[lo];
+  if (a.check_done && a.st->done) return;
+  farfield_body(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);
 }
 
 // CBNS_BC_CHARACTERISTIC, one face direction per launch (dir 0 = i, 1 = j,
@@ -393,6 +439,36 @@ __global__ void bc_wrap(const BCArgs a) {
   }
 }
 
+// Spectral radii of the j = 0 and j = JM-1 grid rows (every i in [0, IM), k in
+// [0, KM)) into st->sigma_fixed: in an inviscid reference-mode block without
+// wake cut or wall these nodes hold their state during a run, so their terms
+// of the boundary kernels' maximum (bc_phase3: j faces, and the k-face copies
+// of those rows) are fixed; the stage kernels that apply the other boundary
+// conditions themselves (fused_bc in stage.cu) leave them to this value.
+__global__ void bc_jrows_sigma(const BCArgs a) {
+  const Dims& d = a.d;
+  const long n = 2L * d.IM * d.KM;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  double sg = 0.0;
+  bool has = false;
+  if (e < n) {
+    const int side = e >= (long)d.IM * d.KM;
+    const long r = side ? e - (long)d.IM * d.KM : e;
+    const int i = (int)(r % d.IM), k = (int)(r / d.IM);
+    const long o = node_off(d, i, side ? d.JM - 1 : 0, k);
+    sg = sigma_inv(a, o, prim_of(a.q, o, d.VOL, a.gam1));
+    has = true;
+  }
+  const bool nan = has && (sg != sg);
+  double m = (has && !nan) ? sg : 0.0;
+  const unsigned anyhas = __ballot_sync(0xffffffffu, has);
+  const unsigned anynan = __ballot_sync(0xffffffffu, nan);
+#pragma unroll
+  for (int k = 16; k > 0; k >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, k));
+  if ((threadIdx.x & 31) == 0 && anyhas != 0u)
+    atomic_max_sigma(&a.st->sigma_fixed, anynan ? __longlong_as_double(0x7ff8000000000000ll) : m);
+}
+
 // Interior primitives (rho,u,v,w,p,T) from Q, the first part of
 // primitive_bc_kernel (:59-79); needed when the primitive arrays do not yet
 // describe the buffer the boundary conditions act on.
@@ -444,7 +520,7 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
       nl += 3;
     }
     if (a.viscous || a.sigma) {
-      bc_farfield<<<nblk((long)d.IG * d.JG * d.KG, B), B, 0, s>>>(a);
+      bc_farfield<<<nblk(shell_nodes(d), B), B, 0, s>>>(a);
       ++nl;
     }
     if (launches) *launches += nl;
@@ -462,6 +538,23 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
   bc_phase3<<<nblk(n3, B), B, 0, s>>>(a);
   ++nl;
   if (launches) *launches += nl;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bc_fixed_sigma(const BCArgs& a, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(&a.st->sigma_fixed, 0, sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  bc_jrows_sigma<<<nblk(2L * a.d.IM * a.d.KM, 128), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// CTAs of 128 threads the batched far-field kernel gives one block.
+int bc_farfield_ctas(const Dims& d) { return (int)nblk(shell_nodes(d), 128); }
+
+cudaError_t launch_bc_farfield_batched(const BCArgs* args, const int* cta, int nblocks, int total_ctas,
+                                       cudaStream_t s) {
+  if (total_ctas <= 0) return cudaSuccess;
+  bc_farfield_batched<<<total_ctas, 128, 0, s>>>(args, cta, nblocks);
   return cudaGetLastError();
 }
 

@@ -85,10 +85,14 @@ void get_metrics(const Block3dInfo*, const Block3dData* d, value_type* xi_x, val
   SHIM_CHECK(cbns_get_metrics(d->ctx, xi_x, xi_y, xi_z, eta_x, eta_y, eta_z, zeta_x, zeta_y, zeta_z, Jac));
 }
 
-void initial_condition(const Block3dInfo*, Block3dData* d) { SHIM_CHECK(cbns_initial_condition(d->ctx)); }
+void initial_condition(const Block3dInfo*, Block3dData* d) {
+  SHIM_CHECK(cbns_initial_condition(d->ctx));
+  SHIM_CHECK(cbns_synchronize(d->ctx));
+}
 
 void calc_conservative(const Block3dInfo*, Block3dData* d, value_type* Q) {
   SHIM_CHECK(cbns_calc_conservative(d->ctx, which_of(d, Q)));
+  SHIM_CHECK(cbns_synchronize(d->ctx));
 }
 
 void set_conservative(const Block3dInfo*, Block3dData* d, const value_type* Q) {
@@ -106,17 +110,22 @@ void get_primitive(const Block3dInfo*, const Block3dData* d, value_type* rho, va
 
 void calc_primitive(const Block3dInfo*, Block3dData* d, const value_type* Q) {
   SHIM_CHECK(cbns_calc_primitive(d->ctx, which_of(d, Q)));
+  SHIM_CHECK(cbns_synchronize(d->ctx));
 }
 
 void set_bc_calc_primitive(const Block3dInfo*, Block3dData* d, value_type* Q) {
   SHIM_CHECK(cbns_set_bc_calc_primitive(d->ctx, which_of(d, Q)));
+  SHIM_CHECK(cbns_synchronize(d->ctx));
 }
 
 void calc_numerical_flux(const Block3dInfo*, Block3dData* d, const value_type* Q) {
   SHIM_CHECK(cbns_calc_numerical_flux(d->ctx, which_of(d, Q)));
 }
 
-void calc_viscous_terms(const Block3dInfo*, Block3dData* d) { SHIM_CHECK(cbns_calc_viscous_terms(d->ctx)); }
+void calc_viscous_terms(const Block3dInfo*, Block3dData* d) {
+  SHIM_CHECK(cbns_calc_viscous_terms(d->ctx));
+  SHIM_CHECK(cbns_synchronize(d->ctx));
+}
 
 void calc_viscous_flux_contribution(const Block3dInfo*, Block3dData* d) {
   SHIM_CHECK(cbns_calc_viscous_flux_contribution(d->ctx));
@@ -124,6 +133,7 @@ void calc_viscous_flux_contribution(const Block3dInfo*, Block3dData* d) {
 
 void update_rk3(const Block3dInfo*, Block3dData* d, const value_type dt, const size_type stage) {
   SHIM_CHECK(cbns_update_rk3(d->ctx, dt, stage));
+  SHIM_CHECK(cbns_synchronize(d->ctx));
 }
 
 value_type calc_dt(const Block3dInfo*, Block3dData* d) {

@@ -25,6 +25,14 @@
 //            registers from the previous plane.
 // Every thread computes 3 faces per plane; face fluxes never leave the SM and
 // no global load sits inside a face evaluation.
+// Staging.  The FP32 kernels built for 2 or 3 CTAs per SM stage the next
+// plane's halo (raw FP64 state) and face-node area vectors (FP32 copies) by
+// TMA: one thread issues six 4-D box copies (tma.cuh) right after the current
+// plane's staging barrier, completing on an mbarrier per plane parity, so they
+// travel while the current plane's three flux rounds run; the ring column goes
+// through registers (fetched a plane early, rounded to FP32 on the way into
+// shared memory).  The FP64 kernel and the 4-CTA hybrid variant, which have no
+// shared memory to spare for a second plane, stage synchronously.
 // HBM traffic per node and stage: the stage input (40 B, halos from L2),
 // area vectors and 1/J (80 B; the FP32 kernels stage FP32 copies of the xi
 // and eta vectors, 56 B), the RK base (0-40 B) and the output (40 B).
@@ -41,6 +49,7 @@
 #include "cbns_common.cuh"
 #include "face_flux.cuh"
 #include "stage.cuh"
+#include "tma.cuh"
 
 namespace cbns {
 
@@ -63,56 +72,159 @@ constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;  // halo nodes of a plane: i-h
 template <typename R>
 using AreaT = typename std::conditional<sizeof(R) == 4, float, double>::type;
 
-// The FP32 kernels built for 2 or 3 CTAs per SM stage the next plane's halo
-// (raw FP64) and face-node area vectors with asynchronous copies while the
-// current plane is computed: the second area-vector buffer and the halo buffer.
-struct AsyncSmem {
-  float sx[3][TJ][TI + 2];
-  float sy[3][TJ + 2][TI];
-  double halo[NEQ][NHI + NHJ];
-};
-
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(smem)), "l"(gmem)
-               : "memory");
-}
 __device__ __forceinline__ void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
 __device__ __forceinline__ void prefetch_l2(const void* p) {
   asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-template <typename S, typename R>
+// PWT: row pitch of the plane buffer (PW; 24 in the FP64 TMA kernel, whose
+// plane is one TMA box starting at tile x = -4)
+template <typename S, typename R, int PWT = PW>
 struct Smem {
   S ring[6][NEQ][NC];
-  S plane[NEQ][PH][PW];
-  AreaT<R> sx[3][TJ][TI + 2];  // J*grad(xi) at node (i0-1+c, j0+r)
-  AreaT<R> sy[3][TJ + 2][TI];  // J*grad(eta) at node (i0+c, j0-1+r)
+  S plane[NEQ][PH][PWT];
   R fi[NEQ][TJ][TI + 1];
   R fj[NEQ][TJ + 1][TI];
 };
 
-template <typename R, int NB>
-__host__ __device__ constexpr bool async_staging() {
-  return sizeof(R) == 4 && NB <= 3;
-}
+// Face-node area vectors of one plane, staged by the synchronous kernels.
+template <typename R>
+struct AreaSync {
+  AreaT<R> sx[3][TJ][TI + 2];  // J*grad(xi) at node (i0-1+c, j0+r)
+  AreaT<R> sy[3][TJ + 2][TI];  // J*grad(eta) at node (i0+c, j0-1+r)
+};
 
-template <typename R, int NB>
+// TMA staging of the FP32 kernels, each box as the copy writes it (x fastest,
+// then rows, then fields): plane k+1's halo (raw FP64; one buffer, refilled
+// after plane k's halo was converted) and the face-node area vectors of planes
+// k and k+1 (two buffers).  Box x origins sit on 16-byte boundaries: the i-side
+// halo boxes start at i0-4 and i0+16, the xi box at i0-4 (node i0-1+c at
+// column c+3), the j-side and eta boxes at i0.
+struct TmaSmem {
+  alignas(128) double hl[NEQ][TJ][4];  // x = i0-4 .. i0-1, rows j0 .. j0+14
+  alignas(128) double hr[NEQ][TJ][4];  // x = i0+16 .. i0+19
+  alignas(128) double hb[NEQ][H][TI];  // x = i0 .. i0+15, rows j0-3 .. j0-1
+  alignas(128) double ht[NEQ][H][TI];  // rows j0+15 .. j0+17
+  struct Area {
+    alignas(128) float xi[3][TJ][24];      // J*grad(xi), x = i0-4 .. i0+19, rows j0 .. j0+14
+    alignas(128) float eta[3][TJ + 2][TI];  // J*grad(eta), x = i0 .. i0+15, rows j0-1 .. j0+15
+  } area[2];
+  alignas(8) unsigned long long bar[2];  // one per plane parity
+};
+// bytes of one plane's six boxes (the mbarrier's transaction count)
+constexpr unsigned kTmaBytes =
+    (unsigned)(sizeof(double) * NEQ * (2 * TJ * 4 + 2 * H * TI) + sizeof(float) * 3 * (TJ * 24 + (TJ + 2) * TI));
+
+// TMA staging of the FP64 kernel: the ring column of a plane lands in its ring
+// slot (box 16 x 15 x 1 x 5, the slot's [field][row][col] layout), the whole
+// plane with its halo in the plane buffer (box 24 x 21 x 1 x 5 from tile x =
+// -4, row pitch 24), the face-node area vectors (FP64) here; all single
+// buffers, refilled for the next plane once the current plane's flux rounds
+// are over, so the copies travel during the RK update.
+struct TmaSmem64 {
+  alignas(128) double xi[3][TJ][24];      // J*grad(xi), x = i0-4 .. i0+19, rows j0 .. j0+14
+  alignas(128) double eta[3][TJ + 2][TI];  // J*grad(eta), x = i0 .. i0+15, rows j0-1 .. j0+15
+  alignas(8) unsigned long long bar[2];
+};
+// bytes of the warm-up set (the ring's first six planes) and of a plane's set
+// (its ring column three planes ahead, the plane with halo, the area vectors)
+constexpr unsigned kTma64Warm = (unsigned)(6 * sizeof(double) * NEQ * NC);
+constexpr unsigned kTma64Plane =
+    (unsigned)(sizeof(double) * (NEQ * NC + NEQ * PH * 24 + 3 * TJ * 24 + 3 * (TJ + 2) * TI));
+
+constexpr size_t round_to(size_t x, size_t m) { return (x + m - 1) / m * m; }
+
+// dynamic shared memory: Smem, then (FP32 TMA kernels) TmaSmem on a 128-byte
+// boundary found at run time, (the FP64 TMA kernel) Smem and TmaSmem64 from a
+// 128-byte boundary, or (synchronous kernels) AreaSync
+template <typename R, int NB, bool TMA>
 __host__ __device__ constexpr size_t stage_smem() {
-  return (sizeof(Smem<R, R>) + 15) / 16 * 16 + (async_staging<R, NB>() ? sizeof(AsyncSmem) : 0);
+  return (TMA && sizeof(R) == 4)   ? round_to(sizeof(Smem<R, R>), 16) + 128 + sizeof(TmaSmem)
+         : (TMA && sizeof(R) == 8) ? 128 + round_to(sizeof(Smem<R, R, 24>), 128) + sizeof(TmaSmem64)
+                                   : round_to(sizeof(Smem<R, R>), 16) + sizeof(AreaSync<R>);
 }
 
 // 4th-order central derivative of a node field along a stride, at offset o.
 __device__ __forceinline__ double d4(const double* f, long o, long s) {
   return (1.0 / 12.0) * __ldg(f + o - 2 * s) - (2.0 / 3.0) * __ldg(f + o - s) + (2.0 / 3.0) * __ldg(f + o + s) -
          (1.0 / 12.0) * __ldg(f + o + 2 * s);
+}
+
+// Spectral-radius sum of time_step_kernel (inviscid form) at node offset o
+// from the conservative state v, with the node's metrics; the arithmetic of
+// the boundary kernels' (bc.cu) so the fused boundary gives the same dt.
+__device__ __forceinline__ double sigma_node(const StageArgs& a, long o, const double v[NEQ]) {
+  const double r = v[0], u = v[1] / r, w = v[2] / r, x = v[3] / r;
+  const double p = a.gam1 * (v[4] - 0.5 * r * (u * u + w * w + x * x));
+  const double c = sqrt(a.gamma * p / r);
+  double sum = 0.0;
+#pragma unroll
+  for (int dd = 0; dd < 3; ++dd) {
+    const double mx = a.met[3 * dd][o], my = a.met[3 * dd + 1][o], mz = a.met[3 * dd + 2][o];
+    sum += fabs(u * mx + w * my + x * mz) + c * sqrt(mx * mx + my * my + mz * mz);
+  }
+  return sum;
+}
+
+// The reference's boundary conditions of an inviscid block without wake cut
+// or wall, applied to the stage output by the thread that formed the new
+// state q of interior node (ci, cj, k) (StageArgs.fuse_bc):
+//   i faces (primitive_bc_kernel.cu:84-186): at ci = 1 the nodes i = 0, -1, -2
+//     take q's density and momentum with the energy that resets the pressure
+//     to p_inf, at ci = IM-2 the nodes IM-1 .. IM+1 likewise;
+//   k faces (:417-492): at k = 1 the nodes k = 0, -1, -2 of every (i, j) in
+//     [0, IM) x [0, JM) copy k = 1 -- here the column's own node and, beside
+//     an i face, the face node i = 0 (IM-1) -- and at k = KM-2 likewise.
+// The j faces hold their state (no wake, no wall, no rewrite of Q), so their
+// k-face copies are already in place; their spectral radii are fixed for the
+// run (StepState.sigma_fixed).  With a.sigma (stage 3) the i- and k-face
+// grid nodes add their spectral radii as bc_phase3 does.
+__device__ __forceinline__ void fused_bc(const StageArgs& a, int ci, int cj, int k, const double q[NEQ],
+                                         double& smax, bool& snan) {
+  const Dims& d = a.d;
+  const bool lo_i = ci == 1, hi_i = ci == d.IM - 2, lo_k = k == 1, hi_k = k == d.KM - 2;
+  if (!(lo_i || hi_i || lo_k || hi_k)) return;
+  const long VOL = d.VOL;
+  double b[NEQ];
+#pragma unroll
+  for (int n = 0; n < 4; ++n) b[n] = q[n];
+  b[4] = a.p_inf / a.gam1 + 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) / q[0];
+  auto put = [&](int i, int kk, const double* v) {
+    const long o = node_off(d, i, cj, kk);
+#pragma unroll
+    for (int n = 0; n < NEQ; ++n) a.out[n * VOL + o] = v[n];
+  };
+  auto sig = [&](int i, int kk, const double* v) {
+    if (a.sigma) {
+      const double x = sigma_node(a, node_off(d, i, cj, kk), v);
+      if (x != x) snan = true;
+      smax = fmax(smax, x);
+    }
+  };
+  if (lo_i) {
+    for (int l = 0; l <= NG; ++l) put(-l, k, b);
+    sig(0, k, b);
+  }
+  if (hi_i) {
+    for (int l = 0; l <= NG; ++l) put(d.IM - 1 + l, k, b);
+    sig(d.IM - 1, k, b);
+  }
+  for (int side = 0; side < 2; ++side) {
+    if (side == 0 ? !lo_k : !hi_k) continue;
+    const int base = side ? d.KM - 1 : 0, dir = side ? 1 : -1;
+    for (int l = 0; l <= NG; ++l) put(ci, base + dir * l, q);
+    sig(ci, base, q);
+    if (lo_i) {
+      for (int l = 0; l <= NG; ++l) put(0, base + dir * l, b);
+      sig(0, base, b);
+    }
+    if (hi_i) {
+      for (int l = 0; l <= NG; ++l) put(d.IM - 1, base + dir * l, b);
+      sig(d.IM - 1, base, b);
+    }
+  }
 }
 
 // NB = CTAs per SM the register budget is cut for: FP64 always 2 (shared
@@ -122,10 +234,25 @@ __device__ __forceinline__ double d4(const double* f, long o, long s) {
 // HYB: hybrid flux (learned-sensor decision per face, see the flux lambda);
 // it evaluates only the linear faces and holds no WENO5 code.
 // The work of one CTA: tile `tile` of the block's (i, j) tiling, k chunk `kc`.
-template <typename R, bool VISC, int MODE, int NB, bool HYB>
-__device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc, unsigned char* smem_raw) {
+// TMA: TMA staging (FP32: halo and area vectors; FP64: ring column, plane and
+// area vectors), else synchronous loads.
+template <typename R, bool VISC, int MODE, int NB, bool HYB, bool TMA>
+__device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* tm, int tile, int kc,
+                                           unsigned char* smem_raw) {
   using S = R;  // shared-memory storage type
-  Smem<S, R>& sm = *reinterpret_cast<Smem<S, R>*>(smem_raw);
+  constexpr bool kTma = TMA && sizeof(R) == 4;
+  constexpr bool kTma64 = TMA && sizeof(R) == 8;
+  constexpr int PWT = kTma64 ? 24 : PW;  // plane row pitch
+  constexpr int X0 = kTma64 ? 1 : 0;     // plane column of tile x = -H, minus H
+  using SM = Smem<S, R, PWT>;
+  unsigned char* base =
+      kTma64 ? reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127))
+             : smem_raw;
+  SM& sm = *reinterpret_cast<SM*>(base);
+  unsigned char* tail = base + round_to(sizeof(SM), kTma64 ? 128 : 16);
+  TmaSmem* ts = reinterpret_cast<TmaSmem*>((reinterpret_cast<uintptr_t>(tail) + 127) & ~uintptr_t(127));
+  TmaSmem64* t64 = reinterpret_cast<TmaSmem64*>(tail);
+  AreaSync<R>* asy = reinterpret_cast<AreaSync<R>*>(tail);
 
   const StepState* st = a.st;
   if (MODE != 0 && st->done) return;
@@ -226,8 +353,6 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     }
   };
 
-  constexpr bool kAsync = async_staging<R, NB>();
-  AsyncSmem* as = reinterpret_cast<AsyncSmem*>(smem_raw + (sizeof(Smem<S, R>) + 15) / 16 * 16);
   // halo node e of a plane: tile-relative (x, y)
   auto halo_xy = [&](int e, int& x, int& y) {
     if (e < NHI) {
@@ -241,50 +366,66 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
       y = r6 < H ? r6 - H : TJ + (r6 - H);
     }
   };
-  // asynchronous copies of plane kp's halo and face-node area vectors (buffer
-  // kp & 1: 0 = Smem, 1 = AsyncSmem)
+  // TMA copies of plane kp's halo and face-node area vectors (area buffer
+  // kp & 1), issued by thread 0 after a CTA barrier that ended every read of
+  // the buffers they overwrite
   auto issue_plane = [&](int kp) {
-    if constexpr (kAsync) {
-      for (int e = t; e < NHI + NHJ; e += NT) {
-        int x, y;
-        halo_xy(e, x, y);
-        const int gi = ti0 + x, gj = tj0 + y;
-        if (gi <= d.IM + 1 && gj <= d.JM + 1) {
-          const long o = node_off(d, gi, gj, kp);
-#pragma unroll
-          for (int n = 0; n < NEQ; ++n) cp_async8(&as->halo[n][e], a.src + n * VOL + o);
-        }
+    if constexpr (kTma) {
+      if (t == 0) {
+        unsigned long long* bar = &ts->bar[kp & 1];
+        tma::fence_proxy();
+        tma::bar_expect(bar, kTmaBytes);
+        const int z = kp + NG, y0 = tj0 + NG;
+        const int xl = (int)LP + NG + ti0 - 4, xc = (int)LP + NG + ti0, xr = (int)LP + NG + ti0 + TI;
+        tma::load_4d(ts->hl, &tm->q_a, xl, y0, z, 0, bar);
+        tma::load_4d(ts->hr, &tm->q_a, xr, y0, z, 0, bar);
+        tma::load_4d(ts->hb, &tm->q_b, xc, y0 - H, z, 0, bar);
+        tma::load_4d(ts->ht, &tm->q_b, xc, y0 + TJ, z, 0, bar);
+        tma::load_4d(ts->area[kp & 1].xi, &tm->xi, xl, y0, z, 0, bar);
+        tma::load_4d(ts->area[kp & 1].eta, &tm->eta, xc, y0 - 1, z, 3, bar);
       }
-      AreaT<R>(*SX)[TJ][TI + 2] = (kp & 1) ? as->sx : sm.sx;
-      AreaT<R>(*SY)[TJ + 2][TI] = (kp & 1) ? as->sy : sm.sy;
-      for (int e = t; e < NSX + NSY; e += NT) {
-        if (e < NSX) {
-          const int c = e % (TI + 2), r = e / (TI + 2);
-          const int gi = ti0 - 1 + c, gj = tj0 + r;
-          if (gi <= d.IM + 1 && gj <= d.JM + 1) {
-            const long o = node_off(d, gi, gj, kp);
-#pragma unroll
-            for (int m = 0; m < 3; ++m) cp_async4(&SX[m][r][c], a.area32[m] + o);
-          }
-        } else {
-          const int e2 = e - NSX;
-          const int c = e2 % TI, r = e2 / TI;
-          const int gi = ti0 + c, gj = tj0 - 1 + r;
-          if (gi <= d.IM + 1 && gj <= d.JM + 1) {
-            const long o = node_off(d, gi, gj, kp);
-#pragma unroll
-            for (int m = 0; m < 3; ++m) cp_async4(&SY[m][r][c], a.area32[3 + m] + o);
-          }
-        }
-      }
-      cp_async_commit();
     }
   };
 
+  // FP64 TMA kernel: the copies of plane kp's set -- its ring column three
+  // planes ahead (kp+3), the plane with its halo, the area vectors -- on
+  // barrier q & 1 (q = kp - kb + 1; the warm-up set is q = 0)
+  auto issue_set64 = [&](int kp) {
+    if constexpr (kTma64) {
+      if (t == 0) {
+        unsigned long long* bar = &t64->bar[(kp - kb + 1) & 1];
+        tma::fence_proxy();
+        tma::bar_expect(bar, kTma64Plane);
+        const int z = kp + NG, y0 = tj0 + NG;
+        const int xl = (int)LP + NG + ti0 - 4, xc = (int)LP + NG + ti0;
+        tma::load_4d(&sm.ring[(kp + 3) % 6][0][0], &tm->q_a, xc, y0, kp + 3 + NG, 0, bar);
+        tma::load_4d(&sm.plane[0][0][0], &tm->q_b, xl, y0 - H, z, 0, bar);
+        tma::load_4d(&t64->xi[0][0][0], &tm->xi, xl, y0, z, 0, bar);
+        tma::load_4d(&t64->eta[0][0][0], &tm->eta, xc, y0 - 1, z, 3, bar);
+      }
+    }
+  };
+
+  if constexpr (kTma || kTma64) {
+    if (t == 0) {
+      tma::bar_init(kTma ? &ts->bar[0] : &t64->bar[0]);
+      tma::bar_init(kTma ? &ts->bar[1] : &t64->bar[1]);
+      tma::fence_init();
+    }
+  }
   // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
-  for (int kp = kb - 3; kp <= kb + 2; ++kp) load_ring(kp);
+  bool landed = true;
+  if constexpr (kTma64) {
+    if (t == 0) {
+      tma::bar_expect(&t64->bar[0], kTma64Warm);
+      for (int kp = kb - 3; kp <= kb + 2; ++kp)
+        tma::load_4d(&sm.ring[(kp + 6) % 6][0][0], &tm->q_a, (int)LP + NG + ti0, tj0 + NG, kp + NG, 0, &t64->bar[0]);
+    }
+  } else {
+    for (int kp = kb - 3; kp <= kb + 2; ++kp) load_ring(kp);
+  }
   if (kPrefetch) fetch_ring(kb + 3);
-  if (kAsync) issue_plane(kb);
+  if (kTma) issue_plane(kb);
   // the column's J*grad(zeta) at planes k and k+1, in FP64 (the stage-3
   // spectral radius uses it exactly)
   double za[3] = {0, 0, 0}, zb[3] = {0, 0, 0};
@@ -292,11 +433,22 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     load_zeta(kb - 1, za);
     load_zeta(kb, zb);
   }
-  __syncthreads();
+  if constexpr (kTma64) landed = tma::bar_wait(&t64->bar[0], 0);
+  if (__syncthreads_or(!landed)) {
+    if (t == 0) {
+      atomicExch(&a.st->stage_fail, 1);
+      tma::bar_wait(&t64->bar[0], 0);  // bounded: the copies in flight
+    }
+    return;
+  }
   R fkm[5] = {0, 0, 0, 0, 0};
   if (col_valid) k_face(kb - 1, za, zb, -1, fkm);
 #pragma unroll
   for (int m = 0; m < 3; ++m) za[m] = zb[m];
+  if constexpr (kTma64) {
+    __syncthreads();  // the warm-up face has read the slot plane kb+3 lands in
+    issue_set64(kb);
+  }
 
   double smax = 0.0;  // running spectral-radius max (stage 3, inviscid)
   bool snan = false;
@@ -361,25 +513,36 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
         if (MODE >= 2) prefetch_l2(a.qp + n * VOL + o);
       }
     }
-    if (kAsync) cp_async_wait_all();     // plane k's halo and area vectors have landed
-    __syncthreads();
-    // plane k's face-node area vectors
-    AreaT<R>(*SXk)[TJ][TI + 2] = sm.sx;
-    AreaT<R>(*SYk)[TJ + 2][TI] = sm.sy;
-    if constexpr (kAsync) {
-      if (k & 1) {
-        SXk = as->sx;
-        SYk = as->sy;
-      }
+    // plane k's halo and area vectors (FP32 TMA kernels), plane k's set (FP64
+    // TMA kernel) have landed; a wait that runs out on any thread ends the
+    // CTA's work, recorded in st->stage_fail
+    unsigned long long* wbar = nullptr;
+    unsigned wpar = 0;
+    if constexpr (kTma) {
+      wbar = &ts->bar[k & 1];
+      wpar = ((k - kb) >> 1) & 1;
+    } else if constexpr (kTma64) {
+      wbar = &t64->bar[(k - kb + 1) & 1];
+      wpar = ((k - kb + 1) >> 1) & 1;
     }
-    if (kPrefetch) {
+    if constexpr (kTma || kTma64) landed = tma::bar_wait(wbar, wpar);
+    if (__syncthreads_or(!landed)) {
+      if (t == 0) {
+        atomicExch(&a.st->stage_fail, 1);
+        tma::bar_wait(wbar, wpar);  // bounded: the copies in flight
+      }
+      return;
+    }
+    if constexpr (kTma64) {
+      // ring column, plane and area vectors are in place
+    } else if (kPrefetch) {
       store_ring(k + 3);
       if (k + 1 < ke) fetch_ring(k + 4);
     } else {
       load_ring(k + 3);
     }
     // plane k with halo: interior from the ring, halo from global memory
-    {
+    if constexpr (!kTma64) {
       const int sk = k % 6;
       for (int e = t; e < NC; e += NT) {
         const int x = e % TI, y = e / TI;
@@ -392,9 +555,12 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
         halo_xy(e, x, y);
         const int gi = ti0 + x, gj = tj0 + y;
         if (gi <= d.IM + 1 && gj <= d.JM + 1) {
-          if (kAsync) {
+          if (kTma) {
 #pragma unroll
-            for (int n = 0; n < NEQ; ++n) sm.plane[n][y + H][x + H] = (S)as->halo[n][e];
+            for (int n = 0; n < NEQ; ++n)
+              sm.plane[n][y + H][x + H] = (S)(x < 0 ? ts->hl[n][y][x + 4]
+                                                     : x >= TI ? ts->hr[n][y][x - TI]
+                                                               : y < 0 ? ts->hb[n][y + H][x] : ts->ht[n][y - TJ][x]);
           } else {
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
@@ -403,7 +569,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
         }
       }
       // area vectors of the face nodes of plane k (synchronous kernels)
-      for (int e = t; !kAsync && e < NSX + NSY; e += NT) {
+      for (int e = t; !kTma && e < NSX + NSY; e += NT) {
         if (e < NSX) {
           const int c = e % (TI + 2), r = e / (TI + 2);
           const int gi = ti0 - 1 + c, gj = tj0 + r;
@@ -411,8 +577,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
-              if constexpr (sizeof(R) == 4) SXk[m][r][c] = __ldg(a.area32[m] + o);
-              else SXk[m][r][c] = __ldg(a.area[m] + o);
+              if constexpr (sizeof(R) == 4) asy->sx[m][r][c] = __ldg(a.area32[m] + o);
+              else asy->sx[m][r][c] = __ldg(a.area[m] + o);
             }
           }
         } else {
@@ -423,17 +589,28 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
             const long o = node_off(d, gi, gj, k);
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
-              if constexpr (sizeof(R) == 4) SYk[m][r][c] = __ldg(a.area32[3 + m] + o);
-              else SYk[m][r][c] = __ldg(a.area[3 + m] + o);
+              if constexpr (sizeof(R) == 4) asy->sy[m][r][c] = __ldg(a.area32[3 + m] + o);
+              else asy->sy[m][r][c] = __ldg(a.area[3 + m] + o);
             }
           }
         }
       }
     }
-    __syncthreads();
+    if constexpr (!kTma64) __syncthreads();
     // plane k+1's halo and area vectors travel while plane k is computed (the
     // buffers they overwrite were last read by plane k-1 and by the staging)
-    if (kAsync && k + 1 < ke) issue_plane(k + 1);
+    if (kTma && k + 1 < ke) issue_plane(k + 1);
+    // the area vectors of plane k's face nodes: node (i0-1+c, j0+r) and (i0+c, j0-1+r)
+    auto ax = [&](int m, int r, int c) -> R {
+      if constexpr (kTma) return (R)ts->area[k & 1].xi[m][r][c + 3];
+      else if constexpr (kTma64) return (R)t64->xi[m][r][c + 3];
+      else return (R)asy->sx[m][r][c];
+    };
+    auto ay = [&](int m, int r, int c) -> R {
+      if constexpr (kTma) return (R)ts->area[k & 1].eta[m][r][c];
+      else if constexpr (kTma64) return (R)t64->eta[m][r][c];
+      else return (R)asy->sy[m][r][c];
+    };
 
     R fkp[5];
     // round A: i-faces.  Face fx (0..TI) of row fy lies between tile columns fx-1 and fx.
@@ -441,12 +618,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
       const int fx = t % (TI + 1), fy = t / (TI + 1);
       const int ga = ti0 + fx - 1, gj = tj0 + fy;
       if (ga <= d.IM - 2 && gj <= d.JM - 2) {
-        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p]; };
+        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p + X0]; };
         R f[5];
         const long e = ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1));
-        flux(ld, R(0.5) * ((R)SXk[0][fy][fx] + (R)SXk[0][fy][fx + 1]),
-             R(0.5) * ((R)SXk[1][fy][fx] + (R)SXk[1][fy][fx + 1]),
-             R(0.5) * ((R)SXk[2][fy][fx] + (R)SXk[2][fy][fx + 1]), e, HYB ? (int)(mcur & 1u) : 0, f);
+        flux(ld, R(0.5) * (ax(0, fy, fx) + ax(0, fy, fx + 1)), R(0.5) * (ax(1, fy, fx) + ax(1, fy, fx + 1)),
+             R(0.5) * (ax(2, fy, fx) + ax(2, fy, fx + 1)), e, HYB ? (int)(mcur & 1u) : 0, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fi[n][fy][fx] = f[n];
       }
@@ -456,12 +632,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
       const int fx = t % TI, fy = t / TI;
       const int gi = ti0 + fx, ga = tj0 + fy - 1;
       if (gi <= d.IM - 2 && ga <= d.JM - 2) {
-        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H]; };
+        auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H + X0]; };
         R f[5];
         const long e = nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1));
-        flux(ld, R(0.5) * ((R)SYk[0][fy][fx] + (R)SYk[0][fy + 1][fx]),
-             R(0.5) * ((R)SYk[1][fy][fx] + (R)SYk[1][fy + 1][fx]),
-             R(0.5) * ((R)SYk[2][fy][fx] + (R)SYk[2][fy + 1][fx]), e, HYB ? (int)((mcur >> 1) & 1u) : 0, f);
+        flux(ld, R(0.5) * (ay(0, fy, fx) + ay(0, fy + 1, fx)), R(0.5) * (ay(1, fy, fx) + ay(1, fy + 1, fx)),
+             R(0.5) * (ay(2, fy, fx) + ay(2, fy + 1, fx)), e, HYB ? (int)((mcur >> 1) & 1u) : 0, f);
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) sm.fj[n][fy][fx] = f[n];
       }
@@ -469,6 +644,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     // round C: the k+1/2 face of this column
     if (col_valid) k_face(k, za, zb, HYB ? (int)((mcur >> 2) & 1u) : 0, fkp);
     __syncthreads();
+    // FP64 TMA kernel: plane k+1's set travels during the update (it
+    // overwrites the plane, the area vectors and plane k-2's ring slot, which
+    // the rounds above were the last to read)
+    if (kTma64 && k + 1 < ke) issue_set64(k + 1);
 
     if (col_valid) {
       const long o = node_off(d, ci, cj, k);
@@ -514,6 +693,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
         }
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) a.out[n * VOL + o] = q[n];
+        if (!VISC && a.fuse_bc) fused_bc(a, ci, cj, k, q, smax, snan);
         if (VISC || a.sigma) {
           const double r = q[0], ir = 1.0 / r;
           const double uu = q[1] * ir, vv = q[2] * ir, ww = q[3] * ir;
@@ -532,10 +712,10 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
             double g[9];
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
-              if constexpr (sizeof(R) == 8) {
-                g[m] = SXk[m][cy][cx + 1] * iJ;
-                g[3 + m] = SYk[m][cy + 1][cx] * iJ;
-              } else {  // the FP32 kernels stage FP32 copies
+              if constexpr (sizeof(R) == 8 && !kTma64) {
+                g[m] = asy->sx[m][cy][cx + 1] * iJ;
+                g[3 + m] = asy->sy[m][cy + 1][cx] * iJ;
+              } else {  // the FP32 kernels stage FP32 copies; the FP64 TMA kernel's are being refilled
                 g[m] = __ldg(a.area[m] + o) * iJ;
                 g[3 + m] = __ldg(a.area[3 + m] + o) * iJ;
               }
@@ -560,7 +740,15 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
     for (int m = 0; m < 3; ++m) za[m] = zb[m];
   }
 
-  if (kAsync) cp_async_wait_all();  // nothing in flight when the CTA moves on
+  if constexpr (kTma || kTma64) {
+    // every issued copy was waited for: nothing is in flight; retire the
+    // barriers so a batched CTA can initialise them again for its next item
+    __syncthreads();
+    if (t == 0) {
+      tma::bar_inval(kTma ? &ts->bar[0] : &t64->bar[0]);
+      tma::bar_inval(kTma ? &ts->bar[1] : &t64->bar[1]);
+    }
+  }
   if (MODE != 0 && !VISC && a.sigma) {
     // CTA max, one atomic per CTA
     __shared__ double red[NT / 32];
@@ -580,17 +768,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, int tile, int kc,
   }
 }
 
-template <typename R, bool VISC, int MODE, int NB, bool HYB>
-__global__ void __launch_bounds__(NT, NB) stage_kernel(const StageArgs a) {
+template <typename R, bool VISC, int MODE, int NB, bool HYB, bool TMA>
+__global__ void __launch_bounds__(NT, NB) stage_kernel(const __grid_constant__ StageArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  stage_body<R, VISC, MODE, NB, HYB>(a, blockIdx.x, blockIdx.y, smem_raw);
+  stage_body<R, VISC, MODE, NB, HYB, TMA>(a, &a.tm, blockIdx.x, blockIdx.y, smem_raw);
 }
 
 // Many blocks in one launch: persistent CTAs take work items (block, tile, k
 // chunk) from a queue (one atomic counter); each item's StageArgs are copied
 // from the table into shared memory.  Items are numbered block by block, tiles
-// fastest, so CTAs of one block work on neighbouring columns together.
-template <typename R, bool VISC, int MODE, int NB, bool HYB>
+// fastest, so CTAs of one block work on neighbouring columns together.  The
+// TMA copies read their tensor maps from the table in global memory.
+template <typename R, bool VISC, int MODE, int NB, bool HYB, bool TMA>
 __global__ void __launch_bounds__(NT, NB) stage_kernel_batched(const BatchStage b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ StageArgs args;
@@ -608,14 +797,15 @@ __global__ void __launch_bounds__(NT, NB) stage_kernel_batched(const BatchStage 
     __syncthreads();
     const int local = w - __ldg(b.start + blk);
     const int ntiles = args.ntile_i * args.ntile_j;
-    stage_body<R, VISC, MODE, NB, HYB>(args, local % ntiles, local / ntiles, smem_raw);
+    stage_body<R, VISC, MODE, NB, HYB, TMA>(args, &b.args[blk].tm, local % ntiles, local / ntiles, smem_raw);
     __syncthreads();  // args, item and the shared staging are reused by the next item
   }
 }
 
 
 // The batched kernels run at 2 CTAs per SM (3 for the hybrid, whose stage
-// kernel holds no WENO5 code).
+// kernel holds no WENO5 code); the FP32 ones stage by TMA, the FP64 one
+// synchronously (its TMA form leaves no room for the item's StageArgs).
 template <bool HYB>
 constexpr int batched_nb() {
   return HYB ? 3 : 2;
@@ -624,17 +814,18 @@ constexpr int batched_nb() {
 template <typename R, bool VISC, int MODE, bool HYB>
 cudaError_t launch_batched_t(const BatchStage& b, cudaStream_t s) {
   constexpr int NB = batched_nb<HYB>();
-  const int smem = (int)stage_smem<R, NB>();
+  constexpr bool TMA = sizeof(R) == 4;
+  const int smem = (int)stage_smem<R, NB, TMA>();
   static int grid = 0;
   if (grid == 0) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, NB, HYB>,
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, NB, HYB, TMA>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, NB, HYB>,
+      e = cudaFuncSetAttribute(stage_kernel_batched<R, VISC, MODE, NB, HYB, TMA>,
                                cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     int per_sm = 0, dev = 0, nsm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel_batched<R, VISC, MODE, NB, HYB>, NT,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stage_kernel_batched<R, VISC, MODE, NB, HYB, TMA>, NT,
                                                       smem);
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -643,7 +834,7 @@ cudaError_t launch_batched_t(const BatchStage& b, cudaStream_t s) {
   }
   const int g = b.total < grid ? b.total : grid;
   if (g <= 0) return cudaSuccess;
-  stage_kernel_batched<R, VISC, MODE, NB, HYB><<<g, NT, smem, s>>>(b);
+  stage_kernel_batched<R, VISC, MODE, NB, HYB, TMA><<<g, NT, smem, s>>>(b);
   return cudaGetLastError();
 }
 
@@ -663,47 +854,47 @@ cudaError_t launch_batched_r(const BatchStage& b, int mode, bool visc, cudaStrea
   }
 }
 
-template <typename R, bool VISC, int MODE, int NB, bool HYB>
+template <typename R, bool VISC, int MODE, int NB, bool HYB, bool TMA>
 cudaError_t launch_t(const StageArgs& a, cudaStream_t s) {
-  const size_t smem = stage_smem<R, NB>();
+  const size_t smem = stage_smem<R, NB, TMA>();
   dim3 grid(a.ntile_i * a.ntile_j, (a.d.KM - 2 + a.kchunk - 1) / a.kchunk);
-  stage_kernel<R, VISC, MODE, NB, HYB><<<grid, NT, smem, s>>>(a);
+  stage_kernel<R, VISC, MODE, NB, HYB, TMA><<<grid, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <typename R, int NB, bool HYB>
+template <typename R, int NB, bool HYB, bool TMA>
 void prepare_nb() {
-  const int smem = (int)stage_smem<R, NB>();
+  const int smem = (int)stage_smem<R, NB, TMA>();
   // the largest shared-memory carveout, so that NB CTAs fit on an SM
   auto set = [&](const void* f) {
     cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
   };
-  set((const void*)stage_kernel<R, false, 0, NB, HYB>);
-  set((const void*)stage_kernel<R, false, 1, NB, HYB>);
-  set((const void*)stage_kernel<R, false, 2, NB, HYB>);
-  set((const void*)stage_kernel<R, false, 3, NB, HYB>);
-  set((const void*)stage_kernel<R, true, 0, NB, HYB>);
-  set((const void*)stage_kernel<R, true, 1, NB, HYB>);
-  set((const void*)stage_kernel<R, true, 2, NB, HYB>);
-  set((const void*)stage_kernel<R, true, 3, NB, HYB>);
+  set((const void*)stage_kernel<R, false, 0, NB, HYB, TMA>);
+  set((const void*)stage_kernel<R, false, 1, NB, HYB, TMA>);
+  set((const void*)stage_kernel<R, false, 2, NB, HYB, TMA>);
+  set((const void*)stage_kernel<R, false, 3, NB, HYB, TMA>);
+  set((const void*)stage_kernel<R, true, 0, NB, HYB, TMA>);
+  set((const void*)stage_kernel<R, true, 1, NB, HYB, TMA>);
+  set((const void*)stage_kernel<R, true, 2, NB, HYB, TMA>);
+  set((const void*)stage_kernel<R, true, 3, NB, HYB, TMA>);
 }
 
-template <typename R, int NB, bool HYB>
+template <typename R, int NB, bool HYB, bool TMA>
 cudaError_t launch_r(const StageArgs& a, int mode, bool visc, cudaStream_t s) {
   if (visc) {
     switch (mode) {
-      case 0: return launch_t<R, true, 0, NB, HYB>(a, s);
-      case 1: return launch_t<R, true, 1, NB, HYB>(a, s);
-      case 2: return launch_t<R, true, 2, NB, HYB>(a, s);
-      default: return launch_t<R, true, 3, NB, HYB>(a, s);
+      case 0: return launch_t<R, true, 0, NB, HYB, TMA>(a, s);
+      case 1: return launch_t<R, true, 1, NB, HYB, TMA>(a, s);
+      case 2: return launch_t<R, true, 2, NB, HYB, TMA>(a, s);
+      default: return launch_t<R, true, 3, NB, HYB, TMA>(a, s);
     }
   }
   switch (mode) {
-    case 0: return launch_t<R, false, 0, NB, HYB>(a, s);
-    case 1: return launch_t<R, false, 1, NB, HYB>(a, s);
-    case 2: return launch_t<R, false, 2, NB, HYB>(a, s);
-    default: return launch_t<R, false, 3, NB, HYB>(a, s);
+    case 0: return launch_t<R, false, 0, NB, HYB, TMA>(a, s);
+    case 1: return launch_t<R, false, 1, NB, HYB, TMA>(a, s);
+    case 2: return launch_t<R, false, 2, NB, HYB, TMA>(a, s);
+    default: return launch_t<R, false, 3, NB, HYB, TMA>(a, s);
   }
 }
 
@@ -714,12 +905,13 @@ cudaError_t launch_r(const StageArgs& a, int mode, bool visc, cudaStream_t s) {
 void stage_prepare() {
   static bool done = false;
   if (done) return;
-  prepare_nb<double, 2, false>();
-  prepare_nb<float, 2, false>();
-  prepare_nb<float, 3, false>();
-  prepare_nb<float, 2, true>();
-  prepare_nb<float, 3, true>();
-  prepare_nb<float, 4, true>();
+  prepare_nb<double, 2, false, false>();
+  prepare_nb<double, 2, false, true>();
+  prepare_nb<float, 2, false, true>();
+  prepare_nb<float, 3, false, true>();
+  prepare_nb<float, 2, true, true>();
+  prepare_nb<float, 3, true, true>();
+  prepare_nb<float, 4, true, false>();
   done = true;
 }
 
@@ -728,8 +920,10 @@ void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j) {
   *ntile_j = (d.JM - 2 + TJ - 1) / TJ;
 }
 
-// FP64: 2 CTAs per SM; split FP32: 2 or 3; hybrid: 2, 3 or 4 (variant = CTAs per SM - 2).
-int stage_variants(bool fp32, bool hybrid) { return !fp32 ? 1 : (hybrid ? 3 : 2); }
+// FP64: 2 CTAs per SM, synchronous (variant 0) or TMA staging (variant 1);
+// split FP32: 2 or 3 CTAs per SM; hybrid: 2, 3 or 4 (FP32 variant = CTAs per
+// SM - 2; TMA staging at 2 and 3).
+int stage_variants(bool fp32, bool hybrid) { return !fp32 ? 2 : (hybrid ? 3 : 2); }
 
 cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool fp32, bool hybrid, cudaStream_t s) {
   if (mode < 1 || mode > 3) return cudaErrorInvalidValue;
@@ -739,12 +933,16 @@ cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool 
 }
 
 cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s) {
-  if (!fp32) return launch_r<double, 2, false>(a, mode, visc, s);
+  if (!fp32)
+    return variant == 1 ? launch_r<double, 2, false, true>(a, mode, visc, s)
+                        : launch_r<double, 2, false, false>(a, mode, visc, s);
   if (a.mask) {
-    if (variant == 2) return launch_r<float, 4, true>(a, mode, visc, s);
-    return variant == 1 ? launch_r<float, 3, true>(a, mode, visc, s) : launch_r<float, 2, true>(a, mode, visc, s);
+    if (variant == 2) return launch_r<float, 4, true, false>(a, mode, visc, s);
+    return variant == 1 ? launch_r<float, 3, true, true>(a, mode, visc, s)
+                        : launch_r<float, 2, true, true>(a, mode, visc, s);
   }
-  return variant == 1 ? launch_r<float, 3, false>(a, mode, visc, s) : launch_r<float, 2, false>(a, mode, visc, s);
+  return variant == 1 ? launch_r<float, 3, false, true>(a, mode, visc, s)
+                      : launch_r<float, 2, false, true>(a, mode, visc, s);
 }
 
 }  // namespace cbns

@@ -1,11 +1,25 @@
 // stage.cuh - launch interface of the fused RK3 stage kernel (stage.cu).
 #pragma once
 
+#include <cuda.h>
+
 #include "cbns_common.cuh"
 
 namespace cbns {
 
+// TMA tensor maps of the stage kernels' plane staging (tma.cuh), 4-D: x,
+// rows, planes, fields.  FP32 kernels: q_a the stage input's i-side halo box
+// (4 x 15 x 1 x 5, FP64), q_b its j-side halo box (16 x 3 x 1 x 5), xi / eta
+// the FP32 face-node area vectors (the 6 area32 components; 24 x 15 x 1 x 3
+// and 16 x 17 x 1 x 3).  FP64 TMA kernel: q_a the ring column box (16 x 15 x
+// 1 x 5), q_b the plane-with-halo box (24 x 21 x 1 x 5), xi / eta the FP64
+// area vectors (the 10 area components; the same boxes).
+struct StageMaps {
+  CUtensorMap q_a, q_b, xi, eta;
+};
+
 struct StageArgs {
+  StageMaps tm;        // FP32 kernels: TMA maps for src and area32
   Dims d;
   double gamma, gam1, gam1_inv, gM2;
   const double* src;   // stage input (stencil source), 5 fields
@@ -24,6 +38,9 @@ struct StageArgs {
   int ntile_i, ntile_j, kchunk;
   int visdiv;          // CBNS_VISDIV_*
   int sigma;           // accumulate the interior spectral-radius max (inviscid stage 3)
+  int fuse_bc;         // apply the reference's boundary conditions of an inviscid block without wake
+                       // cut or wall to the output (i faces, k faces; bc_fusable in abi.cu)
+  double p_inf;        // fuse_bc: the pressure the i faces reset to
 };
 
 // Many blocks in one launch (a persistent work queue): args[b] are the

@@ -69,14 +69,15 @@ __global__ void sigma_nodes(const SigmaArgs a) {
 }
 
 // One thread: the host-side prologue of a time step of Block3d::solve.
-__global__ void step_prologue(StepState* st, double CFL) {
+__device__ __forceinline__ void prologue_body(StepState* st, double CFL) {
   if (st->done) return;
   const double t_cur = st->t_cur, t_end = st->t_end;
   if (t_cur + 1.0e-8 > t_end) {  // is_finished (src/Block3d.cpp:476-488)
     st->done = 1;
     return;
   }
-  const double smax = __longlong_as_double((long long)st->sigma_bits);
+  const unsigned long long bits = st->sigma_bits > st->sigma_fixed ? st->sigma_bits : st->sigma_fixed;
+  const double smax = __longlong_as_double((long long)bits);
   double dt = CFL / smax;
   if (dt != dt) {  // calc_dt throws on NaN (src/calc_dt.cu:56-58)
     st->nan_dt = 1;
@@ -89,6 +90,14 @@ __global__ void step_prologue(StepState* st, double CFL) {
   st->sigma_bits = 0ull;  // stage 3 of this step accumulates the next maximum
   st->force_weno = 0;     // the hybrid's audit decides afresh for every step
   st->steps += 1;
+}
+
+__global__ void step_prologue(StepState* st, double CFL) { prologue_body(st, CFL); }
+
+// The prologues of many blocks, one thread each.
+__global__ void step_prologue_batched(StepState* const* st, const double* CFL, int n) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < n) prologue_body(st[b], CFL[b]);
 }
 
 // The per-call path's dt for the stages that follow; new_step (stage 1) also
@@ -113,6 +122,12 @@ cudaError_t launch_sigma_nodes(const SigmaArgs& a, cudaStream_t s) {
 
 cudaError_t launch_step_prologue(StepState* st, double CFL, cudaStream_t s) {
   step_prologue<<<1, 1, 0, s>>>(st, CFL);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_prologue_batched(StepState* const* st, const double* CFL, int n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  step_prologue_batched<<<(n + 63) / 64, 64, 0, s>>>(st, CFL, n);
   return cudaGetLastError();
 }
 

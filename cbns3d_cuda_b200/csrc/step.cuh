@@ -20,6 +20,8 @@ struct SigmaArgs {
 // Zero the accumulator and reduce the spectral radius over all grid nodes.
 cudaError_t launch_sigma_nodes(const SigmaArgs& a, cudaStream_t s);
 cudaError_t launch_step_prologue(StepState* st, double CFL, cudaStream_t s);
+// the prologues of n blocks in one launch (device tables st[n], CFL[n])
+cudaError_t launch_step_prologue_batched(StepState* const* st, const double* CFL, int n, cudaStream_t s);
 // new_step: count a step (per-call stage 1); restart: the count starts over first
 cudaError_t launch_set_dt(StepState* st, double dt, bool new_step, bool restart, cudaStream_t s);
 

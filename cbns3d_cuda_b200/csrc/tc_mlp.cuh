@@ -208,9 +208,14 @@ __device__ __forceinline__ bool run_tile(Smem& s, int t, unsigned& phase, float*
     mma_commit(&s.bar);
   }
   // warp 0 waits on the barrier, the other warps at the CTA barrier (which
-  // issues nothing); every thread then takes the same branch
+  // issues nothing); every thread then takes the same branch.  A wait that
+  // runs out is given a second bounded window: an MMA whose commit has not
+  // arrived may still own its accumulator columns, and the caller frees TMEM
+  // once this returns false, so the MMA gets every chance to retire first; if
+  // it has not after both windows, the tensor pipe is making no progress and
+  // the caller's failure flag is the only recourse.
   const int warp = t >> 5;
-  bool ok = warp == 0 ? mbar_wait(&s.bar, phase) : true;
+  bool ok = warp == 0 ? (mbar_wait(&s.bar, phase) || mbar_wait(&s.bar, phase)) : true;
   phase ^= 1u;
   if (!__syncthreads_and(ok)) return false;
   fence_after_sync();
@@ -238,7 +243,7 @@ __device__ __forceinline__ bool run_tile(Smem& s, int t, unsigned& phase, float*
     mma_bf16(tmem + 32, sdesc(smem_u32(s.one), 128, 256), sdesc(smem_u32(s.b2), 128, 256), true);
     mma_commit(&s.bar);
   }
-  ok = warp == 0 ? mbar_wait(&s.bar, phase) : true;
+  ok = warp == 0 ? (mbar_wait(&s.bar, phase) || mbar_wait(&s.bar, phase)) : true;
   phase ^= 1u;
   if (!__syncthreads_and(ok)) return false;
   fence_after_sync();

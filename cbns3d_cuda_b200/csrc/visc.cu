@@ -29,11 +29,11 @@ __device__ __forceinline__ double dg(const double* f, long o, long s, int g, int
   return (1.0 / 12.0) * f[o - 2 * s] - 2.0 / 3.0 * f[o - s] + (2.0 / 3.0) * f[o + s] - 1.0 / 12.0 * f[o + 2 * s];
 }
 
-__global__ void __launch_bounds__(128) visc_node_kernel(const ViscArgs a) {
-  if (a.check_done && a.st->done) return;
+// Node e of the ghosted box minus its outer layer (i fastest); every lane of
+// the warp calls this (the spectral-radius maximum is a warp reduction).
+__device__ __forceinline__ void visc_node_body(const ViscArgs& a, long e) {
   const Dims& d = a.d;
   const int VI = d.IG - 2, VJ = d.JG - 2, VK = d.KG - 2;
-  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
   double sg = 0.0;
   bool has = false;
   if (e < (long)VI * VJ * VK) {
@@ -114,11 +114,40 @@ __global__ void __launch_bounds__(128) visc_node_kernel(const ViscArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(128) visc_node_kernel(const ViscArgs a) {
+  if (a.check_done && a.st->done) return;
+  visc_node_body(a, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
+// Many blocks in one launch: block b owns CTAs cta[b] .. cta[b+1]-1, args[b]
+// are its ViscArgs.
+__global__ void __launch_bounds__(128) visc_node_batched(const ViscArgs* args, const int* cta, int nblocks) {
+  int lo = 0, hi = nblocks - 1;  // the last b with cta[b] <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(cta + mid) <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const ViscArgs& a = args[lo];
+  if (a.check_done && a.st->done) return;
+  visc_node_body(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);
+}
+
 }  // namespace
 
 cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s) {
-  const long n = (long)(a.d.IG - 2) * (a.d.JG - 2) * (a.d.KG - 2);
-  visc_node_kernel<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(a);
+  visc_node_kernel<<<visc_ctas(a.d), 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+int visc_ctas(const Dims& d) {
+  const long n = (long)(d.IG - 2) * (d.JG - 2) * (d.KG - 2);
+  return (int)((n + 127) / 128);
+}
+
+cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas, cudaStream_t s) {
+  if (total_ctas <= 0) return cudaSuccess;
+  visc_node_batched<<<total_ctas, 128, 0, s>>>(args, cta, nblocks);
   return cudaGetLastError();
 }
 

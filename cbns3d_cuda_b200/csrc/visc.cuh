@@ -20,5 +20,9 @@ struct ViscArgs {
 };
 
 cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s);
+// The same for many blocks in one launch: args and cta are device tables,
+// block b owning CTAs cta[b] .. cta[b+1]-1, cta[b+1] - cta[b] = visc_ctas(its Dims).
+int visc_ctas(const Dims& d);
+cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas, cudaStream_t s);
 
 }  // namespace cbns

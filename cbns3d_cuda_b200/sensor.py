@@ -128,14 +128,3 @@ def save_weights_bin(path, params, tau):
     assert p.size == NPARAM
     with open(path, "wb") as f:
         f.write(b"CBNSSNS1" + struct.pack("<If", NPARAM, float(tau)) + p.tobytes())
-
-
-def choose_threshold(prob, Y, recall=0.995):
-    """Smallest threshold whose recall of WENO-needing faces is at least `recall`
-    (faces at or above it take WENO: uncertain faces fall back to WENO)."""
-    import torch
-    p = prob[Y.bool()]
-    if p.numel() == 0:
-        return 0.5
-    q = torch.quantile(p.float(), 1.0 - recall).item()
-    return float(max(min(q, 0.5), 1e-4))

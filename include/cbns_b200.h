@@ -180,7 +180,20 @@ int cbns_get_conservative(cbns_ctx* ctx, int which, double* Q_host);
 int cbns_get_primitive(cbns_ctx* ctx, double* rho, double* u, double* v, double* w,
                        double* p, double* T);
 
-/* The RK3 right-hand-side path, one reference entry point each. */
+/* The RK3 right-hand-side path, one reference entry point each.
+ * Calls are stream-ordered on the context's stream: the entry points that only
+ * launch device work (cbns_initial_condition, cbns_calc_conservative,
+ * cbns_calc_primitive, cbns_set_bc_calc_primitive, cbns_calc_numerical_flux,
+ * cbns_calc_viscous_terms, cbns_calc_viscous_flux_contribution,
+ * cbns_update_rk3) return once their kernels are enqueued; every call that
+ * reads into or from host memory (cbns_calc_dt, cbns_get_*, cbns_set_*,
+ * cbns_calc_metrics, ...) waits for the stream first, so a caller sees the
+ * results of all earlier calls.  Errors of enqueued kernels surface at the
+ * next waiting call.  The block3d_cuda:: shims wait after every call, as the
+ * reference does (each of its calls ends with cudaDeviceSynchronize). */
+/* Wait for every call enqueued on the context's stream (no counterpart in the
+ * reference; the shims' per-call cudaDeviceSynchronize). */
+int cbns_synchronize(cbns_ctx* ctx);
 int cbns_set_bc_calc_primitive(cbns_ctx* ctx, int which);
 int cbns_calc_primitive(cbns_ctx* ctx, int which);
 int cbns_calc_numerical_flux(cbns_ctx* ctx, int which);
@@ -271,10 +284,15 @@ int cbns_mlp_adam(float* params_dev, const float* grad_dev, float* m_dev, float*
 int cbns_mlp_predict(const float* params_dev, const float* x_dev, unsigned n, float* out_dev,
                      int use_tensor_cores, int* status_dev, void* stream);
 
-/* The hybrid flux (CBNS_PREC_HYBRID).  Every time step the network is
- * evaluated on every face of the step's starting state on the tensor cores;
- * faces with probability >= tau take the characteristic WENO5 flux, the others
- * the linear upwind-5 flux (same Lax-Friedrichs splitting, component-wise).
+/* The hybrid flux (CBNS_PREC_HYBRID).  On every n-th time step
+ * (cbns_sensor_interval, default 3) the network is evaluated on every face of
+ * the step's starting state on the tensor cores; faces with probability >= tau
+ * take the characteristic WENO5 flux -- the faces the network is confident
+ * need it and those it is unsure about -- and only the faces it is confident
+ * are smooth (p < tau) take the linear upwind-5 flux (same Lax-Friedrichs
+ * splitting, component-wise).  The trained weights' tau is the lower edge of
+ * that uncertainty band: at most 0.5, with a held-out recall floor of the
+ * WENO5-labelled faces (cbns3d_cuda_b200/train_sensor.py).
  * The WENO5 decisions are then widened, per face direction, by 2 faces along
  * the face's own grid line and 1 face in the two other index directions (a
  * discontinuity moves less than a cell per step), and hold for the three
@@ -283,7 +301,10 @@ int cbns_mlp_predict(const float* params_dev, const float* x_dev, unsigned n, fl
  * on the linear faces whose run of 128 consecutive global face indices r =
  * index / 128 has r % audit_stride equal to step % audit_stride, both
  * fluxes; a relative difference above audit_bound
- * on any of them makes the whole step take WENO5 everywhere.  A context of
+ * on any of them makes the whole step take WENO5 everywhere.  The audit runs on
+ * the step's starting state before its first stage, so a step that would
+ * break the bound is taken with WENO5 from the start instead of being taken
+ * and reverted (the same state, without the discarded stage work).  A context of
  * precision HYBRID refuses to step (CBNS_ERR_STATE) until cbns_sensor_load.
  * params_host: CBNS_SENSOR_NPARAM floats in host memory. */
 int cbns_sensor_load(cbns_ctx* ctx, const float* params_host, float tau);
@@ -349,6 +370,11 @@ int cbns_batch_run_async(cbns_batch* batch, unsigned nsteps, double t_end);
  * stage kernel for this context's precision (the state is not modified);
  * *chosen (may be null) receives the variant index.  Later steps use it. */
 int cbns_autotune(cbns_ctx* ctx, int* chosen);
+/* Use compiled variant `variant` of the stage kernel (0 .. count-1; count from
+ * *count when not null, variant -1 only queries it).  FP64: 0 stages each
+ * plane synchronously, 1 by TMA (the same arithmetic, bit for bit); FP32:
+ * 2 + variant CTAs per SM.  No counterpart in the reference. */
+int cbns_stage_variant(cbns_ctx* ctx, int variant, int* count);
 
 /* Per-kernel device timing with CUDA events on the launch stream.  Kernel ids:
  * 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous node

@@ -40,10 +40,17 @@ def _block(case, precision):
     return b
 
 
-@pytest.mark.parametrize("precision,viscous", [(PREC_FP64, False), (PREC_SPLIT, False), (PREC_SPLIT, True),
-                                               (PREC_FP64, True), (PREC_HYBRID, False)])
-def test_batch_equals_blocks_alone(precision, viscous):
+# bc_mode 1 (far field on every face, the batched-block configuration's) runs
+# the blocks' boundary and viscous node kernels as one batched launch each per
+# stage; bc_mode 0 (the reference's boundaries) runs them block by block
+@pytest.mark.parametrize("precision,viscous,bc_mode", [(PREC_FP64, False, 1), (PREC_SPLIT, False, 1),
+                                                       (PREC_SPLIT, True, 1), (PREC_FP64, True, 1),
+                                                       (PREC_HYBRID, False, 1), (PREC_HYBRID, True, 1),
+                                                       (PREC_FP64, True, 0), (PREC_SPLIT, False, 0)])
+def test_batch_equals_blocks_alone(precision, viscous, bc_mode):
     cs, draw = cases.case_batch(5, seed=3, size_lo=(20, 14, 10), size_hi=(44, 30, 18), viscous=viscous)
+    for c in cs:
+        c.params["bc_mode"] = bc_mode
     n = 8
     alone = [_block(c, precision) for c in cs]
     for b in alone:

@@ -231,6 +231,47 @@ def test_trained_sensor_sweep_matches_sampled_faces():
     assert 0 < m.sum() < m.size
 
 
+def test_uncertain_faces_take_weno():
+    """Only faces the committed network is confident are smooth take the linear
+    flux: its threshold is at most 0.5 (the network's own decision boundary)
+    and keeps the recorded held-out recall floor; scaling a real face's
+    features sweeps the network's answer through the uncertainty band [tau,
+    0.9); and on a live state every face the predictor places in that band is
+    a WENO5 face in the sweep's decisions."""
+    import json
+    from pathlib import Path
+    w = np.load(Path(__file__).resolve().parents[1] / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz")
+    P, tau = w["params"].astype(np.float32), float(w["tau"])
+    summ = json.loads(str(w["summary"]))
+    assert tau <= 0.5
+    assert summ["val_recall"] >= summ["recall_floor"] >= 0.95
+    # crafted features in the band: interpolate between a flat face (p ~ 0) and
+    # a strong-jump face (p ~ 1) and keep the points whose p lies in [tau, 0.9)
+    c = cases.case_shock_vortex(64, 64, 16)
+    h = _block(c, PREC_HYBRID, P, tau)
+    X, _ = sensor.sample_faces(h)
+    Pt = torch.from_numpy(P).cuda()
+    p = sensor.predict(Pt, X, tensor_cores=True)
+    hi = X[int(torch.argmax(p))]
+    a = torch.linspace(0.0, 1.0, 4096, device="cuda")[:, None]
+    Xc = (a * hi[None, :]).contiguous()
+    pc = sensor.predict(Pt, Xc, tensor_cores=True).cpu().numpy()
+    band = (pc >= tau + 1e-3) & (pc < 0.9)
+    # the scaled faces sweep p through the uncertainty band, its lower edge
+    # (the network's decision boundary p = 0.5) included
+    assert band.sum() >= 10 and np.any((pc >= tau) & (pc < tau + 0.05))
+    # the library's decision rule on crafted features: the predictor's p >= tau
+    # is WENO5; on the live state the sweep agrees with that rule face by face
+    h.eval_rhs(CBNS_Q)
+    m, _ = h.sensor_mask()
+    Xs, _y, _d, idx = sensor.sample_faces(h, with_dev=True)
+    ps = sensor.predict(Pt, Xs, tensor_cores=True).cpu().numpy()
+    idx = idx.cpu().numpy()
+    in_band = (ps >= tau + 1e-4) & (ps < 0.9) & ~_flat(Xs)
+    assert in_band.sum() > 0
+    assert np.all(m[idx[in_band]] == 1)
+
+
 def test_sensor_interval_holds_and_widens_decisions():
     """With the network evaluated every 3rd step, a 3-step run uses the first
     step's decisions, widened by 4 along and 3 across, for all three steps."""

@@ -458,7 +458,8 @@ def run_ours(a):
                        "sensor": {"weights": os.path.relpath(a.sensor, ROOT), "tau": SENSOR[1]}},
             "rho_l2_vs_fp64": l2_h, "rho_linf_vs_fp64": linf_h,
             "plain_vs_reference_linf": ref_cmp["max"] if ref_cmp else None,
-            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "kernels": kern_ms(kern64),
+            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "stage_variant": p64["variant"],
+                               "kernels": kern_ms(kern64),
                                "roofline_hbm": {"achieved": ach64, "peak": peak, "unit": "GB/s",
                                                 "frac": (ach64 / peak) if ach64 else None, "traffic": traffic64},
                                "roofline_fp64": {"achieved": tfl64, "peak": fp64_peak, "unit": "TFLOP/s",

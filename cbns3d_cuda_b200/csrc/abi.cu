@@ -513,10 +513,16 @@ int run_prepare(cbns_ctx* c, double t_end) {
   // viscous far field: the steps leave the boundary primitives as they are
   // (enqueue_step); form them here from the state the run starts from
   if (c->ph.viscous && c->prm.bc_mode == CBNS_BC_FARFIELD) RET(bc_launch(c, bc_args(c, c->qb[c->lq], false, false), false));
-  // fused boundary conditions: the held j-face rows' share of every step's dt
+  // fused boundary conditions: the held j-face rows' share of every step's
+  // dt; and one boundary pass over the other two state buffers, so that their
+  // nodes the stage kernel's boundary conditions do not rewrite -- the k-face
+  // copies of the held j-face rows -- equal the logical Q's (the reference's
+  // Q_p receives those copies from its own boundary passes)
   if (bc_fusable(c)) {
     CK(launch_bc_fixed_sigma(bc_args(c, c->qb[c->lq], false, false), c->stream));
     c->launches += 1;
+    for (int b = 0; b < 3; ++b)
+      if (b != c->lq) RET(bc_launch(c, bc_args(c, c->qb[b], false, false), false));
   }
   RET(sync(c));
   if (!c->sigma_valid) {

@@ -72,6 +72,22 @@ constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;  // halo nodes of a plane: i-h
 template <typename R>
 using AreaT = typename std::conditional<sizeof(R) == 4, float, double>::type;
 
+// Loads of values each thread reads once (the ring column, the RK operands,
+// 1/J and the column's zeta area vectors) bypass L1 allocation, so the lines
+// that are re-read there -- the WENO5 face fluxes asked into L1 a plane
+// ahead -- are not evicted by the stream.  ld_stream_rw for the RK base of
+// stage 3, which the kernel itself overwrites (no non-coherent path).
+__device__ __forceinline__ double ld_stream(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double ld_stream_rw(const double* p) {
+  double v;
+  asm volatile("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
+  return v;
+}
+
 __device__ __forceinline__ void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
@@ -310,14 +326,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
       if (ci <= d.IM + 1 && cj <= d.JM + 1) {
         const long o = node_off(d, ci, cj, kp);
 #pragma unroll
-        for (int n = 0; n < NEQ; ++n) dst[n * NC] = (S)__ldg(a.src + n * VOL + o);
+        for (int n = 0; n < NEQ; ++n) dst[n * NC] = (S)ld_stream(a.src + n * VOL + o);
       }
     }
   };
   auto load_zeta = [&](int kp, double z[3]) {
     const long o = node_off(d, ci, cj, kp);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) z[m] = __ldg(a.area[6 + m] + o);
+    for (int m = 0; m < 3; ++m) z[m] = ld_stream(a.area[6 + m] + o);
   };
 
   // k-face between planes kk and kk+1 of this thread's column
@@ -342,7 +358,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
     if (col_thread && ci <= d.IM + 1 && cj <= d.JM + 1) {
       const long o = node_off(d, ci, cj, kp);
 #pragma unroll
-      for (int n = 0; n < NEQ; ++n) pre[n] = __ldg(a.src + n * VOL + o);
+      for (int n = 0; n < NEQ; ++n) pre[n] = ld_stream(a.src + n * VOL + o);
     }
   };
   auto store_ring = [&](int kp) {
@@ -412,6 +428,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
       tma::bar_init(kTma ? &ts->bar[1] : &t64->bar[1]);
       tma::fence_init();
     }
+    __syncthreads();  // no thread waits on a barrier before it is initialised
   }
   // warm-up: planes kb-3 .. kb+2 and the kb-1/2 face
   bool landed = true;
@@ -667,7 +684,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
           df[n + 1] -= dv;
         }
       }
-      const double iJ = __ldg(a.area[9] + o);
+      const double iJ = ld_stream(a.area[9] + o);
       if (MODE == 0) {
         const long r = 5L * ((ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * (k - 1)));
 #pragma unroll
@@ -681,19 +698,18 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
           const long e = n * VOL + o;
           const double qin = kExactRing ? (double)sm.ring[sk][n][t] : 0.0;
           if (MODE == 1) {
-            q[n] = ((kExactRing && a.q0_is_src) ? qin : __ldg(a.q0 + e)) - L;
+            q[n] = ((kExactRing && a.q0_is_src) ? qin : ld_stream(a.q0 + e)) - L;
           } else if (MODE == 2) {
-            q[n] = 0.75 * __ldg(a.q0 + e) + 0.25 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L);
+            q[n] = 0.75 * ld_stream(a.q0 + e) + 0.25 * (((kExactRing && a.qp_is_src) ? qin : ld_stream(a.qp + e)) - L);
           } else {
             // the plain (FP64) kernel divides by 3 as the reference does; the
             // FP32-flux kernels multiply by the rounded 1/3 (one ulp apart)
-            const double sum = a.q0[e] + 2.0 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L);
+            const double sum = ld_stream_rw(a.q0 + e) + 2.0 * (((kExactRing && a.qp_is_src) ? qin : ld_stream(a.qp + e)) - L);
             q[n] = kExactRing ? sum / 3.0 : sum * (1.0 / 3.0);
           }
         }
 #pragma unroll
         for (int n = 0; n < NEQ; ++n) a.out[n * VOL + o] = q[n];
-        if (!VISC && a.fuse_bc) fused_bc(a, ci, cj, k, q, smax, snan);
         if (VISC || a.sigma) {
           const double r = q[0], ir = 1.0 / r;
           const double uu = q[1] * ir, vv = q[2] * ir, ww = q[3] * ir;
@@ -738,6 +754,25 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
     for (int n = 0; n < NEQ; ++n) fkm[n] = fkp[n];
 #pragma unroll
     for (int m = 0; m < 3; ++m) za[m] = zb[m];
+  }
+
+  // fused boundary conditions, after the sweep so that their registers do not
+  // add to the flux rounds': the threads of the columns next to an i face
+  // read back every plane they wrote, the others the planes next to a k face
+  if (MODE != 0 && !VISC && a.fuse_bc && col_valid) {
+    auto apply = [&](int k) {
+      const long o = node_off(d, ci, cj, k);
+      double q[NEQ];
+#pragma unroll
+      for (int n = 0; n < NEQ; ++n) q[n] = a.out[n * VOL + o];  // this thread's own stores
+      fused_bc(a, ci, cj, k, q, smax, snan);
+    };
+    if (ci == 1 || ci == d.IM - 2) {
+      for (int k = kb; k < ke; ++k) apply(k);
+    } else {
+      if (kb == 1) apply(1);
+      if (ke == d.KM - 1 && d.KM - 2 != 1) apply(d.KM - 2);
+    }
   }
 
   if constexpr (kTma || kTma64) {

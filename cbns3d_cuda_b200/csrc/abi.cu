@@ -242,16 +242,7 @@ ViscArgs visc_args(cbns_ctx* c, bool check_done, bool sigma) {
   return a;
 }
 
-// An inviscid block under the reference's boundary conditions with no wake cut
-// (i_begin = 1) and no wall (i_end = 0): its boundary conditions need only
-// the new state of the node next to each boundary node, so the stage kernel
-// applies them itself (fused_bc in stage.cu) in whole-step runs.
-bool bc_fusable(const cbns_ctx* c) {
-  return c->prm.bc_mode == CBNS_BC_REFERENCE && !c->ph.viscous && c->ph.i_begin == 1u && c->ph.i_end == 0u;
-}
-
-StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const double* qp, double* out, bool sigma,
-                     bool fuse_bc = false) {
+StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const double* qp, double* out, bool sigma) {
   StageArgs a;
   a.d = c->d;
   a.gamma = c->ph.gamma;
@@ -274,8 +265,6 @@ StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const dou
   a.kchunk = c->kchunk;
   a.visdiv = c->ph.visdiv;
   a.sigma = sigma;
-  a.fuse_bc = fuse_bc && bc_fusable(c);
-  a.p_inf = c->ph.p_inf;
   a.mask = c->ph.precision == CBNS_PREC_HYBRID ? c->mask : nullptr;
   a.wflux = c->wflux;
   a.tm = c->tm[0];  // src is always one of the three state buffers
@@ -457,14 +446,12 @@ int enqueue_step(cbns_ctx* c) {
     // O-grid: the wrap copy rewrites nodes stage 3 updated, so the spectral
     // radius is swept after the boundary pass
     const bool fuse = last && !visc && !ogrid(c);
-    RET(stage_launch(c, stage_args(c, s[k].src, s[k].q0, s[k].qp, s[k].out, fuse, true), k + 1));
-    // no boundary pass in the step when the stage kernel applied the boundary
-    // conditions (bc_fusable), or for a viscous far-field block, whose
-    // boundary and ghost nodes hold their Q, so that their primitives (formed
-    // at the start of the run) stand, the stage kernel recovering the interior
+    RET(stage_launch(c, stage_args(c, s[k].src, s[k].q0, s[k].qp, s[k].out, fuse), k + 1));
+    // no boundary pass in the step for a viscous far-field block: its
+    // boundary and ghost nodes hold their Q, so their primitives (formed at
+    // the start of the run) stand, the stage kernel recovering the interior
     // primitives and the viscous node kernel the spectral radii
-    if (!bc_fusable(c) && !(visc && c->prm.bc_mode == CBNS_BC_FARFIELD))
-      RET(bc_launch(c, bc_args(c, s[k].out, true, fuse), false));
+    if (!(visc && c->prm.bc_mode == CBNS_BC_FARFIELD)) RET(bc_launch(c, bc_args(c, s[k].out, true, fuse), false));
     if (last && !visc && ogrid(c)) RET(sigma_launch(c));
     if (visc) RET(visc_launch(c, visc_args(c, true, last)));
   }
@@ -508,22 +495,10 @@ int run_prepare(cbns_ctx* c, double t_end) {
   h.done = 0;
   h.nan_dt = 0;
   h.steps = 0;
-  h.sigma_fixed = 0ull;
   CK(cudaMemcpyAsync(c->st, &h, sizeof(h), cudaMemcpyHostToDevice, c->stream));
   // viscous far field: the steps leave the boundary primitives as they are
   // (enqueue_step); form them here from the state the run starts from
   if (c->ph.viscous && c->prm.bc_mode == CBNS_BC_FARFIELD) RET(bc_launch(c, bc_args(c, c->qb[c->lq], false, false), false));
-  // fused boundary conditions: the held j-face rows' share of every step's
-  // dt; and one boundary pass over the other two state buffers, so that their
-  // nodes the stage kernel's boundary conditions do not rewrite -- the k-face
-  // copies of the held j-face rows -- equal the logical Q's (the reference's
-  // Q_p receives those copies from its own boundary passes)
-  if (bc_fusable(c)) {
-    CK(launch_bc_fixed_sigma(bc_args(c, c->qb[c->lq], false, false), c->stream));
-    c->launches += 1;
-    for (int b = 0; b < 3; ++b)
-      if (b != c->lq) RET(bc_launch(c, bc_args(c, c->qb[b], false, false), false));
-  }
   RET(sync(c));
   if (!c->sigma_valid) {
     RET(sigma_launch(c));
@@ -600,9 +575,9 @@ int batch_tables(cbns_batch* b) {
     double* P0 = c->qb[c->lq];
     double* P1 = c->qb[c->ls];
     double* P2 = c->qb[c->lp];
-    tab[0 * nb + i] = stage_args(c, P0, P0, P0, P1, false, true);
-    tab[1 * nb + i] = stage_args(c, P1, P0, P1, P2, false, true);
-    tab[2 * nb + i] = stage_args(c, P2, P0, P2, P0, !b->visc, true);
+    tab[0 * nb + i] = stage_args(c, P0, P0, P0, P1, false);
+    tab[1 * nb + i] = stage_args(c, P1, P0, P1, P2, false);
+    tab[2 * nb + i] = stage_args(c, P2, P0, P2, P0, !b->visc);
     start[i + 1] = start[i] + c->ntile_i * c->ntile_j * ((c->d.KM - 2 + c->kchunk - 1) / c->kchunk);
     b->roles.insert(b->roles.end(), {c->lq, c->lp, c->ls});
   }
@@ -715,7 +690,7 @@ int batch_enqueue_body(cbns_batch* b) {
     RET(batch_fork(b));
     for (cbns_ctx* c : b->blk) {
       double* out = k == 0 ? c->qb[c->ls] : (k == 1 ? c->qb[c->lp] : c->qb[c->lq]);
-      if (!bc_fusable(c)) RET(bc_launch(c, bc_args(c, out, true, last && !b->visc), false));
+      RET(bc_launch(c, bc_args(c, out, true, last && !b->visc), false));
       if (b->visc) RET(visc_launch(c, visc_args(c, true, last)));
     }
   }

@@ -439,36 +439,6 @@ __global__ void bc_wrap(const BCArgs a) {
   }
 }
 
-// Spectral radii of the j = 0 and j = JM-1 grid rows (every i in [0, IM), k in
-// [0, KM)) into st->sigma_fixed: in an inviscid reference-mode block without
-// wake cut or wall these nodes hold their state during a run, so their terms
-// of the boundary kernels' maximum (bc_phase3: j faces, and the k-face copies
-// of those rows) are fixed; the stage kernels that apply the other boundary
-// conditions themselves (fused_bc in stage.cu) leave them to this value.
-__global__ void bc_jrows_sigma(const BCArgs a) {
-  const Dims& d = a.d;
-  const long n = 2L * d.IM * d.KM;
-  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  double sg = 0.0;
-  bool has = false;
-  if (e < n) {
-    const int side = e >= (long)d.IM * d.KM;
-    const long r = side ? e - (long)d.IM * d.KM : e;
-    const int i = (int)(r % d.IM), k = (int)(r / d.IM);
-    const long o = node_off(d, i, side ? d.JM - 1 : 0, k);
-    sg = sigma_inv(a, o, prim_of(a.q, o, d.VOL, a.gam1));
-    has = true;
-  }
-  const bool nan = has && (sg != sg);
-  double m = (has && !nan) ? sg : 0.0;
-  const unsigned anyhas = __ballot_sync(0xffffffffu, has);
-  const unsigned anynan = __ballot_sync(0xffffffffu, nan);
-#pragma unroll
-  for (int k = 16; k > 0; k >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, k));
-  if ((threadIdx.x & 31) == 0 && anyhas != 0u)
-    atomic_max_sigma(&a.st->sigma_fixed, anynan ? __longlong_as_double(0x7ff8000000000000ll) : m);
-}
-
 // Interior primitives (rho,u,v,w,p,T) from Q, the first part of
 // primitive_bc_kernel (:59-79); needed when the primitive arrays do not yet
 // describe the buffer the boundary conditions act on.
@@ -538,13 +508,6 @@ cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int*
   bc_phase3<<<nblk(n3, B), B, 0, s>>>(a);
   ++nl;
   if (launches) *launches += nl;
-  return cudaGetLastError();
-}
-
-cudaError_t launch_bc_fixed_sigma(const BCArgs& a, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(&a.st->sigma_fixed, 0, sizeof(unsigned long long), s);
-  if (e != cudaSuccess) return e;
-  bc_jrows_sigma<<<nblk(2L * a.d.IM * a.d.KM, 128), 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 

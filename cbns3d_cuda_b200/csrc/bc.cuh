@@ -27,10 +27,6 @@ struct BCArgs {
 // primitive arrays do not describe this buffer.  *launches += kernels launched.
 cudaError_t launch_bc(const BCArgs& a, bool interior_prims, cudaStream_t s, int* launches);
 
-// st->sigma_fixed = the spectral-radius max of the j = 0 and j = JM-1 grid
-// rows of a.q (blocks whose stage kernels apply their boundary conditions).
-cudaError_t launch_bc_fixed_sigma(const BCArgs& a, cudaStream_t s);
-
 // CBNS_BC_FARFIELD for many blocks in one launch (the batched form): args and
 // cta are device tables, block b owning CTAs cta[b] .. cta[b+1]-1 (cta has
 // nblocks + 1 entries, cta[b+1] - cta[b] = bc_farfield_ctas(its Dims)).

@@ -68,8 +68,6 @@ struct StepState {
   int sensor_fail;                // hybrid: a tensor-core wait timed out
   unsigned weno_listed;           // hybrid: length of the step's list of WENO5 faces
   int stage_fail;                 // a stage kernel's TMA wait timed out (the state is not valid)
-  unsigned long long sigma_fixed; // spectral-radius max of boundary nodes whose state is held during a run
-                                  // (bit pattern; 0 = none), taken into every step's dt
 };
 
 // Positive doubles order like their bit patterns; a NaN (either sign) compares

@@ -72,22 +72,6 @@ constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;  // halo nodes of a plane: i-h
 template <typename R>
 using AreaT = typename std::conditional<sizeof(R) == 4, float, double>::type;
 
-// Loads of values each thread reads once (the ring column, the RK operands,
-// 1/J and the column's zeta area vectors) bypass L1 allocation, so the lines
-// that are re-read there -- the WENO5 face fluxes asked into L1 a plane
-// ahead -- are not evicted by the stream.  ld_stream_rw for the RK base of
-// stage 3, which the kernel itself overwrites (no non-coherent path).
-__device__ __forceinline__ double ld_stream(const double* p) {
-  double v;
-  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ double ld_stream_rw(const double* p) {
-  double v;
-  asm volatile("ld.global.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p) : "memory");
-  return v;
-}
-
 __device__ __forceinline__ void prefetch_l1(const void* p) {
   asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
 }
@@ -166,81 +150,6 @@ __host__ __device__ constexpr size_t stage_smem() {
 __device__ __forceinline__ double d4(const double* f, long o, long s) {
   return (1.0 / 12.0) * __ldg(f + o - 2 * s) - (2.0 / 3.0) * __ldg(f + o - s) + (2.0 / 3.0) * __ldg(f + o + s) -
          (1.0 / 12.0) * __ldg(f + o + 2 * s);
-}
-
-// Spectral-radius sum of time_step_kernel (inviscid form) at node offset o
-// from the conservative state v, with the node's metrics; the arithmetic of
-// the boundary kernels' (bc.cu) so the fused boundary gives the same dt.
-__device__ __forceinline__ double sigma_node(const StageArgs& a, long o, const double v[NEQ]) {
-  const double r = v[0], u = v[1] / r, w = v[2] / r, x = v[3] / r;
-  const double p = a.gam1 * (v[4] - 0.5 * r * (u * u + w * w + x * x));
-  const double c = sqrt(a.gamma * p / r);
-  double sum = 0.0;
-#pragma unroll
-  for (int dd = 0; dd < 3; ++dd) {
-    const double mx = a.met[3 * dd][o], my = a.met[3 * dd + 1][o], mz = a.met[3 * dd + 2][o];
-    sum += fabs(u * mx + w * my + x * mz) + c * sqrt(mx * mx + my * my + mz * mz);
-  }
-  return sum;
-}
-
-// The reference's boundary conditions of an inviscid block without wake cut
-// or wall, applied to the stage output by the thread that formed the new
-// state q of interior node (ci, cj, k) (StageArgs.fuse_bc):
-//   i faces (primitive_bc_kernel.cu:84-186): at ci = 1 the nodes i = 0, -1, -2
-//     take q's density and momentum with the energy that resets the pressure
-//     to p_inf, at ci = IM-2 the nodes IM-1 .. IM+1 likewise;
-//   k faces (:417-492): at k = 1 the nodes k = 0, -1, -2 of every (i, j) in
-//     [0, IM) x [0, JM) copy k = 1 -- here the column's own node and, beside
-//     an i face, the face node i = 0 (IM-1) -- and at k = KM-2 likewise.
-// The j faces hold their state (no wake, no wall, no rewrite of Q), so their
-// k-face copies are already in place; their spectral radii are fixed for the
-// run (StepState.sigma_fixed).  With a.sigma (stage 3) the i- and k-face
-// grid nodes add their spectral radii as bc_phase3 does.
-__device__ __forceinline__ void fused_bc(const StageArgs& a, int ci, int cj, int k, const double q[NEQ],
-                                         double& smax, bool& snan) {
-  const Dims& d = a.d;
-  const bool lo_i = ci == 1, hi_i = ci == d.IM - 2, lo_k = k == 1, hi_k = k == d.KM - 2;
-  if (!(lo_i || hi_i || lo_k || hi_k)) return;
-  const long VOL = d.VOL;
-  double b[NEQ];
-#pragma unroll
-  for (int n = 0; n < 4; ++n) b[n] = q[n];
-  b[4] = a.p_inf / a.gam1 + 0.5 * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]) / q[0];
-  auto put = [&](int i, int kk, const double* v) {
-    const long o = node_off(d, i, cj, kk);
-#pragma unroll
-    for (int n = 0; n < NEQ; ++n) a.out[n * VOL + o] = v[n];
-  };
-  auto sig = [&](int i, int kk, const double* v) {
-    if (a.sigma) {
-      const double x = sigma_node(a, node_off(d, i, cj, kk), v);
-      if (x != x) snan = true;
-      smax = fmax(smax, x);
-    }
-  };
-  if (lo_i) {
-    for (int l = 0; l <= NG; ++l) put(-l, k, b);
-    sig(0, k, b);
-  }
-  if (hi_i) {
-    for (int l = 0; l <= NG; ++l) put(d.IM - 1 + l, k, b);
-    sig(d.IM - 1, k, b);
-  }
-  for (int side = 0; side < 2; ++side) {
-    if (side == 0 ? !lo_k : !hi_k) continue;
-    const int base = side ? d.KM - 1 : 0, dir = side ? 1 : -1;
-    for (int l = 0; l <= NG; ++l) put(ci, base + dir * l, q);
-    sig(ci, base, q);
-    if (lo_i) {
-      for (int l = 0; l <= NG; ++l) put(0, base + dir * l, b);
-      sig(0, base, b);
-    }
-    if (hi_i) {
-      for (int l = 0; l <= NG; ++l) put(d.IM - 1, base + dir * l, b);
-      sig(d.IM - 1, base, b);
-    }
-  }
 }
 
 // NB = CTAs per SM the register budget is cut for: FP64 always 2 (shared
@@ -326,14 +235,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
       if (ci <= d.IM + 1 && cj <= d.JM + 1) {
         const long o = node_off(d, ci, cj, kp);
 #pragma unroll
-        for (int n = 0; n < NEQ; ++n) dst[n * NC] = (S)ld_stream(a.src + n * VOL + o);
+        for (int n = 0; n < NEQ; ++n) dst[n * NC] = (S)__ldg(a.src + n * VOL + o);
       }
     }
   };
   auto load_zeta = [&](int kp, double z[3]) {
     const long o = node_off(d, ci, cj, kp);
 #pragma unroll
-    for (int m = 0; m < 3; ++m) z[m] = ld_stream(a.area[6 + m] + o);
+    for (int m = 0; m < 3; ++m) z[m] = __ldg(a.area[6 + m] + o);
   };
 
   // k-face between planes kk and kk+1 of this thread's column
@@ -358,7 +267,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
     if (col_thread && ci <= d.IM + 1 && cj <= d.JM + 1) {
       const long o = node_off(d, ci, cj, kp);
 #pragma unroll
-      for (int n = 0; n < NEQ; ++n) pre[n] = ld_stream(a.src + n * VOL + o);
+      for (int n = 0; n < NEQ; ++n) pre[n] = __ldg(a.src + n * VOL + o);
     }
   };
   auto store_ring = [&](int kp) {
@@ -517,6 +426,23 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
       if (!all_weno) {
         prefetch_weno(k, mcur);
         if (k + 1 < ke) mnext = mask_bits(k + 1);
+      }
+    }
+    // viscous kernels ask L2 for the node fluxes the next plane's divergence
+    // reads (the column's own lines of all twelve arrays at plane k+1, and of
+    // the k-direction arrays at the stencil's leading plane k+3; the tile's
+    // other columns cover the neighbouring rows): the divergence's 48 loads
+    // per node then hit L2 instead of waiting for DRAM
+    if (VISC && MODE != 0 && col_valid && k + 1 < ke) {
+      const long o = node_off(d, ci, cj, k + 1);
+      const long sh = a.visdiv == 0 ? 1 : 0;
+      const long oi = o - sh * (d.PX + d.PL), oj = o - sh * (1 + d.PL), ok = o - sh * (1 + d.PX);
+#pragma unroll
+      for (int n = 0; n < 4; ++n) {
+        prefetch_l2(a.vflux[n] + oi);
+        prefetch_l2(a.vflux[4 + n] + oj);
+        prefetch_l2(a.vflux[8 + n] + ok);
+        prefetch_l2(a.vflux[8 + n] + ok + 2 * d.PL);
       }
     }
     // the FP32 kernels ask L2 for the next plane's RK operands and 1/J now, so
@@ -684,7 +610,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
           df[n + 1] -= dv;
         }
       }
-      const double iJ = ld_stream(a.area[9] + o);
+      const double iJ = __ldg(a.area[9] + o);
       if (MODE == 0) {
         const long r = 5L * ((ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * (k - 1)));
 #pragma unroll
@@ -698,13 +624,13 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
           const long e = n * VOL + o;
           const double qin = kExactRing ? (double)sm.ring[sk][n][t] : 0.0;
           if (MODE == 1) {
-            q[n] = ((kExactRing && a.q0_is_src) ? qin : ld_stream(a.q0 + e)) - L;
+            q[n] = ((kExactRing && a.q0_is_src) ? qin : __ldg(a.q0 + e)) - L;
           } else if (MODE == 2) {
-            q[n] = 0.75 * ld_stream(a.q0 + e) + 0.25 * (((kExactRing && a.qp_is_src) ? qin : ld_stream(a.qp + e)) - L);
+            q[n] = 0.75 * __ldg(a.q0 + e) + 0.25 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L);
           } else {
             // the plain (FP64) kernel divides by 3 as the reference does; the
             // FP32-flux kernels multiply by the rounded 1/3 (one ulp apart)
-            const double sum = ld_stream_rw(a.q0 + e) + 2.0 * (((kExactRing && a.qp_is_src) ? qin : ld_stream(a.qp + e)) - L);
+            const double sum = a.q0[e] + 2.0 * (((kExactRing && a.qp_is_src) ? qin : __ldg(a.qp + e)) - L);
             q[n] = kExactRing ? sum / 3.0 : sum * (1.0 / 3.0);
           }
         }
@@ -754,25 +680,6 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
     for (int n = 0; n < NEQ; ++n) fkm[n] = fkp[n];
 #pragma unroll
     for (int m = 0; m < 3; ++m) za[m] = zb[m];
-  }
-
-  // fused boundary conditions, after the sweep so that their registers do not
-  // add to the flux rounds': the threads of the columns next to an i face
-  // read back every plane they wrote, the others the planes next to a k face
-  if (MODE != 0 && !VISC && a.fuse_bc && col_valid) {
-    auto apply = [&](int k) {
-      const long o = node_off(d, ci, cj, k);
-      double q[NEQ];
-#pragma unroll
-      for (int n = 0; n < NEQ; ++n) q[n] = a.out[n * VOL + o];  // this thread's own stores
-      fused_bc(a, ci, cj, k, q, smax, snan);
-    };
-    if (ci == 1 || ci == d.IM - 2) {
-      for (int k = kb; k < ke; ++k) apply(k);
-    } else {
-      if (kb == 1) apply(1);
-      if (ke == d.KM - 1 && d.KM - 2 != 1) apply(d.KM - 2);
-    }
   }
 
   if constexpr (kTma || kTma64) {

@@ -38,9 +38,6 @@ struct StageArgs {
   int ntile_i, ntile_j, kchunk;
   int visdiv;          // CBNS_VISDIV_*
   int sigma;           // accumulate the interior spectral-radius max (inviscid stage 3)
-  int fuse_bc;         // apply the reference's boundary conditions of an inviscid block without wake
-                       // cut or wall to the output (i faces, k faces; bc_fusable in abi.cu)
-  double p_inf;        // fuse_bc: the pressure the i faces reset to
 };
 
 // Many blocks in one launch (a persistent work queue): args[b] are the

@@ -76,8 +76,7 @@ __device__ __forceinline__ void prologue_body(StepState* st, double CFL) {
     st->done = 1;
     return;
   }
-  const unsigned long long bits = st->sigma_bits > st->sigma_fixed ? st->sigma_bits : st->sigma_fixed;
-  const double smax = __longlong_as_double((long long)bits);
+  const double smax = __longlong_as_double((long long)st->sigma_bits);
   double dt = CFL / smax;
   if (dt != dt) {  // calc_dt throws on NaN (src/calc_dt.cu:56-58)
     st->nan_dt = 1;

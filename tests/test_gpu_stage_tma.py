@@ -59,8 +59,11 @@ def test_fp64_tma_variant_equals_synchronous(name):
         out.append((r0, b.get_conservative(), t))
         b.close()
     (ra, qa, ta), (rb, qb, tb) = out
-    assert np.all(np.isfinite(qa))
-    assert np.array_equal(ra, rb)
+    assert np.all(np.isfinite(qa)) and np.all(np.isfinite(qb))
+    d = np.flatnonzero(ra != rb)
+    detail = (f"{d.size} of {ra.size} right-hand-side values differ; max relative difference "
+              f"{np.max(np.abs(ra - rb)) / np.max(np.abs(ra)):.3e}; first {d[:8].tolist()}")
+    assert np.array_equal(ra, rb), detail
     assert np.array_equal(qa, qb)
     assert ta == tb
 

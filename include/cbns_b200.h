@@ -372,7 +372,8 @@ int cbns_batch_run_async(cbns_batch* batch, unsigned nsteps, double t_end);
 int cbns_autotune(cbns_ctx* ctx, int* chosen);
 /* Use compiled variant `variant` of the stage kernel (0 .. count-1; count from
  * *count when not null, variant -1 only queries it).  FP64: 0 stages each
- * plane synchronously, 1 by TMA (the same arithmetic, bit for bit); FP32:
+ * plane synchronously, 1 by TMA (the same arithmetic, to the rounding of a
+ * separate compilation); FP32:
  * 2 + variant CTAs per SM.  No counterpart in the reference. */
 int cbns_stage_variant(cbns_ctx* ctx, int variant, int* count);
 

@@ -94,6 +94,21 @@ def args():
     return ap.parse_args()
 
 
+def replica_max(x, dist, torch, device):
+    """The maximum of x over the ranks of the process group (x itself without one)."""
+    if not dist:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(n_updates_per_step, steps, ms_max, world):
+    """Whole-job cell-updates/s of `world` replicas, each advancing its own block
+    of n_updates_per_step by `steps` steps, timed by the slowest rank (ms_max)."""
+    return world * n_updates_per_step * steps / (ms_max / 1e3)
+
+
 def make_case(name, size):
     from cbns3d_cuda_b200 import cases
     if name == "shock_vortex":
@@ -390,25 +405,21 @@ def run_ours(a):
     l2_h, linf_h = err(rh)
 
     def reduce_max(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(x, dist, torch, "cuda")
 
     ms32, ms64, msh = reduce_max(ms32), reduce_max(ms64), reduce_max(msh)
-    value = world * N * K / (msh / 1e3)
-    value32 = world * N * K / (ms32 / 1e3)
-    value64 = world * N * K / (ms64 / 1e3)
+    value = replica_throughput(N, K, msh, world)
+    value32 = replica_throughput(N, K, ms32, world)
+    value64 = replica_throughput(N, K, ms64, world)
 
     e2e = e2e64 = None
     if not a.no_e2e:
         ems, eb = e2e_pass(case, K, torch, PREC_HYBRID)
         ems = reduce_max(ems)
-        e2e = {"value": world * N * K / (ems / 1e3), "unit": "cell-updates/s", **eb}
+        e2e = {"value": replica_throughput(N, K, ems, world), "unit": "cell-updates/s", **eb}
         ems, eb = e2e_pass(case, K, torch, PREC_FP64)
         ems = reduce_max(ems)
-        e2e64 = {"value": world * N * K / (ems / 1e3), "unit": "cell-updates/s", **eb}
+        e2e64 = {"value": replica_throughput(N, K, ems, world), "unit": "cell-updates/s", **eb}
 
     peak, peak_kind = measured_peaks()
     fp64_peak = fp64_peak_tflops(torch)

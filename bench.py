@@ -21,6 +21,10 @@ step; N_upd = (IM-2)(JM-2)(KM-2).
           and downloaded after the K steps inside the timed region; the same
           for the plain FP64 path under paths.fp64.e2e (the precision-matched
           end-to-end figure).
+  paths.batch  the batched-blocks workload on the same GPU: 64 independent
+          viscous blocks of uneven size (seeded draw), learned-sensor hybrid,
+          one persistent stage launch per RK stage, per-block dt, W + K steps
+          (--case batch runs it alone, beside the blocks stepped one by one).
   plain_vs_reference_linf  the plain FP64 path's state after the W + K steps
           against the reference's own CUDA build run on the same files for the
           same steps (largest relative L-inf over the five variables).
@@ -88,6 +92,7 @@ def args():
                     help="run each path from the initial state to the case's end time (precision-form runs)")
     ap.add_argument("--t-end", type=float, default=None, help="--to-tend: end time (default: the case's)")
     ap.add_argument("--max-steps", type=int, default=100000, help="--to-tend: step limit")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-blocks pass of the default line")
     ap.add_argument("--no-reference-check", action="store_true",
                     help="skip the plain path's comparison with the reference build")
     ap.add_argument("--sensor", default=str(ROOT / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz"))
@@ -435,6 +440,15 @@ def run_ours(a):
     ach64 = alg_per_launch / st64_launch_s / 1e9 if st64_n else None
     tfl64 = FP64_FLOP_PER_UPDATE / 3.0 * N / st64_launch_s / 1e12 if st64_n else None
 
+    # the batched-blocks workload on this GPU (64 viscous blocks, hybrid)
+    batch = None
+    if not a.no_batch:
+        batch = batch_pass(a.blocks, K, W, torch, one_by_one=False)
+        batch.pop("shapes")
+        bms = reduce_max(batch["ms_per_step"] * K)
+        batch["ms_per_step"] = bms / K
+        batch["value"] = replica_throughput(batch["cell_updates_per_step"], K, bms, world)
+
     # the plain path against the reference's own build after the same W + K
     # steps of the same case: relative L-inf per conservative variable
     ref_cmp = None
@@ -488,6 +502,7 @@ def run_ours(a):
                                  "audit_faces": stats["audit_faces"], "audit_max_rel_diff": stats["audit_max"],
                                  "sensor_timeouts": stats["sensor_fail"], "stage_variant": varianth,
                                  "kernels": kern_ms(kernh)},
+                      "batch": batch,
                       "hybrid_over_fp64": value / value64, "hybrid_over_split": value / value32},
             "e2e": e2e,
             "gpu_launches": launches,
@@ -686,18 +701,15 @@ def run_naca(a):
         "stable": ok, "history": history, "kernels": kern, "clocks": clk.summary()}))
 
 
-def run_batch(a):
-    """Batched-blocks workload: independent viscous blocks of uneven size (seeded draw),
-    learned-sensor hybrid, advanced by one persistent work-queue launch of the
-    stage kernel per RK stage (cbns_batch_run) with per-block dt; beside it the
-    same blocks stepped one after the other on the same stream (one CUDA graph
-    per block).  Both timed with CUDA events on that stream."""
-    import torch
+def batch_pass(nblocks, K, W, torch, one_by_one=True, clocks=None):
+    """The batched-blocks workload: independent viscous blocks of uneven size
+    (seeded draw), learned-sensor hybrid, advanced by one persistent
+    work-queue launch of the stage kernel per RK stage (cbns_batch_run) with
+    per-block dt; optionally beside it the same blocks stepped one after the
+    other on the same stream (one CUDA graph per block).  Both timed with CUDA
+    events on that stream.  Returns a dict."""
     from cbns3d_cuda_b200 import CBNS_Q, PREC_HYBRID, Batch, Block, cases, make_params
-    torch.cuda.set_device(0)
-    load_sensor(a.sensor)
-    cs, draw = cases.case_batch(a.blocks, seed=0)
-    K, W = a.steps, a.warmup
+    cs, draw = cases.case_batch(nblocks, seed=0)
     N = sum((c.shape[0] - 2) * (c.shape[1] - 2) * (c.shape[2] - 2) for c in cs)
 
     def make():
@@ -728,40 +740,54 @@ def run_batch(a):
     blocks = make()
     bt = Batch(blocks, stream.cuda_stream)
     bt.run(W)
-    clk = Clocks(0)
-    clk.__enter__()
+    if clocks:
+        clocks.__enter__()
     ms_batch = timed(lambda: bt.run_async(K))
-    clk.__exit__(None, None, None)
-    clocks = clk.summary()
+    if clocks:
+        clocks.__exit__(None, None, None)
     bt.close()
     for b in blocks:
         b.close()
-    blocks = make()
-    for b in blocks:
-        b.set_stream(stream.cuda_stream)
-        b.run(W)
-
-    def one_by_one():
+    out = {"value": N * K / (ms_batch / 1e3), "ms_per_step": ms_batch / K, "steps": K, "blocks": len(cs),
+           "cell_updates_per_step": N, "shapes": [d["shape"] for d in draw],
+           "workload": f"batched blocks: {len(cs)} viscous blocks, sizes 32^3..128x64x64 (seed 0), Mach U[0.3,2], "
+                       "Re U[1e3,1e5], far-field boundaries, learned-sensor hybrid, per-block dt"}
+    if one_by_one:
+        blocks = make()
         for b in blocks:
-            b.run_async(K)
+            b.set_stream(stream.cuda_stream)
+            b.run(W)
 
-    ms_alone = timed(one_by_one)
-    for b in blocks:
-        b.close()
-    value = N * K / (ms_batch / 1e3)
+        def alone():
+            for b in blocks:
+                b.run_async(K)
+
+        ms_alone = timed(alone)
+        for b in blocks:
+            b.close()
+        out["blocks_one_by_one"] = {"value": N * K / (ms_alone / 1e3), "ms_per_step": ms_alone / K}
+        out["batch_over_one_by_one"] = ms_alone / ms_batch
+    return out
+
+
+def run_batch(a):
+    """The batched-blocks workload alone, as its own bench line (batch_pass)."""
+    import torch
+    torch.cuda.set_device(0)
+    load_sensor(a.sensor)
+    clk = Clocks(0)
+    r = batch_pass(a.blocks, a.steps, a.warmup, torch, one_by_one=True, clocks=clk)
     print(json.dumps({
         "metric": "cell-updates/s: learned-hybrid FP32 vs plain FP64 WENO5, same B200, rho-L2<=1e-5",
-        "value": value, "unit": "cell-updates/s", "n_gpus": 1, "steps": K, "warmup": W,
-        "ms_per_step": ms_batch / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "value": r["value"], "unit": "cell-updates/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 flux / f64 state", "data": "synthetic",
-        "config": {"workload": f"batched blocks: {len(cs)} viscous blocks, sizes 32^3..128x64x64 (seed 0), "
-                               "Mach U[0.3,2], Re U[1e3,1e5], far-field boundaries, learned-sensor hybrid, per-block dt",
-                   "cell_updates_per_step": N, "blocks": len(cs),
-                   "shapes": [d["shape"] for d in draw]},
-        "paths": {"batch": {"value": value, "ms_per_step": ms_batch / K},
-                  "blocks_one_by_one": {"value": N * K / (ms_alone / 1e3), "ms_per_step": ms_alone / K},
-                  "batch_over_one_by_one": ms_alone / ms_batch},
-        "clocks": clocks,
+        "config": {"workload": r["workload"], "cell_updates_per_step": r["cell_updates_per_step"],
+                   "blocks": r["blocks"], "shapes": r["shapes"]},
+        "paths": {"batch": {"value": r["value"], "ms_per_step": r["ms_per_step"]},
+                  "blocks_one_by_one": r["blocks_one_by_one"],
+                  "batch_over_one_by_one": r["batch_over_one_by_one"]},
+        "clocks": clk.summary(),
     }))
 
 

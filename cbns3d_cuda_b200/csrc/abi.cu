@@ -235,6 +235,8 @@ ViscArgs visc_args(cbns_ctx* c, bool check_done, bool sigma) {
   for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
   fill_met(c, a.met);
   for (int m = 0; m < 12; ++m) a.vflux[m] = c->f.vflux[m];
+  for (int m = 0; m < 4; ++m) a.dfv[m] = c->f.dfv[m];
+  a.visdiv = c->ph.visdiv;
   a.mu = c->f.prim[6];
   a.st = c->st;
   a.check_done = check_done;
@@ -255,7 +257,7 @@ StageArgs stage_args(cbns_ctx* c, const double* src, const double* q0, const dou
   a.out = out;
   fill_met(c, a.met);
   for (int m = 0; m < 10; ++m) a.area[m] = c->f.area[m];
-  for (int m = 0; m < 12; ++m) a.vflux[m] = c->f.vflux[m];
+  for (int m = 0; m < 4; ++m) a.dfv[m] = c->f.dfv[m];
   for (int m = 0; m < 6; ++m) a.prim[m] = c->f.prim[m];
   a.st = c->st;
   a.q0_is_src = q0 == src;
@@ -297,7 +299,7 @@ int bc_launch(cbns_ctx* c, const BCArgs& a, bool interior_prims) {
 int visc_launch(cbns_ctx* c, const ViscArgs& a) {
   Prof p(c, PK_VISC);
   CK(launch_visc(a, c->stream));
-  c->launches += 1;
+  c->launches += 2;  // node fluxes, their divergence
   return CBNS_OK;
 }
 
@@ -539,7 +541,8 @@ struct cbns_batch {
   ViscArgs* visc_tab = nullptr;      // 3 stages x nblocks
   int* bc_cta = nullptr;             // nblocks + 1
   int* visc_cta = nullptr;           // nblocks + 1
-  int bc_total = 0, visc_total = 0;
+  int* div_cta = nullptr;            // nblocks + 1 (the divergence kernel's CTAs)
+  int bc_total = 0, visc_total = 0, div_total = 0;
   std::vector<int> roles;     // (lq, lp, ls) per block at capture
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -590,7 +593,7 @@ int batch_tables(cbns_batch* b) {
   std::vector<double> cfl(nb);
   std::vector<BCArgs> bct(3 * nb);
   std::vector<ViscArgs> vt(3 * nb);
-  std::vector<int> bcc(nb + 1, 0), vc(nb + 1, 0);
+  std::vector<int> bcc(nb + 1, 0), vc(nb + 1, 0), dc(nb + 1, 0);
   for (int i = 0; i < nb; ++i) {
     cbns_ctx* c = b->blk[i];
     sts[i] = c->st;
@@ -602,9 +605,11 @@ int batch_tables(cbns_batch* b) {
     }
     bcc[i + 1] = bcc[i] + bc_farfield_ctas(c->d);
     vc[i + 1] = vc[i] + (b->visc ? visc_ctas(c->d) : 0);
+    dc[i + 1] = dc[i] + (b->visc ? visc_div_ctas(c->d) : 0);
   }
   b->bc_total = bcc[nb];
   b->visc_total = vc[nb];
+  b->div_total = dc[nb];
   CK(cudaMemcpyAsync(b->st_tab, sts.data(), nb * sizeof(StepState*), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->cfl_tab, cfl.data(), nb * sizeof(double), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->bc_tab, bct.data(), bct.size() * sizeof(BCArgs), cudaMemcpyHostToDevice, b->stream));
@@ -612,6 +617,7 @@ int batch_tables(cbns_batch* b) {
     CK(cudaMemcpyAsync(b->visc_tab, vt.data(), vt.size() * sizeof(ViscArgs), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->bc_cta, bcc.data(), bcc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->visc_cta, vc.data(), vc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->div_cta, dc.data(), dc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaStreamSynchronize(b->stream));
   return CBNS_OK;
 }
@@ -681,8 +687,9 @@ int batch_enqueue_body(cbns_batch* b) {
         b->blk[0]->launches += 1;
       }
       if (b->visc) {
-        CK(launch_visc_batched(b->visc_tab + k * nb, b->visc_cta, nb, b->visc_total, b->stream));
-        b->blk[0]->launches += 1;
+        CK(launch_visc_batched(b->visc_tab + k * nb, b->visc_cta, nb, b->visc_total, b->div_cta, b->div_total,
+                               b->stream));
+        b->blk[0]->launches += 2;
       }
       if (!last) RET(batch_fork(b));
       continue;
@@ -853,8 +860,11 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   }
   for (int m = 0; m < 7 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.prim[m], d.VOL);
   for (int m = 0; m < 12; ++m) c->f.vflux[m] = nullptr;
-  if (p->viscous)
+  for (int m = 0; m < 4; ++m) c->f.dfv[m] = nullptr;
+  if (p->viscous) {
     for (int m = 0; m < 12 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.vflux[m], d.VOL);
+    for (int m = 0; m < 4 && rc == CBNS_OK; ++m) rc = dalloc(c, &c->f.dfv[m], d.VOL);
+  }
   const long NGt = (long)d.IG * d.JG * d.KG;
   c->staging_elems = (size_t)std::max(5 * NGt, 10L * d.IM * d.JM * d.KM);
   if (rc == CBNS_OK) rc = dalloc(c, &c->staging, c->staging_elems);
@@ -934,8 +944,10 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   for (int m = 0; m < 6; ++m)
     if (c->f.area32[m]) cudaMemsetAsync(c->f.area32[m], 0, d.VOL * sizeof(float), c->stream);
   for (int m = 0; m < 7; ++m) cudaMemsetAsync(c->f.prim[m], 0, d.VOL * sizeof(double), c->stream);
-  if (p->viscous)
+  if (p->viscous) {
     for (int m = 0; m < 12; ++m) cudaMemsetAsync(c->f.vflux[m], 0, d.VOL * sizeof(double), c->stream);
+    for (int m = 0; m < 4; ++m) cudaMemsetAsync(c->f.dfv[m], 0, d.VOL * sizeof(double), c->stream);
+  }
 
   stage_tiles(d, &c->ntile_i, &c->ntile_j);
   const int ntiles = c->ntile_i * c->ntile_j;
@@ -1132,7 +1144,8 @@ int cbns_calc_numerical_flux(cbns_ctx* c, int which) {
 
 int cbns_calc_viscous_flux_contribution(cbns_ctx* c) {
   RET(check_ready(c));
-  // the divergence of the node fluxes is taken inside the stage kernel
+  // the node fluxes and their divergence were formed by cbns_calc_viscous_terms
+  // (visc.cu); the stage kernel subtracts the divergence
   return CBNS_OK;
 }
 
@@ -1604,8 +1617,9 @@ int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, c
     auto up = [](size_t x) { return (x + 255) / 256 * 256; };
     const size_t o1 = up(nblocks * sizeof(StepState*)), o2 = o1 + up(nblocks * sizeof(double)),
                  o3 = o2 + up(3 * nblocks * sizeof(BCArgs)), o4 = o3 + up(3 * nblocks * sizeof(ViscArgs)),
-                 o5 = o4 + up((nblocks + 1) * sizeof(int)), o6 = o5 + up((nblocks + 1) * sizeof(int));
-    e = cudaMalloc(&b->tables, o6);
+                 o5 = o4 + up((nblocks + 1) * sizeof(int)), o6 = o5 + up((nblocks + 1) * sizeof(int)),
+                 o7 = o6 + up((nblocks + 1) * sizeof(int));
+    e = cudaMalloc(&b->tables, o7);
     if (e == cudaSuccess) {
       char* t = static_cast<char*>(b->tables);
       b->st_tab = reinterpret_cast<StepState**>(t);
@@ -1614,6 +1628,7 @@ int cbns_batch_create(cbns_ctx* const* blocks, unsigned nblocks, void* stream, c
       b->visc_tab = reinterpret_cast<ViscArgs*>(t + o3);
       b->bc_cta = reinterpret_cast<int*>(t + o4);
       b->visc_cta = reinterpret_cast<int*>(t + o5);
+      b->div_cta = reinterpret_cast<int*>(t + o6);
     }
   }
   if (e == cudaSuccess) e = cudaMalloc(&b->counter, sizeof(unsigned));

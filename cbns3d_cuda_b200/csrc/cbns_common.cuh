@@ -49,6 +49,7 @@ struct Fields {
   float* area32[6];  // FP32 and hybrid contexts: J*grad(xi), J*grad(eta) rounded to FP32
   double* prim[7];   // rho, u, v, w, p, T, mu (viscous upkeep; on-demand otherwise)
   double* vflux[12]; // E0..E3, F0..F3, G0..G3 (viscous node fluxes, times J-scaled normals)
+  double* dfv[4];    // divergence of the viscous node fluxes at the interior nodes (momentum 3, energy)
 };
 
 // Per-run scalars kept on the device so a whole step can be replayed from a graph.

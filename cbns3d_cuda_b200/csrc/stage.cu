@@ -1,11 +1,11 @@
 // stage.cu - one SSP-RK3 stage in one kernel: inviscid WENO5-char/LF fluxes in
-// all three directions, their differences, the viscous divergence, division by
-// J and the Shu-Osher stage combination, for every interior node.
+// all three directions, their differences, the viscous divergence (formed
+// ahead of it by visc_div_kernel, visc.cu), division by J and the Shu-Osher
+// stage combination, for every interior node.
 //
 // Replaces, for one stage, the reference's
 //   calc_numerical_flux  (src/calc_numerical_flux.cu:15-74; three face kernels
 //                         writing Ep/Fp/Gp to HBM)
-//   viscous_contribution_kernel (src/viscous_contribution_kernel.cu:13-71)
 //   update_rk3 / rk3_kernel     (src/time_integration.cu:15-40,
 //                                src/runge_kutta_kernel.cu:13-80)
 // and, in stage 3 of an inviscid step, the per-node half of calc_dt
@@ -144,12 +144,6 @@ __host__ __device__ constexpr size_t stage_smem() {
   return (TMA && sizeof(R) == 4)   ? round_to(sizeof(Smem<R, R>), 16) + 128 + sizeof(TmaSmem)
          : (TMA && sizeof(R) == 8) ? 128 + round_to(sizeof(Smem<R, R, 24>), 128) + sizeof(TmaSmem64)
                                    : round_to(sizeof(Smem<R, R>), 16) + sizeof(AreaSync<R>);
-}
-
-// 4th-order central derivative of a node field along a stride, at offset o.
-__device__ __forceinline__ double d4(const double* f, long o, long s) {
-  return (1.0 / 12.0) * __ldg(f + o - 2 * s) - (2.0 / 3.0) * __ldg(f + o - s) + (2.0 / 3.0) * __ldg(f + o + s) -
-         (1.0 / 12.0) * __ldg(f + o + 2 * s);
 }
 
 // NB = CTAs per SM the register budget is cut for: FP64 always 2 (shared
@@ -428,22 +422,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
         if (k + 1 < ke) mnext = mask_bits(k + 1);
       }
     }
-    // viscous kernels ask L2 for the node fluxes the next plane's divergence
-    // reads (the column's own lines of all twelve arrays at plane k+1, and of
-    // the k-direction arrays at the stencil's leading plane k+3; the tile's
-    // other columns cover the neighbouring rows): the divergence's 48 loads
-    // per node then hit L2 instead of waiting for DRAM
+    // viscous kernels ask L2 for the next plane's viscous divergence
     if (VISC && MODE != 0 && col_valid && k + 1 < ke) {
       const long o = node_off(d, ci, cj, k + 1);
-      const long sh = a.visdiv == 0 ? 1 : 0;
-      const long oi = o - sh * (d.PX + d.PL), oj = o - sh * (1 + d.PL), ok = o - sh * (1 + d.PX);
 #pragma unroll
-      for (int n = 0; n < 4; ++n) {
-        prefetch_l2(a.vflux[n] + oi);
-        prefetch_l2(a.vflux[4 + n] + oj);
-        prefetch_l2(a.vflux[8 + n] + ok);
-        prefetch_l2(a.vflux[8 + n] + ok + 2 * d.PL);
-      }
+      for (int n = 0; n < 4; ++n) prefetch_l2(a.dfv[n] + o);
     }
     // the FP32 kernels ask L2 for the next plane's RK operands and 1/J now, so
     // the update's loads one plane later find them there
@@ -613,15 +596,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
         df[n] = (double)(sm.fi[n][cy][cx + 1] - sm.fi[n][cy][cx]) + (double)(sm.fj[n][cy + 1][cx] - sm.fj[n][cy][cx]) +
                 (double)(fkp[n] - fkm[n]);
       if (VISC) {
-        // viscous divergence; the reference takes the i-derivative at (i,j-1,k-1),
-        // the j-derivative at (i-1,j,k-1), the k-derivative at (i-1,j-1,k)
-        const long sh = a.visdiv == 0 ? 1 : 0;
-        const long oi = o - sh * (d.PX + d.PL), oj = o - sh * (1 + d.PL), ok = o - sh * (1 + d.PX);
+        // the viscous flux divergence, formed by visc_div_kernel (visc.cu)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) {
-          const double dv = d4(a.vflux[n], oi, 1) + d4(a.vflux[4 + n], oj, d.PX) + d4(a.vflux[8 + n], ok, d.PL);
-          df[n + 1] -= dv;
-        }
+        for (int n = 0; n < 4; ++n) df[n + 1] -= __ldg(a.dfv[n] + o);
       }
       const double iJ = (kEarly && MODE != 0) ? piJ : __ldg(a.area[9] + o);
       if (MODE == 0) {

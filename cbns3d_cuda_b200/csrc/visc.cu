@@ -10,10 +10,15 @@
 // 4th-order stencils (biased at the second layer of the ghosted box), the
 // Sutherland viscosity, the stress tensor and heat flux, and the three node
 // fluxes E_v, F_v, G_v (momentum and energy components, normals J*grad(xi)).
-// None of the 12 gradients, 6 stresses or 3 heat fluxes go to HBM; the
-// divergence of the node fluxes is taken inside the stage kernel.  In stage 3 of
-// a step (and at start-up) it also forms the viscous spectral radius of every
+// None of the 12 gradients, 6 stresses or 3 heat fluxes go to HBM.  In stage 3
+// of a step (and at start-up) it also forms the viscous spectral radius of every
 // grid node for the next time step (src/time_step_kernel.cu:13-96).
+// A second kernel, visc_div_kernel, takes the 4th-order divergence of the node
+// fluxes at every interior node (the other half of calc_viscous_flux_contribution,
+// viscous_contribution_kernel, src/viscous_contribution_kernel.cu:13-71) into
+// four arrays, which the stage kernel reads with one coalesced load each: the
+// 48-point stencil runs in a streaming kernel of its own instead of in the
+// stage kernel's latency-bound update.
 #include "visc.cuh"
 
 namespace cbns {
@@ -114,6 +119,48 @@ __device__ __forceinline__ void visc_node_body(const ViscArgs& a, long e) {
   }
 }
 
+// 4th-order central derivative of a node field along a stride, at offset o.
+__device__ __forceinline__ double d4(const double* f, long o, long s) {
+  return (1.0 / 12.0) * __ldg(f + o - 2 * s) - (2.0 / 3.0) * __ldg(f + o - s) + (2.0 / 3.0) * __ldg(f + o + s) -
+         (1.0 / 12.0) * __ldg(f + o + 2 * s);
+}
+
+// Interior node e (i fastest): the divergence of the node fluxes; the
+// reference takes the i-derivative at (i,j-1,k-1), the j-derivative at
+// (i-1,j,k-1), the k-derivative at (i-1,j-1,k) (CBNS_VISDIV_REFERENCE), or
+// all three at the node (CBNS_VISDIV_CENTERED).
+__device__ __forceinline__ void visc_div_body(const ViscArgs& a, long e) {
+  const Dims& d = a.d;
+  const int NI = d.IM - 2, NJ = d.JM - 2;
+  if (e >= (long)NI * NJ * (d.KM - 2)) return;
+  const int i = 1 + (int)(e % NI);
+  const long r = e / NI;
+  const int j = 1 + (int)(r % NJ), k = 1 + (int)(r / NJ);
+  const long o = node_off(d, i, j, k);
+  const long sh = a.visdiv == 0 ? 1 : 0;
+  const long oi = o - sh * (d.PX + d.PL), oj = o - sh * (1 + d.PL), ok = o - sh * (1 + d.PX);
+#pragma unroll
+  for (int n = 0; n < 4; ++n)
+    a.dfv[n][o] = d4(a.vflux[n], oi, 1) + d4(a.vflux[4 + n], oj, d.PX) + d4(a.vflux[8 + n], ok, d.PL);
+}
+
+__global__ void __launch_bounds__(256) visc_div_kernel(const ViscArgs a) {
+  if (a.check_done && a.st->done) return;
+  visc_div_body(a, blockIdx.x * (long)blockDim.x + threadIdx.x);
+}
+
+__global__ void __launch_bounds__(256) visc_div_batched(const ViscArgs* args, const int* cta, int nblocks) {
+  int lo = 0, hi = nblocks - 1;  // the last b with cta[b] <= blockIdx.x
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(cta + mid) <= (int)blockIdx.x) lo = mid;
+    else hi = mid - 1;
+  }
+  const ViscArgs& a = args[lo];
+  if (a.check_done && a.st->done) return;
+  visc_div_body(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);
+}
+
 __global__ void __launch_bounds__(128) visc_node_kernel(const ViscArgs a) {
   if (a.check_done && a.st->done) return;
   visc_node_body(a, blockIdx.x * (long)blockDim.x + threadIdx.x);
@@ -137,7 +184,13 @@ __global__ void __launch_bounds__(128) visc_node_batched(const ViscArgs* args, c
 
 cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s) {
   visc_node_kernel<<<visc_ctas(a.d), 128, 0, s>>>(a);
+  visc_div_kernel<<<visc_div_ctas(a.d), 256, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+int visc_div_ctas(const Dims& d) {
+  const long n = (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 2);
+  return (int)((n + 255) / 256);
 }
 
 int visc_ctas(const Dims& d) {
@@ -145,9 +198,11 @@ int visc_ctas(const Dims& d) {
   return (int)((n + 127) / 128);
 }
 
-cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas, cudaStream_t s) {
+cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas,
+                                const int* dcta, int dtotal, cudaStream_t s) {
   if (total_ctas <= 0) return cudaSuccess;
   visc_node_batched<<<total_ctas, 128, 0, s>>>(args, cta, nblocks);
+  visc_div_batched<<<dtotal, 256, 0, s>>>(args, dcta, nblocks);
   return cudaGetLastError();
 }
 

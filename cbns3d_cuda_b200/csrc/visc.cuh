@@ -13,16 +13,22 @@ struct ViscArgs {
   const double* prim[6];     // rho,u,v,w,p,T
   const double* met[10];
   double* vflux[12];         // E0..E3, F0..F3, G0..G3
+  double* dfv[4];            // their divergence at the interior nodes
+  int visdiv;                // CBNS_VISDIV_*
   double* mu;
   StepState* st;
   int check_done;
   int sigma;                 // accumulate the spectral-radius max over the grid nodes
 };
 
+// The node fluxes, then their divergence (two kernels).
 cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s);
 // The same for many blocks in one launch: args and cta are device tables,
 // block b owning CTAs cta[b] .. cta[b+1]-1, cta[b+1] - cta[b] = visc_ctas(its Dims).
 int visc_ctas(const Dims& d);
-cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas, cudaStream_t s);
+// The divergence kernel's CTAs for one block (cta tables of the batched divergence launch).
+int visc_div_ctas(const Dims& d);
+cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas,
+                                const int* dcta, int dtotal, cudaStream_t s);
 
 }  // namespace cbns

@@ -377,11 +377,13 @@ int cbns_autotune(cbns_ctx* ctx, int* chosen);
  * 2 + variant CTAs per SM.  No counterpart in the reference. */
 int cbns_stage_variant(cbns_ctx* ctx, int variant, int* count);
 
-/* Per-kernel device timing with CUDA events on the launch stream.  Kernel ids:
- * 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous node
- * fluxes, 3 dt/step bookkeeping, 4 hybrid sensor network, 5 hybrid audit,
- * 6 hybrid WENO5 faces (the per-step list and the per-stage evaluation).
- * total_ms is the summed event time. */
+/* Per-kernel-group device timing with CUDA events on the launch stream.  Group
+ * ids: 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous
+ * (node fluxes and their divergence), 3 dt/step bookkeeping, 4 hybrid sensor
+ * network, 5 hybrid audit, 6 hybrid WENO5 faces (the per-step list and the
+ * per-stage evaluation).  total_ms is the summed event time; *launches counts
+ * the timed groups (one group can be several kernel launches, e.g. the three
+ * ordered boundary launches); cbns_launch_count counts kernels. */
 int cbns_prof_enable(cbns_ctx* ctx, int on);
 int cbns_prof_read(cbns_ctx* ctx, int kernel_id, double* total_ms, unsigned* launches);
 int cbns_prof_reset(cbns_ctx* ctx);

@@ -241,6 +241,7 @@ ViscArgs visc_args(cbns_ctx* c, bool check_done, bool sigma) {
   a.st = c->st;
   a.check_done = check_done;
   a.sigma = sigma;
+  a.kc = visc_kchunk(c->d, c->nsm);
   return a;
 }
 
@@ -349,18 +350,20 @@ void drop_graph(cbns_ctx* c) {
   c->graph = nullptr;
 }
 
-// The hybrid flux's decisions for the state q: the sensor network on every
-// face (tensor cores), then the audit of a rotating sample of its linear-flux
-// faces against WENO5 (which forces WENO5 for the step on a violation).
-// every_step: evaluate the network now instead of on every sensor_every-th
-// step of a run; widen: widening interval (0: that of the evaluation
-// schedule).  hold: the per-call path's steps between evaluations — only the
-// audit and the WENO5-face count run, the decisions (and their list) stand.
-int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step = false, unsigned widen = 0,
-                  bool hold = false) {
+// The arguments of one context's sensor kernels (sensor_launch, and the
+// batched launches of a batch).
+struct SensorSet {
+  MaskArgs m;
+  DilateArgs w[3];  // widening in i, j, k: raw -> mask -> raw -> mask
+  AuditArgs au;
+  ListArgs li;
+};
+
+SensorSet sensor_set(cbns_ctx* c, const double* q, bool check_done, bool every_step, unsigned widen, bool hold) {
   const unsigned every = every_step ? 1u : c->sensor_every;
   const unsigned wn = widen ? widen : every;
-  MaskArgs m;
+  SensorSet ss;
+  MaskArgs& m = ss.m;
   m.d = c->d;
   m.gamma = (float)c->ph.gamma;
   m.gam1 = (float)c->ph.gam1;
@@ -372,33 +375,22 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step
   m.mask = c->mask_raw;
   m.st = c->st;
   m.check_done = check_done;
-  int n = 0;
-  {
-    Prof p(c, PK_SENSOR);
-    if (!hold) {
-      CK(launch_sensor_mask(m, c->stream));
-      n += 2;
-    }
-    // widening in i, j, k: raw -> mask -> raw -> mask (held: the count only)
-    unsigned char* bufs[4] = {c->mask_raw, c->mask, c->mask_raw, c->mask};
-    for (int dim = hold ? 2 : 0; dim < 3; ++dim) {
-      DilateArgs w;
-      w.d = c->d;
-      w.in = bufs[dim];
-      w.out = bufs[dim + 1];
-      w.dim = dim;
-      w.along = 1 + (int)wn;
-      w.across = (int)wn;
-      w.st = c->st;
-      w.count = dim == 2;
-      w.every = every;
-      w.hold = hold;
-      w.check_done = check_done;
-      CK(launch_sensor_dilate(w, c->stream));
-      n += 1;
-    }
+  unsigned char* bufs[4] = {c->mask_raw, c->mask, c->mask_raw, c->mask};
+  for (int dim = 0; dim < 3; ++dim) {
+    DilateArgs& w = ss.w[dim];
+    w.d = c->d;
+    w.in = bufs[dim];
+    w.out = bufs[dim + 1];
+    w.dim = dim;
+    w.along = 1 + (int)wn;
+    w.across = (int)wn;
+    w.st = c->st;
+    w.count = dim == 2;
+    w.every = every;
+    w.hold = hold;
+    w.check_done = check_done;
   }
-  AuditArgs a;
+  AuditArgs& a = ss.au;
   a.d = c->d;
   a.gamma = (float)c->ph.gamma;
   a.gam1 = (float)c->ph.gam1;
@@ -410,9 +402,42 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step
   a.bound = c->audit_bound;
   a.st = c->st;
   a.check_done = check_done;
+  ListArgs& l = ss.li;
+  l.d = c->d;
+  l.mask = c->mask;
+  l.nf = c->nfaces;
+  l.st = c->st;
+  l.list = c->wlist;
+  l.check_done = check_done;
+  return ss;
+}
+
+// The hybrid flux's decisions for the state q: the sensor network on every
+// face (tensor cores), then the audit of a rotating sample of its linear-flux
+// faces against WENO5 (which forces WENO5 for the step on a violation).
+// every_step: evaluate the network now instead of on every sensor_every-th
+// step of a run; widen: widening interval (0: that of the evaluation
+// schedule).  hold: the per-call path's steps between evaluations — only the
+// audit and the WENO5-face count run, the decisions (and their list) stand.
+int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step = false, unsigned widen = 0,
+                  bool hold = false) {
+  const SensorSet ss = sensor_set(c, q, check_done, every_step, widen, hold);
+  int n = 0;
+  {
+    Prof p(c, PK_SENSOR);
+    if (!hold) {
+      CK(launch_sensor_mask(ss.m, c->stream));
+      n += 2;
+    }
+    // widening (held: the count only)
+    for (int dim = hold ? 2 : 0; dim < 3; ++dim) {
+      CK(launch_sensor_dilate(ss.w[dim], c->stream));
+      n += 1;
+    }
+  }
   {
     Prof p(c, PK_AUDIT);
-    CK(launch_sensor_audit(a, c->stream));
+    CK(launch_sensor_audit(ss.au, c->stream));
   }
   n += 1;
   if (!hold) {
@@ -517,15 +542,16 @@ struct cbns_batch {
   cudaStream_t stream = nullptr;           // the caller's, or owned by the batch
   bool own_stream = false;
   std::vector<cudaStream_t> saved;         // the blocks' streams before the batch
-  // the blocks' own kernels (prologue, sensor, WENO5 faces, boundary, viscous)
-  // are captured on side streams, so the graph runs different blocks' small
-  // kernels side by side between the batched stage launches
+  // the blocks' own kernels (the sensor sweeps, widening, audit and WENO5-face
+  // lists; boundary and viscous kernels unless every block is far field) are
+  // captured on side streams, so the graph runs different blocks' small
+  // kernels side by side between the batched launches
   std::vector<cudaStream_t> side;
   cudaEvent_t ev_fork = nullptr;
   std::vector<cudaEvent_t> ev_join;
   bool visc = false, fp32 = false, hyb = false;
   StageArgs* args = nullptr;  // device: 3 stages x nblocks
-  std::vector<StageArgs> host_args;  // the same, on the host (hybrid: WENO5-face passes)
+  std::vector<StageArgs> host_args;  // the same, on the host (hybrid: the WENO5-face passes)
   int* start = nullptr;       // device: nblocks + 1
   unsigned* counter = nullptr;
   int total = 0;
@@ -543,6 +569,20 @@ struct cbns_batch {
   int* visc_cta = nullptr;           // nblocks + 1
   int* div_cta = nullptr;            // nblocks + 1 (the divergence kernel's CTAs)
   int bc_total = 0, visc_total = 0, div_total = 0;
+  // hybrid, every block with the same network: the sensor sweeps, widening
+  // passes, audits and WENO5-face lists of all blocks in one launch each
+  bool sensor_batched = false;
+  void* stables = nullptr;           // one allocation holding the tables below
+  MaskArgs* mask_tab = nullptr;      // nblocks
+  DilateArgs* dil_tab = nullptr;     // 3 passes x nblocks
+  AuditArgs* aud_tab = nullptr;      // nblocks
+  ListArgs* list_tab = nullptr;      // nblocks
+  int* dil_cta = nullptr;            // nblocks + 1
+  int* aud_cta = nullptr;            // nblocks + 1
+  int* list_cta = nullptr;           // nblocks + 1
+  long* ipre = nullptr;              // 2 x (nblocks + 1): sweep work items of the two kinds
+  int dil_total = 0, aud_total = 0, list_total = 0;
+  long items_total[2] = {0, 0};
   std::vector<int> roles;     // (lq, lp, ls) per block at capture
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
@@ -564,6 +604,76 @@ void batch_drop_graph(cbns_batch* b) {
   if (b->graph) cudaGraphDestroy(b->graph);
   b->gexec = nullptr;
   b->graph = nullptr;
+}
+
+// Hybrid batches whose blocks all carry the same network: the tables of the
+// batched sensor launches (for the fixed buffer roles, as batch_tables).
+// Otherwise the blocks' sensor kernels stay per block, on the side streams.
+int batch_sensor_tables(cbns_batch* b) {
+  const int nb = (int)b->blk.size();
+  b->sensor_batched = false;
+  if (!b->hyb) return CBNS_OK;
+  std::vector<float> p0(CBNS_SENSOR_NPARAM), pi(CBNS_SENSOR_NPARAM);
+  CK(cudaDeviceSynchronize());  // the blocks' weight uploads, on whatever streams they were issued
+  for (int i = 0; i < nb; ++i) {
+    if (!b->blk[i]->sensor_params) return CBNS_OK;
+    CK(cudaMemcpy(i ? pi.data() : p0.data(), b->blk[i]->sensor_params, CBNS_SENSOR_NPARAM * sizeof(float),
+                  cudaMemcpyDeviceToHost));
+    if (i && std::memcmp(p0.data(), pi.data(), CBNS_SENSOR_NPARAM * sizeof(float)) != 0) return CBNS_OK;
+  }
+  if (!b->stables) {
+    auto up = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t o1 = up(nb * sizeof(MaskArgs)), o2 = o1 + up(3 * nb * sizeof(DilateArgs)),
+                 o3 = o2 + up(nb * sizeof(AuditArgs)), o4 = o3 + up(nb * sizeof(ListArgs)),
+                 o5 = o4 + up((nb + 1) * sizeof(int)), o6 = o5 + up((nb + 1) * sizeof(int)),
+                 o7 = o6 + up((nb + 1) * sizeof(int)), o8 = o7 + up(2 * (nb + 1) * sizeof(long));
+    CK(cudaMalloc(&b->stables, o8));
+    char* t = static_cast<char*>(b->stables);
+    b->mask_tab = reinterpret_cast<MaskArgs*>(t);
+    b->dil_tab = reinterpret_cast<DilateArgs*>(t + o1);
+    b->aud_tab = reinterpret_cast<AuditArgs*>(t + o2);
+    b->list_tab = reinterpret_cast<ListArgs*>(t + o3);
+    b->dil_cta = reinterpret_cast<int*>(t + o4);
+    b->aud_cta = reinterpret_cast<int*>(t + o5);
+    b->list_cta = reinterpret_cast<int*>(t + o6);
+    b->ipre = reinterpret_cast<long*>(t + o7);
+  }
+  std::vector<MaskArgs> mt(nb);
+  std::vector<DilateArgs> dt(3 * nb);
+  std::vector<AuditArgs> at(nb);
+  std::vector<ListArgs> lt(nb);
+  std::vector<int> dc(nb + 1, 0), ac(nb + 1, 0), lc(nb + 1, 0);
+  std::vector<long> ip(2 * (nb + 1), 0);
+  for (int i = 0; i < nb; ++i) {
+    cbns_ctx* c = b->blk[i];
+    const SensorSet ss = sensor_set(c, c->qb[c->lq], true, false, 0, false);
+    mt[i] = ss.m;
+    for (int dim = 0; dim < 3; ++dim) dt[dim * nb + i] = ss.w[dim];
+    at[i] = ss.au;
+    lt[i] = ss.li;
+    dc[i + 1] = dc[i] + sensor_dilate_ctas(c->d);
+    ac[i + 1] = ac[i] + sensor_audit_ctas(ss.au);
+    lc[i + 1] = lc[i] + weno_list_ctas(c->nfaces);
+    long n0, n1;
+    sensor_mask_items(c->d, &n0, &n1);
+    ip[i + 1] = ip[i] + n0;
+    ip[nb + 1 + i + 1] = ip[nb + 1 + i] + n1;
+  }
+  b->dil_total = dc[nb];
+  b->aud_total = ac[nb];
+  b->list_total = lc[nb];
+  b->items_total[0] = ip[nb];
+  b->items_total[1] = ip[2 * nb + 1];
+  CK(cudaMemcpyAsync(b->mask_tab, mt.data(), nb * sizeof(MaskArgs), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->dil_tab, dt.data(), 3 * nb * sizeof(DilateArgs), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->aud_tab, at.data(), nb * sizeof(AuditArgs), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->list_tab, lt.data(), nb * sizeof(ListArgs), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->dil_cta, dc.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->aud_cta, ac.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->list_cta, lc.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->ipre, ip.data(), 2 * (nb + 1) * sizeof(long), cudaMemcpyHostToDevice, b->stream));
+  b->sensor_batched = true;
+  return CBNS_OK;
 }
 
 // The StageArgs of the three stages of every block for the fixed buffer roles
@@ -604,7 +714,7 @@ int batch_tables(cbns_batch* b) {
       if (b->visc) vt[k * nb + i] = visc_args(c, true, k == 2);
     }
     bcc[i + 1] = bcc[i] + bc_farfield_ctas(c->d);
-    vc[i + 1] = vc[i] + (b->visc ? visc_ctas(c->d) : 0);
+    vc[i + 1] = vc[i] + (b->visc ? visc_ctas(vt[i]) : 0);
     dc[i + 1] = dc[i] + (b->visc ? visc_div_ctas(c->d) : 0);
   }
   b->bc_total = bcc[nb];
@@ -618,6 +728,7 @@ int batch_tables(cbns_batch* b) {
   CK(cudaMemcpyAsync(b->bc_cta, bcc.data(), bcc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->visc_cta, vc.data(), vc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->div_cta, dc.data(), dc.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  RET(batch_sensor_tables(b));
   CK(cudaStreamSynchronize(b->stream));
   return CBNS_OK;
 }
@@ -655,20 +766,42 @@ int batch_enqueue_body(cbns_batch* b) {
   // every block's prologue (own dt) in one launch
   CK(launch_step_prologue_batched(b->st_tab, b->cfl_tab, nb, b->stream));
   b->blk[0]->launches += 1;
-  RET(batch_fork(b));
-  for (int i = 0; i < nb; ++i) {
-    cbns_ctx* c = b->blk[i];
-    if (b->hyb) RET(sensor_launch(c, c->qb[c->lq], true));
+  bool forked = false;
+  if (b->hyb && b->sensor_batched) {
+    // every block's decisions: sweeps, widening, audit, WENO5-face list
+    CK(launch_sensor_mask_batched(b->mask_tab, b->ipre, b->ipre + nb + 1, b->items_total[0], b->items_total[1], nb,
+                                  b->stream));
+    for (int dim = 0; dim < 3; ++dim)
+      CK(launch_sensor_dilate_batched(b->dil_tab + dim * nb, b->dil_cta, nb, b->dil_total, b->stream));
+    CK(launch_sensor_audit_batched(b->aud_tab, b->aud_cta, nb, b->aud_total, b->stream));
+    CK(launch_weno_list_batched(b->list_tab, b->list_cta, nb, b->list_total, b->stream));
+    b->blk[0]->launches += 8;
+  } else if (b->hyb) {
+    RET(batch_fork(b));
+    forked = true;
+    for (int i = 0; i < nb; ++i) {
+      cbns_ctx* c = b->blk[i];
+      RET(sensor_launch(c, c->qb[c->lq], true));
+    }
   }
   for (int k = 0; k < 3; ++k) {
     const bool last = k == 2;
-    if (b->hyb)
+    if (forked) {
+      RET(batch_join(b));
+      forked = false;
+    }
+    if (b->hyb) {
+      // the blocks' WENO5-face passes side by side on the side streams: one
+      // launch over every block's list (tiles of one block per CTA, the
+      // StageArgs staged in shared memory) measured 1.9% slower per step
+      RET(batch_fork(b));
       for (int i = 0; i < nb; ++i) {
         CK(launch_weno_faces(b->host_args[k * nb + i], k + 1, b->blk[i]->nfaces, b->blk[i]->wlist,
                              b->blk[i]->stream));
         b->blk[i]->launches += 1;
       }
-    RET(batch_join(b));
+      RET(batch_join(b));
+    }
     CK(cudaMemsetAsync(b->counter, 0, sizeof(unsigned), b->stream));
     BatchStage bs;
     bs.args = b->args + k * nb;
@@ -691,18 +824,17 @@ int batch_enqueue_body(cbns_batch* b) {
                                b->stream));
         b->blk[0]->launches += 2;
       }
-      if (!last) RET(batch_fork(b));
       continue;
     }
     RET(batch_fork(b));
+    forked = true;
     for (cbns_ctx* c : b->blk) {
       double* out = k == 0 ? c->qb[c->ls] : (k == 1 ? c->qb[c->lp] : c->qb[c->lq]);
       RET(bc_launch(c, bc_args(c, out, true, last && !b->visc), false));
       if (b->visc) RET(visc_launch(c, visc_args(c, true, last)));
     }
   }
-  if (b->farfield) return CBNS_OK;  // the side streams were joined before the last stage
-  RET(batch_join(b));
+  if (forked) RET(batch_join(b));
   return CBNS_OK;
 }
 
@@ -1668,6 +1800,7 @@ int cbns_batch_destroy(cbns_batch* b) {
   cudaFree(b->start);
   cudaFree(b->counter);
   cudaFree(b->tables);
+  cudaFree(b->stables);
   batch_release_side(b);
   if (b->own_stream) cudaStreamDestroy(b->stream);
   delete b;

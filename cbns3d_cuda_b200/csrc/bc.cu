@@ -324,12 +324,7 @@ __global__ void bc_farfield(const BCArgs a) {
 // cta[b+1]-1 (so a warp's spectral-radius maximum stays within one block);
 // args[b] are its BCArgs.
 __global__ void bc_farfield_batched(const BCArgs* args, const int* cta, int nblocks) {
-  int lo = 0, hi = nblocks - 1;  // the last b with cta[b] <= blockIdx.x
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(cta + mid) <= (int)blockIdx.x) lo = mid;
-    else hi = mid - 1;
-  }
+  const int lo = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const BCArgs& a = args[lo];
   if (a.check_done && a.st->done) return;
   farfield_body(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);

@@ -71,6 +71,19 @@ struct StepState {
   int stage_fail;                 // a stage kernel's TMA wait timed out (the state is not valid)
 };
 
+// Batched launches of per-block kernels: block b of a batch owns the CTAs
+// cta[b] .. cta[b+1]-1 of the grid.  Returns the block of CTA x (the last b
+// with cta[b] <= x; blocks that own no CTA are never returned).
+__device__ __forceinline__ int block_of_cta(const int* cta, int nblocks, int x) {
+  int lo = 0, hi = nblocks - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(cta + mid) <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Positive doubles order like their bit patterns; a NaN (either sign) compares
 // above every finite value, so a max over bit patterns propagates NaN.
 __device__ inline void atomic_max_sigma(unsigned long long* a, double s) {

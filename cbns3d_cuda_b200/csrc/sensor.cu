@@ -207,22 +207,27 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float* __restrict__ 
 // Grid: x over the faces of a line along i, y over groups of DL lines along
 // j, z over (direction, k); no index division per face.
 constexpr int DL = 16;
-__global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) {
+__device__ __forceinline__ dim3 dilate_grid(const Dims& d) {
+  return dim3((unsigned)((d.IM - 1 + 127) / 128), (unsigned)((d.JM - 1 + DL - 1) / DL), (unsigned)(3 * (d.KM - 1)));
+}
+
+// CTA (bx, by, bz) of one block's widening grid
+__device__ __forceinline__ void dilate_body(const DilateArgs& a, unsigned bx, unsigned by, unsigned bz) {
   if (a.check_done && a.st->done) return;
   if (a.hold || !sensor_step(a.st, a.every)) {
     // decisions of an earlier step: only the statistics
     if (a.count) {
       const Dims& d = a.d;
-      const int dir = blockIdx.z / (d.KM - 1), x2 = blockIdx.z % (d.KM - 1);
+      const int dir = bz / (d.KM - 1), x2 = bz % (d.KM - 1);
       const int n0 = dir == 0 ? d.IM - 1 : d.IM - 2, n1 = dir == 1 ? d.JM - 1 : d.JM - 2;
       const int n2 = dir == 2 ? d.KM - 1 : d.KM - 2;
       const int first = dir == 0 ? 0 : (dir == 1 ? (d.IM - 1) * (d.JM - 2) * (d.KM - 2)
                                                  : (d.IM - 1) * (d.JM - 2) * (d.KM - 2) +
                                                        (d.IM - 2) * (d.JM - 1) * (d.KM - 2));
-      const int x0 = blockIdx.x * blockDim.x + threadIdx.x;
+      const int x0 = bx * 128 + threadIdx.x;
       unsigned cnt = 0;
       if (x2 < n2 && x0 < n0) {
-        const int y0 = blockIdx.y * DL, y1 = min(n1, y0 + DL);
+        const int y0 = by * DL, y1 = min(n1, y0 + DL);
         for (int x1 = y0; x1 < y1; ++x1) cnt += __ldg(a.out + first + x0 + n0 * (x1 + n1 * x2));
       }
 #pragma unroll
@@ -233,8 +238,8 @@ __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) 
   }
   const Dims& d = a.d;
   const int IM = d.IM, JM = d.JM, KM = d.KM;
-  const int dir = blockIdx.z / (KM - 1), x2 = blockIdx.z % (KM - 1);
-  const int x0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int dir = bz / (KM - 1), x2 = bz % (KM - 1);
+  const int x0 = bx * 128 + threadIdx.x;
   // extents (n0, n1, n2) and first index of this direction's faces
   const int n0 = dir == 0 ? IM - 1 : IM - 2, n1 = dir == 1 ? JM - 1 : JM - 2, n2 = dir == 2 ? KM - 1 : KM - 2;
   const int first = dir == 0 ? 0 : (dir == 1 ? (IM - 1) * (JM - 2) * (KM - 2)
@@ -247,7 +252,7 @@ __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) 
   unsigned cnt = 0;
   const unsigned char* __restrict__ in = a.in;
   unsigned char* __restrict__ out = a.out;
-  const int y0 = blockIdx.y * DL, y1 = min(n1, y0 + DL);
+  const int y0 = by * DL, y1 = min(n1, y0 + DL);
   if (valid) {
     // all lines' loads are independent: let them be in flight together
 #pragma unroll 4
@@ -268,15 +273,29 @@ __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) 
   }
 }
 
+__global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) {
+  dilate_body(a, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// Many blocks in one launch: block b owns CTAs cta[b] .. cta[b+1]-1, args[b]
+// are its DilateArgs.
+__global__ void __launch_bounds__(128) sensor_dilate_batched(const DilateArgs* args, const int* cta, int nblocks) {
+  const int b = block_of_cta(cta, nblocks, (int)blockIdx.x);
+  const DilateArgs& a = args[b];
+  const dim3 g = dilate_grid(a.d);
+  const unsigned l = blockIdx.x - (unsigned)__ldg(cta + b);
+  dilate_body(a, l % g.x, (l / g.x) % g.y, l / (g.x * g.y));
+}
+
 // ---------------------------------------------------------------- audit
-__global__ void __launch_bounds__(128) sensor_audit_kernel(const AuditArgs a) {
+__device__ __forceinline__ void audit_body(const AuditArgs& a, unsigned bx) {
   if (a.check_done && a.st->done) return;
   const Dims& d = a.d;
   const long nf = total_faces(d);
   // runs of 128 consecutive faces (coalesced loads): run r is audited when
   // r % stride == steps % stride
   const unsigned off = a.st->steps % a.stride;
-  const long e = ((long)blockIdx.x * a.stride + off) * 128 + threadIdx.x;
+  const long e = ((long)bx * a.stride + off) * 128 + threadIdx.x;
   float err = 0.f;
   bool audited = false;
   int dir, i, j, k;
@@ -313,6 +332,13 @@ __global__ void __launch_bounds__(128) sensor_audit_kernel(const AuditArgs a) {
   }
 }
 
+__global__ void __launch_bounds__(128) sensor_audit_kernel(const AuditArgs a) { audit_body(a, blockIdx.x); }
+
+__global__ void __launch_bounds__(128) sensor_audit_batched(const AuditArgs* args, const int* cta, int nblocks) {
+  const int b = block_of_cta(cta, nblocks, (int)blockIdx.x);
+  audit_body(args[b], blockIdx.x - (unsigned)__ldg(cta + b));
+}
+
 __global__ void adam_kernel(float* P, const float* G, float* M, float* V, float lr, float c1, float c2) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= SP_N) return;
@@ -347,18 +373,40 @@ cudaError_t launch_sample_faces(const SampleArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_sensor_audit(const AuditArgs& a, cudaStream_t s) {
+int sensor_audit_ctas(const AuditArgs& a) {
   const long nf = (long)(a.d.IM - 1) * (a.d.JM - 2) * (a.d.KM - 2) + (long)(a.d.IM - 2) * (a.d.JM - 1) * (a.d.KM - 2) +
                   (long)(a.d.IM - 2) * (a.d.JM - 2) * (a.d.KM - 1);
   const long runs = (nf + 127) / 128;
-  sensor_audit_kernel<<<(unsigned)((runs + a.stride - 1) / a.stride), 128, 0, s>>>(a);
+  return (int)((runs + a.stride - 1) / a.stride);
+}
+
+cudaError_t launch_sensor_audit(const AuditArgs& a, cudaStream_t s) {
+  sensor_audit_kernel<<<(unsigned)sensor_audit_ctas(a), 128, 0, s>>>(a);
   return cudaGetLastError();
+}
+
+int sensor_dilate_ctas(const Dims& d) {
+  return ((d.IM - 1 + 127) / 128) * ((d.JM - 1 + DL - 1) / DL) * (3 * (d.KM - 1));
 }
 
 cudaError_t launch_sensor_dilate(const DilateArgs& a, cudaStream_t s) {
   const dim3 grid((unsigned)((a.d.IM - 1 + 127) / 128), (unsigned)((a.d.JM - 1 + DL - 1) / DL),
                   (unsigned)(3 * (a.d.KM - 1)));
   sensor_dilate_kernel<<<grid, 128, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sensor_audit_batched(const AuditArgs* args, const int* cta, int nblocks, int total,
+                                        cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  sensor_audit_batched<<<total, 128, 0, s>>>(args, cta, nblocks);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sensor_dilate_batched(const DilateArgs* args, const int* cta, int nblocks, int total,
+                                         cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  sensor_dilate_batched<<<total, 128, 0, s>>>(args, cta, nblocks);
   return cudaGetLastError();
 }
 

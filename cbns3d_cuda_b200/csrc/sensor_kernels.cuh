@@ -83,6 +83,20 @@ cudaError_t launch_sample_faces(const SampleArgs& a, cudaStream_t s);
 cudaError_t launch_sensor_mask(const MaskArgs& a, cudaStream_t s);
 cudaError_t launch_sensor_audit(const AuditArgs& a, cudaStream_t s);
 cudaError_t launch_sensor_dilate(const DilateArgs& a, cudaStream_t s);
+// Batched forms (many blocks in one launch): args and cta are device tables,
+// block b owning CTAs cta[b] .. cta[b+1]-1 of total, cta[b+1] - cta[b] the
+// block's count below.  Mask: ipre[b] .. ipre[b+1]-1 are block b's work items
+// of each kind (sensor_mask_items); every block's MaskArgs::params must hold
+// the same network (it is loaded once per CTA, from args[0]).
+int sensor_dilate_ctas(const Dims& d);
+int sensor_audit_ctas(const AuditArgs& a);
+void sensor_mask_items(const Dims& d, long* items0, long* items1);
+cudaError_t launch_sensor_dilate_batched(const DilateArgs* args, const int* cta, int nblocks, int total,
+                                         cudaStream_t s);
+cudaError_t launch_sensor_audit_batched(const AuditArgs* args, const int* cta, int nblocks, int total,
+                                        cudaStream_t s);
+cudaError_t launch_sensor_mask_batched(const MaskArgs* args, const long* ipre0, const long* ipre1, long total0,
+                                       long total1, int nblocks, cudaStream_t s);
 cudaError_t launch_mlp_grad(const float* P, const float* X, const unsigned char* Y, unsigned n, float pos_w, float* G,
                             float* loss, cudaStream_t s);
 cudaError_t launch_adam(float* P, const float* G, float* M, float* V, unsigned step, float lr, cudaStream_t s);

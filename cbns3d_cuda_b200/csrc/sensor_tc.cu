@@ -105,24 +105,11 @@ __device__ __forceinline__ bool classify(SweepCtx& c, int t, const float f[SN_IN
   return true;
 }
 
-// KIND 0: the i-face rows; KIND 1: the j- and k-face window sweeps (two
-// launches, so that each path gets its own register allocation).
+// One work item (KIND 0: i-face rows; KIND 1: j- or k-face window sweeps) of
+// the block a: its decisions into a.mask.  Called by all threads of the CTA;
+// false if a tensor-core wait timed out (the CTA then classifies nothing more).
 template <int KIND>
-__global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(const MaskArgs a) {
-  if ((a.check_done && a.st->done) || !sensor_step(a.st, a.every)) return;
-  extern __shared__ unsigned char raw[];
-  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
-  tc::Smem& s = *reinterpret_cast<tc::Smem*>(base);
-  RowSmem& rs = *reinterpret_cast<RowSmem*>(base + sizeof(tc::Smem));
-  WinSmem& ws = *reinterpret_cast<WinSmem*>(base + sizeof(tc::Smem));
-  const int t = threadIdx.x;
-  if (t < 32) tc::tmem_alloc(&s.tmem, tc::TMEM_COLS);
-  if (t == 0) tc::mbar_init(&s.bar);
-  tc::load_weights(s, a.params, t, SW_T);
-  tc::fence_before_sync();
-  __syncthreads();
-  tc::fence_after_sync();
-
+__device__ __forceinline__ bool mask_item(const MaskArgs& a, long item, SweepCtx& cx, RowSmem& rs, WinSmem& ws, int t) {
   const Dims& d = a.d;
   const int IM = d.IM, JM = d.JM, KM = d.KM;
   const long VOL = d.VOL;
@@ -134,7 +121,6 @@ __global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(co
   const long n1 = (long)nseg * (KM - 2) * ((JM - 1 + SW_CH - 1) / SW_CH);
   const long n2 = (long)nseg * (JM - 2) * ((KM - 1 + SW_CH - 1) / SW_CH);
   const float gamma = a.gamma, gam1 = a.gam1;
-  SweepCtx cx{&s, 0u, logf(a.tau / (1.f - a.tau)), a.mask};  // p >= tau  <=>  logit >= zcut
   bool ok = true;
 
   auto load_q = [&](const double* p, double q[5]) {
@@ -145,212 +131,322 @@ __global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(co
     return node_prim((float)q[0], (float)q[1], (float)q[2], (float)q[3], (float)q[4], gam1);
   };
 
-  const long it0 = KIND == 0 ? 0 : n0, it1 = KIND == 0 ? n0 : n0 + n1 + n2;
-  for (long item = it0 + blockIdx.x; ok && item < it1; item += gridDim.x) {
-    float f[SN_IN];
-    if (KIND == 0) {  // i-faces, row by row
-      const int seg = (int)(item % nseg0), rc = (int)(item / nseg0);
-      const int i0 = seg * SW_T;
-      const int r0 = rc * SW_CH, r1 = min(rows, (rc + 1) * SW_CH);
-      // this thread's share of a row: node x = t (and x = SW_T + t for t < 5)
-      // and the area vector of node x = t (and x = SW_T for t = 0); the next
-      // row's share is loaded while the current row goes through the network
-      double q0[5], q1[5], a0[3], a1[3];
-      auto fetch = [&](int r) {
-        const int j = 1 + r % (JM - 2), k = 1 + r / (JM - 2);
-        const int ia = i0 - 2 + t, ib = i0 - 2 + SW_T + t;
-        if (ia <= IM + 1) load_q(a.q + node_off(d, ia, j, k), q0);
-        if (t < 5 && ib <= IM + 1) load_q(a.q + node_off(d, ib, j, k), q1);
-        if (i0 + t <= IM + 1) {
-          const long o = node_off(d, i0 + t, j, k);
+  float f[SN_IN];
+  if (KIND == 0) {  // i-faces, row by row
+    const int seg = (int)(item % nseg0), rc = (int)(item / nseg0);
+    const int i0 = seg * SW_T;
+    const int r0 = rc * SW_CH, r1 = min(rows, (rc + 1) * SW_CH);
+    // this thread's share of a row: node x = t (and x = SW_T + t for t < 5)
+    // and the area vector of node x = t (and x = SW_T for t = 0); the next
+    // row's share is loaded while the current row goes through the network
+    double q0[5], q1[5], a0[3], a1[3];
+    auto fetch = [&](int r) {
+      const int j = 1 + r % (JM - 2), k = 1 + r / (JM - 2);
+      const int ia = i0 - 2 + t, ib = i0 - 2 + SW_T + t;
+      if (ia <= IM + 1) load_q(a.q + node_off(d, ia, j, k), q0);
+      if (t < 5 && ib <= IM + 1) load_q(a.q + node_off(d, ib, j, k), q1);
+      if (i0 + t <= IM + 1) {
+        const long o = node_off(d, i0 + t, j, k);
 #pragma unroll
-          for (int m = 0; m < 3; ++m) a0[m] = __ldg(a.area[m] + o);
-        }
-        if (t == 0 && i0 + SW_T <= IM + 1) {
-          const long o = node_off(d, i0 + SW_T, j, k);
-#pragma unroll
-          for (int m = 0; m < 3; ++m) a1[m] = __ldg(a.area[m] + o);
-        }
-      };
-      auto put = [&](int x, const double q[5]) {
-        const NodePrim p = prim_of(q);
-        rs.pr[0][x] = p.r;
-        rs.pr[1][x] = p.p;
-        rs.pr[2][x] = p.u;
-        rs.pr[3][x] = p.v;
-        rs.pr[4][x] = p.w;
-      };
-      fetch(r0);
-      for (int r = r0; ok && r < r1; ++r) {
-        const int j = 1 + r % (JM - 2), k = 1 + r / (JM - 2);
-        __syncthreads();  // the previous row's staging is no longer read
-        if (i0 - 2 + t <= IM + 1) put(t, q0);
-        if (t < 5 && i0 - 2 + SW_T + t <= IM + 1) put(SW_T + t, q1);
-        if (i0 + t <= IM + 1) {
-#pragma unroll
-          for (int m = 0; m < 3; ++m) rs.ax[m][t] = (float)a0[m];
-        }
-        if (t == 0 && i0 + SW_T <= IM + 1) {
-#pragma unroll
-          for (int m = 0; m < 3; ++m) rs.ax[m][SW_T] = (float)a1[m];
-        }
-        if (r + 1 < r1) fetch(r + 1);
-        __syncthreads();
-        const int i = i0 + t;
-        const bool valid = i <= IM - 2;
-        if (valid) {
-          const float A[3] = {rs.ax[0][t], rs.ax[1][t], rs.ax[2][t]};
-          const float B[3] = {rs.ax[0][t + 1], rs.ax[1][t + 1], rs.ax[2][t + 1]};
-          float nx, ny, nz;
-          face_unit_normal(A, B, nx, ny, nz);
-          auto P = [&](int q) {
-            NodePrim p;
-            p.r = rs.pr[0][t + q];
-            p.p = rs.pr[1][t + q];
-            p.u = rs.pr[2][t + q];
-            p.v = rs.pr[3][t + q];
-            p.w = rs.pr[4][t + q];
-            return p;
-          };
-          features_of(P, nx, ny, nz, gamma, f);
-        } else {
-#pragma unroll
-          for (int m = 0; m < SN_IN; ++m) f[m] = 0.f;
-        }
-        ok = classify(cx, t, f, valid, i + (long)(IM - 1) * ((j - 1) + (long)(JM - 2) * (k - 1)));
+        for (int m = 0; m < 3; ++m) a0[m] = __ldg(a.area[m] + o);
       }
-    } else {  // j- or k-faces: a window sweep along the direction
-      const bool dj = item < n0 + n1;
-      const long it = dj ? item - n0 : item - n0 - n1;
-      const int seg = (int)(it % nseg);
-      const long r2 = it / nseg;
-      // dj: c = k (1..KM-2), faces along j; else c = j (1..JM-2), faces along k
-      const int cdim = dj ? KM - 2 : JM - 2;
-      const int c = 1 + (int)(r2 % cdim), ch = (int)(r2 / cdim);
-      const int nface = dj ? JM - 1 : KM - 1;
-      const int f0 = ch * SW_CH, f1 = min(nface, f0 + SW_CH);
-      const int i = 1 + seg * SW_T + t;
+      if (t == 0 && i0 + SW_T <= IM + 1) {
+        const long o = node_off(d, i0 + SW_T, j, k);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) a1[m] = __ldg(a.area[m] + o);
+      }
+    };
+    auto put = [&](int x, const double q[5]) {
+      const NodePrim p = prim_of(q);
+      rs.pr[0][x] = p.r;
+      rs.pr[1][x] = p.p;
+      rs.pr[2][x] = p.u;
+      rs.pr[3][x] = p.v;
+      rs.pr[4][x] = p.w;
+    };
+    fetch(r0);
+    for (int r = r0; ok && r < r1; ++r) {
+      const int j = 1 + r % (JM - 2), k = 1 + r / (JM - 2);
+      __syncthreads();  // the previous row's staging is no longer read
+      if (i0 - 2 + t <= IM + 1) put(t, q0);
+      if (t < 5 && i0 - 2 + SW_T + t <= IM + 1) put(SW_T + t, q1);
+      if (i0 + t <= IM + 1) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) rs.ax[m][t] = (float)a0[m];
+      }
+      if (t == 0 && i0 + SW_T <= IM + 1) {
+#pragma unroll
+        for (int m = 0; m < 3; ++m) rs.ax[m][SW_T] = (float)a1[m];
+      }
+      if (r + 1 < r1) fetch(r + 1);
+      __syncthreads();
+      const int i = i0 + t;
       const bool valid = i <= IM - 2;
-      const long sd = dj ? d.PX : d.PL;
-      const int am = dj ? 3 : 6;  // J grad(eta) or J grad(zeta)
-      // offset of the sweep's position 0 for this column; face fc has global
-      // index e0 + fc * es
-      const long obase = dj ? node_off(d, valid ? i : 1, 0, c) : node_off(d, valid ? i : 1, c, 0);
-      const long e0 = dj ? nfi + (i - 1) + (long)(IM - 2) * (JM - 1) * (c - 1) : nfi + nfj + (i - 1) + (long)(IM - 2) * (c - 1);
-      const long es = dj ? (long)(IM - 2) : (long)(IM - 2) * (JM - 2);
-      NodePrim W0, W1, W2, W3, W4, W5;
-      float Aa[3], Ab[3];
-      // step u (face f0+u) consumes node f0+3+u and the area vector of node f0+1+u
-      auto issue = [&](int u) {
-        if (valid && f0 + u < f1) {
-          const int slot = u % SW_D;
-          const long on = obase + (long)(f0 + 3 + u) * sd, oa = obase + (long)(f0 + 1 + u) * sd;
-#pragma unroll
-          for (int n = 0; n < 5; ++n) cp_async8(&ws.v[slot][n][t], a.q + n * VOL + on);
-#pragma unroll
-          for (int m = 0; m < 3; ++m) cp_async8(&ws.v[slot][5 + m][t], a.area[am + m] + oa);
-        }
-        cp_async_commit();  // one group per step, empty or not
-      };
-#pragma unroll
-      for (int u = 0; u < SW_D; ++u) issue(u);
       if (valid) {
-        double qq[5];
-        load_q(a.q + obase + (long)(f0 - 2) * sd, qq);
-        W0 = prim_of(qq);
-        load_q(a.q + obase + (long)(f0 - 1) * sd, qq);
-        W1 = prim_of(qq);
-        load_q(a.q + obase + (long)f0 * sd, qq);
-        W2 = prim_of(qq);
-        load_q(a.q + obase + (long)(f0 + 1) * sd, qq);
-        W3 = prim_of(qq);
-        load_q(a.q + obase + (long)(f0 + 2) * sd, qq);
-        W4 = prim_of(qq);
+        const float A[3] = {rs.ax[0][t], rs.ax[1][t], rs.ax[2][t]};
+        const float B[3] = {rs.ax[0][t + 1], rs.ax[1][t + 1], rs.ax[2][t + 1]};
+        float nx, ny, nz;
+        face_unit_normal(A, B, nx, ny, nz);
+        auto P = [&](int q) {
+          NodePrim p;
+          p.r = rs.pr[0][t + q];
+          p.p = rs.pr[1][t + q];
+          p.u = rs.pr[2][t + q];
+          p.v = rs.pr[3][t + q];
+          p.w = rs.pr[4][t + q];
+          return p;
+        };
+        features_of(P, nx, ny, nz, gamma, f);
+      } else {
 #pragma unroll
-        for (int m = 0; m < 3; ++m) Aa[m] = (float)__ldg(a.area[am + m] + obase + (long)f0 * sd);
+        for (int m = 0; m < SN_IN; ++m) f[m] = 0.f;
       }
-      // One face: the window (w0..w4 hold positions fc-2..fc+2, wn receives
-      // fc+3), the area vectors of positions fc (A0) and fc+1 (A1 receives).
-      // The unrolled loop below rotates the roles instead of moving values.
-      auto face = [&](int fc, NodePrim& w0, NodePrim& w1, NodePrim& w2, NodePrim& w3, NodePrim& w4, NodePrim& wn,
-                      float* A0, float* A1) {
-        const int u = fc - f0;
-        cp_async_wait_ring();  // the copies of step u have landed
-        if (valid) {
-          const int slot = u % SW_D;
-          double nq[5];
-#pragma unroll
-          for (int n = 0; n < 5; ++n) nq[n] = ws.v[slot][n][t];
-          wn = prim_of(nq);
-#pragma unroll
-          for (int m = 0; m < 3; ++m) A1[m] = (float)ws.v[slot][5 + m][t];
-        }
-        issue(u + SW_D);  // refill the slot just read
-        if (valid) {
-          float nx, ny, nz;
-          face_unit_normal(A0, A1, nx, ny, nz);
-          auto P = [&](int q) { return q == 0 ? w0 : q == 1 ? w1 : q == 2 ? w2 : q == 3 ? w3 : q == 4 ? w4 : wn; };
-          features_of(P, nx, ny, nz, gamma, f);
-        } else {
-#pragma unroll
-          for (int m = 0; m < SN_IN; ++m) f[m] = 0.f;
-        }
-        return classify(cx, t, f, valid, e0 + fc * es);
-      };
-      for (int fc = f0; ok && fc < f1; fc += 6) {
-        ok = face(fc, W0, W1, W2, W3, W4, W5, Aa, Ab);
-        if (!ok || fc + 1 >= f1) break;
-        ok = face(fc + 1, W1, W2, W3, W4, W5, W0, Ab, Aa);
-        if (!ok || fc + 2 >= f1) break;
-        ok = face(fc + 2, W2, W3, W4, W5, W0, W1, Aa, Ab);
-        if (!ok || fc + 3 >= f1) break;
-        ok = face(fc + 3, W3, W4, W5, W0, W1, W2, Ab, Aa);
-        if (!ok || fc + 4 >= f1) break;
-        ok = face(fc + 4, W4, W5, W0, W1, W2, W3, Aa, Ab);
-        if (!ok || fc + 5 >= f1) break;
-        ok = face(fc + 5, W5, W0, W1, W2, W3, W4, Ab, Aa);
-      }
-      cp_async_wait_all();  // the ring is reused by the next item
+      ok = classify(cx, t, f, valid, i + (long)(IM - 1) * ((j - 1) + (long)(JM - 2) * (k - 1)));
     }
+  } else {  // j- or k-faces: a window sweep along the direction
+    const bool dj = item < n0 + n1;
+    const long it = dj ? item - n0 : item - n0 - n1;
+    const int seg = (int)(it % nseg);
+    const long r2 = it / nseg;
+    // dj: c = k (1..KM-2), faces along j; else c = j (1..JM-2), faces along k
+    const int cdim = dj ? KM - 2 : JM - 2;
+    const int c = 1 + (int)(r2 % cdim), ch = (int)(r2 / cdim);
+    const int nface = dj ? JM - 1 : KM - 1;
+    const int f0 = ch * SW_CH, f1 = min(nface, f0 + SW_CH);
+    const int i = 1 + seg * SW_T + t;
+    const bool valid = i <= IM - 2;
+    const long sd = dj ? d.PX : d.PL;
+    const int am = dj ? 3 : 6;  // J grad(eta) or J grad(zeta)
+    // offset of the sweep's position 0 for this column; face fc has global
+    // index e0 + fc * es
+    const long obase = dj ? node_off(d, valid ? i : 1, 0, c) : node_off(d, valid ? i : 1, c, 0);
+    const long e0 = dj ? nfi + (i - 1) + (long)(IM - 2) * (JM - 1) * (c - 1) : nfi + nfj + (i - 1) + (long)(IM - 2) * (c - 1);
+    const long es = dj ? (long)(IM - 2) : (long)(IM - 2) * (JM - 2);
+    NodePrim W0, W1, W2, W3, W4, W5;
+    float Aa[3], Ab[3];
+    // step u (face f0+u) consumes node f0+3+u and the area vector of node f0+1+u
+    auto issue = [&](int u) {
+      if (valid && f0 + u < f1) {
+        const int slot = u % SW_D;
+        const long on = obase + (long)(f0 + 3 + u) * sd, oa = obase + (long)(f0 + 1 + u) * sd;
+#pragma unroll
+        for (int n = 0; n < 5; ++n) cp_async8(&ws.v[slot][n][t], a.q + n * VOL + on);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) cp_async8(&ws.v[slot][5 + m][t], a.area[am + m] + oa);
+      }
+      cp_async_commit();  // one group per step, empty or not
+    };
+#pragma unroll
+    for (int u = 0; u < SW_D; ++u) issue(u);
+    if (valid) {
+      double qq[5];
+      load_q(a.q + obase + (long)(f0 - 2) * sd, qq);
+      W0 = prim_of(qq);
+      load_q(a.q + obase + (long)(f0 - 1) * sd, qq);
+      W1 = prim_of(qq);
+      load_q(a.q + obase + (long)f0 * sd, qq);
+      W2 = prim_of(qq);
+      load_q(a.q + obase + (long)(f0 + 1) * sd, qq);
+      W3 = prim_of(qq);
+      load_q(a.q + obase + (long)(f0 + 2) * sd, qq);
+      W4 = prim_of(qq);
+#pragma unroll
+      for (int m = 0; m < 3; ++m) Aa[m] = (float)__ldg(a.area[am + m] + obase + (long)f0 * sd);
+    }
+    // One face: the window (w0..w4 hold positions fc-2..fc+2, wn receives
+    // fc+3), the area vectors of positions fc (A0) and fc+1 (A1 receives).
+    // The unrolled loop below rotates the roles instead of moving values.
+    auto face = [&](int fc, NodePrim& w0, NodePrim& w1, NodePrim& w2, NodePrim& w3, NodePrim& w4, NodePrim& wn,
+                    float* A0, float* A1) {
+      const int u = fc - f0;
+      cp_async_wait_ring();  // the copies of step u have landed
+      if (valid) {
+        const int slot = u % SW_D;
+        double nq[5];
+#pragma unroll
+        for (int n = 0; n < 5; ++n) nq[n] = ws.v[slot][n][t];
+        wn = prim_of(nq);
+#pragma unroll
+        for (int m = 0; m < 3; ++m) A1[m] = (float)ws.v[slot][5 + m][t];
+      }
+      issue(u + SW_D);  // refill the slot just read
+      if (valid) {
+        float nx, ny, nz;
+        face_unit_normal(A0, A1, nx, ny, nz);
+        auto P = [&](int q) { return q == 0 ? w0 : q == 1 ? w1 : q == 2 ? w2 : q == 3 ? w3 : q == 4 ? w4 : wn; };
+        features_of(P, nx, ny, nz, gamma, f);
+      } else {
+#pragma unroll
+        for (int m = 0; m < SN_IN; ++m) f[m] = 0.f;
+      }
+      return classify(cx, t, f, valid, e0 + fc * es);
+    };
+    for (int fc = f0; ok && fc < f1; fc += 6) {
+      ok = face(fc, W0, W1, W2, W3, W4, W5, Aa, Ab);
+      if (!ok || fc + 1 >= f1) break;
+      ok = face(fc + 1, W1, W2, W3, W4, W5, W0, Ab, Aa);
+      if (!ok || fc + 2 >= f1) break;
+      ok = face(fc + 2, W2, W3, W4, W5, W0, W1, Aa, Ab);
+      if (!ok || fc + 3 >= f1) break;
+      ok = face(fc + 3, W3, W4, W5, W0, W1, W2, Ab, Aa);
+      if (!ok || fc + 4 >= f1) break;
+      ok = face(fc + 4, W4, W5, W0, W1, W2, W3, Aa, Ab);
+      if (!ok || fc + 5 >= f1) break;
+      ok = face(fc + 5, W5, W0, W1, W2, W3, W4, Ab, Aa);
+    }
+    cp_async_wait_all();  // the ring is reused by the next item
   }
-  if (!ok && t == 0) {  // decisions incomplete: the step takes WENO5 everywhere
-    atomicExch(&a.st->sensor_fail, 1);
-    atomicExch(&a.st->force_weno, 1);
-  }
+  return ok;
+}
+
+// The items of one kind of a block: [*it0, *it1) of the numbering both kinds share.
+__device__ __forceinline__ void mask_items(const Dims& d, int kind, long* it0, long* it1) {
+  const int nseg0 = (d.IM - 1 + SW_T - 1) / SW_T, nseg = (d.IM - 2 + SW_T - 1) / SW_T;
+  const int rows = (d.JM - 2) * (d.KM - 2);
+  const long n0 = (long)nseg0 * ((rows + SW_CH - 1) / SW_CH);
+  const long n1 = (long)nseg * (d.KM - 2) * ((d.JM - 1 + SW_CH - 1) / SW_CH);
+  const long n2 = (long)nseg * (d.JM - 2) * ((d.KM - 1 + SW_CH - 1) / SW_CH);
+  *it0 = kind == 0 ? 0 : n0;
+  *it1 = kind == 0 ? n0 : n0 + n1 + n2;
+}
+
+__device__ __forceinline__ float logit_cut(float tau) { return logf(tau / (1.f - tau)); }  // p >= tau <=> logit >= cut
+
+__device__ __forceinline__ void mask_fail(StepState* st) {  // decisions incomplete: the step takes WENO5 everywhere
+  atomicExch(&st->sensor_fail, 1);
+  atomicExch(&st->force_weno, 1);
+}
+
+// CTA set-up of the sweeps: TMEM columns, the mbarrier, the network's weights.
+struct MaskSmem {
+  tc::Smem* s;
+  RowSmem* rs;
+  WinSmem* ws;
+};
+__device__ __forceinline__ MaskSmem mask_setup(const float* params, int t) {
+  extern __shared__ unsigned char raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(raw) + 127) & ~uintptr_t(127));
+  MaskSmem m{reinterpret_cast<tc::Smem*>(base), reinterpret_cast<RowSmem*>(base + sizeof(tc::Smem)),
+             reinterpret_cast<WinSmem*>(base + sizeof(tc::Smem))};
+  if (t < 32) tc::tmem_alloc(&m.s->tmem, tc::TMEM_COLS);
+  if (t == 0) tc::mbar_init(&m.s->bar);
+  tc::load_weights(*m.s, params, t, SW_T);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  return m;
+}
+
+__device__ __forceinline__ void mask_teardown(const MaskSmem& m, int t) {
   tc::fence_before_sync();
   __syncthreads();
   if (t < 32) {
     tc::fence_after_sync();
-    tc::tmem_dealloc(s.tmem, tc::TMEM_COLS);
+    tc::tmem_dealloc(m.s->tmem, tc::TMEM_COLS);
   }
+}
+
+// KIND 0: the i-face rows; KIND 1: the j- and k-face window sweeps (two
+// launches, so that each path gets its own register allocation).
+template <int KIND>
+__global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(const MaskArgs a) {
+  if ((a.check_done && a.st->done) || !sensor_step(a.st, a.every)) return;
+  const int t = threadIdx.x;
+  const MaskSmem m = mask_setup(a.params, t);
+  SweepCtx cx{m.s, 0u, logit_cut(a.tau), a.mask};
+  long it0, it1;
+  mask_items(a.d, KIND, &it0, &it1);
+  bool ok = true;
+  for (long item = it0 + blockIdx.x; ok && item < it1; item += gridDim.x)
+    ok = mask_item<KIND>(a, item, cx, *m.rs, *m.ws, t);
+  if (!ok && t == 0) mask_fail(a.st);
+  mask_teardown(m, t);
+}
+
+// Many blocks in one launch: the work items of every block that takes the
+// network this step (block b's items of this kind numbered ipre[b] ..
+// ipre[b+1]-1), handed out round robin to a grid sized for the device.  The
+// weights are loaded once per CTA, from args[0] (every block of a batch
+// carries the same network).  After a tensor-core wait timed out, a CTA
+// marks the block of each item it still owns as failed (WENO5 everywhere).
+template <int KIND>
+__global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_batched(const MaskArgs* args, const long* ipre,
+                                                                              int nblocks) {
+  const int t = threadIdx.x;
+  const long total = ipre[nblocks];
+  if ((long)blockIdx.x >= total) return;
+  const MaskSmem m = mask_setup(args[0].params, t);
+  SweepCtx cx{m.s, 0u, 0.f, nullptr};
+  bool ok = true;
+  int b = 0;  // the block of item g: g only grows, so does b
+  for (long g = blockIdx.x; g < total; g += gridDim.x) {
+    while (ipre[b + 1] <= g) ++b;
+    const MaskArgs& a = args[b];
+    if ((a.check_done && a.st->done) || !sensor_step(a.st, a.every)) continue;
+    if (ok) {
+      cx.zcut = logit_cut(a.tau);
+      cx.mask = a.mask;
+      long it0, it1;
+      mask_items(a.d, KIND, &it0, &it1);
+      ok = mask_item<KIND>(a, it0 + (g - ipre[b]), cx, *m.rs, *m.ws, t);
+    }
+    if (!ok && t == 0) mask_fail(a.st);
+  }
+  mask_teardown(m, t);
 }
 
 }  // namespace
 
-cudaError_t launch_sensor_mask(const MaskArgs& a, cudaStream_t s) {
-  const int smem0 = (int)(sizeof(tc::Smem) + sizeof(RowSmem)) + 128;
-  const int smem1 = (int)(sizeof(tc::Smem) + sizeof(WinSmem)) + 128;
+constexpr int kMaskSmem0 = (int)(sizeof(tc::Smem) + sizeof(RowSmem)) + 128;
+constexpr int kMaskSmem1 = (int)(sizeof(tc::Smem) + sizeof(WinSmem)) + 128;
+// at most 8 CTAs per SM hold TMEM (64 columns each of 512); the two launches
+// of a sweep run back to back on the stream
+constexpr long kMaskCap0 = 148L * 5, kMaskCap1 = 148L * 4;
+
+cudaError_t mask_prepare() {
   static bool attr = false;
-  if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(sensor_mask_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem0);
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(sensor_mask_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem1);
-    if (e != cudaSuccess) return e;
-    attr = true;
-  }
-  const Dims& d = a.d;
+  if (attr) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(sensor_mask_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaskSmem0);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(sensor_mask_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaskSmem1);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(sensor_mask_batched<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaskSmem0);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(sensor_mask_batched<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaskSmem1);
+  attr = e == cudaSuccess;
+  return e;
+}
+
+void sensor_mask_items(const Dims& d, long* items0, long* items1) {
   const long rows = (long)(d.JM - 2) * (d.KM - 2);
   const long nseg0 = (d.IM - 1 + SW_T - 1) / SW_T, nseg = (d.IM - 2 + SW_T - 1) / SW_T;
-  const long items0 = nseg0 * ((rows + SW_CH - 1) / SW_CH);
-  const long items1 = nseg * (d.KM - 2) * ((d.JM - 1 + SW_CH - 1) / SW_CH) +
-                      nseg * (d.JM - 2) * ((d.KM - 1 + SW_CH - 1) / SW_CH);
-  // at most 8 CTAs per SM hold TMEM (64 columns each of 512); the two
-  // launches run back to back on the stream
-  const long cap0 = 148L * 5, cap1 = 148L * 4;
-  sensor_mask_kernel<0><<<(unsigned)(items0 < cap0 ? items0 : cap0), SW_T, smem0, s>>>(a);
-  cudaError_t e = cudaGetLastError();
+  *items0 = nseg0 * ((rows + SW_CH - 1) / SW_CH);
+  *items1 = nseg * (d.KM - 2) * ((d.JM - 1 + SW_CH - 1) / SW_CH) + nseg * (d.JM - 2) * ((d.KM - 1 + SW_CH - 1) / SW_CH);
+}
+
+cudaError_t launch_sensor_mask(const MaskArgs& a, cudaStream_t s) {
+  cudaError_t e = mask_prepare();
   if (e != cudaSuccess) return e;
-  sensor_mask_kernel<1><<<(unsigned)(items1 < cap1 ? items1 : cap1), SW_T, smem1, s>>>(a);
+  long items0, items1;
+  sensor_mask_items(a.d, &items0, &items1);
+  sensor_mask_kernel<0><<<(unsigned)(items0 < kMaskCap0 ? items0 : kMaskCap0), SW_T, kMaskSmem0, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  sensor_mask_kernel<1><<<(unsigned)(items1 < kMaskCap1 ? items1 : kMaskCap1), SW_T, kMaskSmem1, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_sensor_mask_batched(const MaskArgs* args, const long* ipre0, const long* ipre1, long total0,
+                                       long total1, int nblocks, cudaStream_t s) {
+  cudaError_t e = mask_prepare();
+  if (e != cudaSuccess) return e;
+  if (total0 > 0)
+    sensor_mask_batched<0><<<(unsigned)(total0 < kMaskCap0 ? total0 : kMaskCap0), SW_T, kMaskSmem0, s>>>(args, ipre0,
+                                                                                                       nblocks);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || total1 <= 0) return e;
+  sensor_mask_batched<1><<<(unsigned)(total1 < kMaskCap1 ? total1 : kMaskCap1), SW_T, kMaskSmem1, s>>>(args, ipre1,
+                                                                                                     nblocks);
   return cudaGetLastError();
 }
 

@@ -65,6 +65,18 @@ cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfac
 cudaError_t launch_weno_faces(const StageArgs& a, int mode, long nfaces, const int2* list, cudaStream_t s);
 // Size the evaluation kernel's grid (once, outside any stream capture).
 cudaError_t weno_prepare();
+// The lists of many blocks in one launch (after zeroing each block's count):
+// block b owns CTAs cta[b] .. cta[b+1]-1 of total, weno_list_ctas(its faces) of them.
+struct ListArgs {
+  Dims d;
+  const unsigned char* mask;
+  long nf;
+  StepState* st;
+  int2* list;
+  int check_done;
+};
+int weno_list_ctas(long nfaces);
+cudaError_t launch_weno_list_batched(const ListArgs* args, const int* cta, int nblocks, int total, cudaStream_t s);
 // modes 1..3 only; hybrid: the StageArgs carry decision masks.
 cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool fp32, bool hybrid, cudaStream_t s);
 void stage_tiles(const Dims& d, int* ntile_i, int* ntile_j);

@@ -25,90 +25,211 @@ namespace cbns {
 
 namespace {
 
-// derivative of a ghosted field along stride s at ghosted index g of n
-__device__ __forceinline__ double dg(const double* f, long o, long s, int g, int n) {
-  if (g == 1)
-    return -5.0 / 6.0 * f[o] - 0.25 * f[o - s] + 1.5 * f[o + s] - 0.5 * f[o + 2 * s] + (1.0 / 12.0) * f[o + 3 * s];
-  if (g == n - 2)
-    return (5.0 / 6.0) * f[o] - 1.0 / 12.0 * f[o - 3 * s] + 0.5 * f[o - 2 * s] - 1.5 * f[o - s] + 0.25 * f[o + s];
-  return (1.0 / 12.0) * f[o - 2 * s] - 2.0 / 3.0 * f[o - s] + (2.0 / 3.0) * f[o + s] - 1.0 / 12.0 * f[o + 2 * s];
+// Tiles of the node kernel: 32 x 8 nodes of the box (i fastest, one warp per
+// row), marched through a chunk of k planes.  Shared memory holds the plane
+// being computed with a 3-node halo in i and j (the stencils reach 2 nodes, the
+// one-sided ones at the box edges 3) and a ring of the tile's own nodes on the
+// planes k-2 .. k+2 (the k stencils), for the four differentiated fields u, v,
+// w, T.  Each thread holds the next plane's values for the ring (plane k+3)
+// and the halo (plane k+1) in registers: their loads are issued before the
+// plane's arithmetic and stored to shared memory after it.
+constexpr int VTI = 32, VTJ = 8, VH = 3, VT = VTI * VTJ, VR = 5;
+constexpr int CW = VTI + 2 * VH, CJ = VTJ + 2 * VH;
+constexpr int VHALO = 2 * VH * VTJ + 2 * VH * VTI;  // 240 halo nodes: i strips, then j strips
+static_assert(VHALO <= VT, "one halo node per thread");
+
+struct ViscSmem {
+  double c[4][CJ][CW];            // plane k with its halo (corners unused)
+  double ring[VR][4][VTJ][VTI];   // the tile on planes k-2 .. k+2, slot = plane mod 5
+};
+
+// derivative from the values v(-3) .. v(+3) along the axis (only those the
+// stencil uses are read), at ghosted index g of n: the reference's 4th-order
+// stencils, one-sided at g = 1 and g = n - 2 (src/gradient_kernel.cu:135-255)
+template <typename V>
+__device__ __forceinline__ double dgv(const V& v, int g, int n) {
+  if (g == 1) return -5.0 / 6.0 * v(0) - 0.25 * v(-1) + 1.5 * v(1) - 0.5 * v(2) + (1.0 / 12.0) * v(3);
+  if (g == n - 2) return (5.0 / 6.0) * v(0) - 1.0 / 12.0 * v(-3) + 0.5 * v(-2) - 1.5 * v(-1) + 0.25 * v(1);
+  return (1.0 / 12.0) * v(-2) - 2.0 / 3.0 * v(-1) + (2.0 / 3.0) * v(1) - 1.0 / 12.0 * v(2);
 }
 
-// Node e of the ghosted box minus its outer layer (i fastest); every lane of
-// the warp calls this (the spectral-radius maximum is a warp reduction).
-__device__ __forceinline__ void visc_node_body(const ViscArgs& a, long e) {
+// halo node h of the tile at (i0, j0): ghosted (gi, gj) and its place in c
+__device__ __forceinline__ void halo_node(int h, int i0, int j0, int& gi, int& gj, int& cy, int& cx) {
+  if (h < 2 * VH * VTJ) {  // i strips: 3 columns x 8 rows each side
+    const int side = h / (VH * VTJ), r = h % (VH * VTJ), col = r % VH, row = r / VH;
+    cx = side ? VH + VTI + col : col;
+    cy = VH + row;
+    gi = side ? i0 + VTI + col : i0 - VH + col;
+    gj = j0 + row;
+  } else {  // j strips: 32 columns x 3 rows each side
+    const int h2 = h - 2 * VH * VTJ, side = h2 / (VH * VTI), r = h2 % (VH * VTI), col = r % VTI, row = r / VTI;
+    cx = VH + col;
+    cy = side ? VH + VTJ + row : row;
+    gi = i0 + col;
+    gj = side ? j0 + VTJ + row : j0 - VH + row;
+  }
+}
+
+// CTA `cta` of one block's node-kernel grid (tiles in i, then j, then k chunks).
+// Every thread of the CTA calls this (block-wide barriers; the spectral-radius
+// maximum is a warp reduction).
+__device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscSmem& sm) {
   const Dims& d = a.d;
-  const int VI = d.IG - 2, VJ = d.JG - 2, VK = d.KG - 2;
-  double sg = 0.0;
-  bool has = false;
-  if (e < (long)VI * VJ * VK) {
-    const int gi = 1 + (int)(e % VI);
-    const long r = e / VI;
-    const int gj = 1 + (int)(r % VJ), gk = 1 + (int)(r / VJ);
-    const int i = gi - NG, j = gj - NG, k = gk - NG;
-    const long o = node_off(d, i, j, k);
-    const long sj = d.PX, sk = d.PL;
-    const double *U = a.prim[1], *V = a.prim[2], *W = a.prim[3], *T = a.prim[5];
-    const double u_x = dg(U, o, 1, gi, d.IG), u_e = dg(U, o, sj, gj, d.JG), u_z = dg(U, o, sk, gk, d.KG);
-    const double v_x = dg(V, o, 1, gi, d.IG), v_e = dg(V, o, sj, gj, d.JG), v_z = dg(V, o, sk, gk, d.KG);
-    const double w_x = dg(W, o, 1, gi, d.IG), w_e = dg(W, o, sj, gj, d.JG), w_z = dg(W, o, sk, gk, d.KG);
-    const double T_x = dg(T, o, 1, gi, d.IG), T_e = dg(T, o, sj, gj, d.JG), T_z = dg(T, o, sk, gk, d.KG);
-    double m9[9];
+  const int IG = d.IG, JG = d.JG, KG = d.KG;
+  const int nti = (IG - 2 + VTI - 1) / VTI, ntj = (JG - 2 + VTJ - 1) / VTJ;
+  const int ti = cta % nti, tj = (cta / nti) % ntj, kc = cta / (nti * ntj);
+  const int i0 = 1 + ti * VTI, j0 = 1 + tj * VTJ;
+  const int kb = 1 + kc * a.kc, ke = min(KG - 1, kb + a.kc);  // planes kb .. ke-1 of 1 .. KG-2
+  const int t = threadIdx.x, tx = t % VTI, ty = t / VTI;
+  const int gi = i0 + tx, gj = j0 + ty;
+  const bool own = gi <= IG - 1 && gj <= JG - 1;        // a node of the ghosted box: kept in the ring
+  const bool valid = gi <= IG - 2 && gj <= JG - 2;      // a node whose fluxes this thread forms
+  const long sj = d.PX, sk = d.PL;
+  const double* F[4] = {a.prim[1], a.prim[2], a.prim[3], a.prim[5]};
+  const long o_own = node_off(d, gi - NG, gj - NG, -NG);  // plane 0 of this thread's column
+  int hgi = 0, hgj = 0, hcy = 0, hcx = 0;
+  const bool hal = t < VHALO;
+  if (hal) halo_node(t, i0, j0, hgi, hgj, hcy, hcx);
+  const bool hin = hal && hgi >= 0 && hgi <= IG - 1 && hgj >= 0 && hgj <= JG - 1;
+  const long o_hal = hin ? node_off(d, hgi - NG, hgj - NG, -NG) : 0;
+
+  double rn[4], hn[4];
+  auto load_ring = [&](int p, double v[4]) {
+    if (own && p >= 0 && p <= KG - 1) {
 #pragma unroll
-    for (int m = 0; m < 9; ++m) m9[m] = a.met[m][o];
-    const double J = a.met[9][o];
-    const double Tl = T[o];
-    double mu = (1.0 + a.C_T_inf) / (Tl + a.C_T_inf) * sqrt(Tl * Tl * Tl);
-    a.mu[o] = mu;
-    // chain rule: d/dx = xi_x d/dxi + eta_x d/deta + zeta_x d/dzeta, etc.
-    const double ux = u_x * m9[0] + u_e * m9[3] + u_z * m9[6];
-    const double uy = u_x * m9[1] + u_e * m9[4] + u_z * m9[7];
-    const double uz = u_x * m9[2] + u_e * m9[5] + u_z * m9[8];
-    const double vx = v_x * m9[0] + v_e * m9[3] + v_z * m9[6];
-    const double vy = v_x * m9[1] + v_e * m9[4] + v_z * m9[7];
-    const double vz = v_x * m9[2] + v_e * m9[5] + v_z * m9[8];
-    const double wx = w_x * m9[0] + w_e * m9[3] + w_z * m9[6];
-    const double wy = w_x * m9[1] + w_e * m9[4] + w_z * m9[7];
-    const double wz = w_x * m9[2] + w_e * m9[5] + w_z * m9[8];
-    const double mr = mu * a.Re_inv;
-    const double txx = (2.0 / 3.0) * mr * (2.0 * ux - vy - wz);
-    const double tyy = (2.0 / 3.0) * mr * (2.0 * vy - ux - wz);
-    const double tzz = (2.0 / 3.0) * mr * (2.0 * wz - ux - vy);
-    const double txy = mr * (uy + vx), txz = mr * (uz + wx), tyz = mr * (vz + wy);
-    const double kq = mr * a.qc;
-    const double qx = kq * (m9[0] * T_x + m9[3] * T_e + m9[6] * T_z);
-    const double qy = kq * (m9[1] * T_x + m9[4] * T_e + m9[7] * T_z);
-    const double qz = kq * (m9[2] * T_x + m9[5] * T_e + m9[8] * T_z);
-    const double uu = U[o], vv = V[o], ww = W[o];
-    const double ex = uu * txx + vv * txy + ww * txz - qx;
-    const double ey = uu * txy + vv * tyy + ww * tyz - qy;
-    const double ez = uu * txz + vv * tyz + ww * tzz - qz;
-#pragma unroll
-    for (int dd = 0; dd < 3; ++dd) {
-      const double nx = m9[3 * dd] * J, ny = m9[3 * dd + 1] * J, nz = m9[3 * dd + 2] * J;
-      a.vflux[4 * dd + 0][o] = nx * txx + ny * txy + nz * txz;
-      a.vflux[4 * dd + 1][o] = nx * txy + ny * tyy + nz * tyz;
-      a.vflux[4 * dd + 2][o] = nx * txz + ny * tyz + nz * tzz;
-      a.vflux[4 * dd + 3][o] = nx * ex + ny * ey + nz * ez;
+      for (int f = 0; f < 4; ++f) v[f] = __ldg(F[f] + o_own + p * sk);
     }
-    if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && k >= 0 && k < d.KM) {
-      const double rr = a.prim[0][o], pp = a.prim[4][o];
-      const double c = sqrt(a.gamma * pp / rr);
-      const double fv = a.dt_full ? 2.0 * mu * a.C_dt_v / rr
-                                  : 2.0 * mu * a.C_dt_v * sqrt(uu * uu + vv * vv + ww * ww) / c / rr;
-      double s = 0.0;
+  };
+  auto load_halo = [&](int p, double v[4]) {
+    if (hin) {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) v[f] = __ldg(F[f] + o_hal + p * sk);
+    }
+  };
+  auto put_ring = [&](int p, const double v[4]) {
+    if (own && p >= 0 && p <= KG - 1) {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) sm.ring[p % VR][f][ty][tx] = v[f];
+    }
+  };
+  auto put_plane = [&](int p, const double h[4]) {  // c <- plane p: halo from h, the tile from the ring
+    if (hin) {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) sm.c[f][hcy][hcx] = h[f];
+    }
+    if (own) {
+#pragma unroll
+      for (int f = 0; f < 4; ++f) sm.c[f][VH + ty][VH + tx] = sm.ring[p % VR][f][ty][tx];
+    }
+  };
+
+  // warm-up: the ring on planes kb-2 .. kb+2, plane kb in c
+  for (int p = kb - 2; p <= kb + 2; ++p) {
+    load_ring(p, rn);
+    put_ring(p, rn);
+  }
+  load_halo(kb, hn);
+  put_plane(kb, hn);
+  __syncthreads();
+
+  double sg = 0.0;  // the thread's largest spectral radius (grid nodes only)
+  bool has = false, nanseen = false;
+  for (int k = kb; k < ke; ++k) {
+    const bool more = k + 1 < ke;
+    if (more) {
+      load_ring(k + 3, rn);
+      load_halo(k + 1, hn);
+    }
+    if (valid) {
+      const long o = o_own + k * sk;
+      double m9[9];
+#pragma unroll
+      for (int m = 0; m < 9; ++m) m9[m] = __ldg(a.met[m] + o);
+      const double J = __ldg(a.met[9] + o);
+      double gx[4], ge[4], gz[4];
+      const int s0 = (k + VR - 2) % VR, s1 = (k + VR - 1) % VR, s3 = (k + 1) % VR, s4 = (k + 2) % VR;
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const double (*cp)[CW] = sm.c[f];
+        const int y = VH + ty, x = VH + tx;
+        gx[f] = dgv([&](int q) { return cp[y][x + q]; }, gi, IG);
+        ge[f] = dgv([&](int q) { return cp[y + q][x]; }, gj, JG);
+        // along k: the ring; the one-sided stencils of planes 1 and KG-2 reach
+        // a third plane (4 and KG-5), read from global memory
+        gz[f] = dgv(
+            [&](int q) {
+              switch (q) {
+                case -2: return sm.ring[s0][f][ty][tx];
+                case -1: return sm.ring[s1][f][ty][tx];
+                case 0: return cp[y][x];
+                case 1: return sm.ring[s3][f][ty][tx];
+                case 2: return sm.ring[s4][f][ty][tx];
+                default: return __ldg(F[f] + o + q * sk);
+              }
+            },
+            k, KG);
+      }
+      const double uu = sm.c[0][VH + ty][VH + tx], vv = sm.c[1][VH + ty][VH + tx], ww = sm.c[2][VH + ty][VH + tx];
+      const double Tl = sm.c[3][VH + ty][VH + tx];
+      const double mu = (1.0 + a.C_T_inf) / (Tl + a.C_T_inf) * sqrt(Tl * Tl * Tl);
+      a.mu[o] = mu;
+      // chain rule: d/dx = xi_x d/dxi + eta_x d/deta + zeta_x d/dzeta, etc.
+      const double ux = gx[0] * m9[0] + ge[0] * m9[3] + gz[0] * m9[6];
+      const double uy = gx[0] * m9[1] + ge[0] * m9[4] + gz[0] * m9[7];
+      const double uz = gx[0] * m9[2] + ge[0] * m9[5] + gz[0] * m9[8];
+      const double vx = gx[1] * m9[0] + ge[1] * m9[3] + gz[1] * m9[6];
+      const double vy = gx[1] * m9[1] + ge[1] * m9[4] + gz[1] * m9[7];
+      const double vz = gx[1] * m9[2] + ge[1] * m9[5] + gz[1] * m9[8];
+      const double wx = gx[2] * m9[0] + ge[2] * m9[3] + gz[2] * m9[6];
+      const double wy = gx[2] * m9[1] + ge[2] * m9[4] + gz[2] * m9[7];
+      const double wz = gx[2] * m9[2] + ge[2] * m9[5] + gz[2] * m9[8];
+      const double mr = mu * a.Re_inv;
+      const double txx = (2.0 / 3.0) * mr * (2.0 * ux - vy - wz);
+      const double tyy = (2.0 / 3.0) * mr * (2.0 * vy - ux - wz);
+      const double tzz = (2.0 / 3.0) * mr * (2.0 * wz - ux - vy);
+      const double txy = mr * (uy + vx), txz = mr * (uz + wx), tyz = mr * (vz + wy);
+      const double kq = mr * a.qc;
+      const double qx = kq * (m9[0] * gx[3] + m9[3] * ge[3] + m9[6] * gz[3]);
+      const double qy = kq * (m9[1] * gx[3] + m9[4] * ge[3] + m9[7] * gz[3]);
+      const double qz = kq * (m9[2] * gx[3] + m9[5] * ge[3] + m9[8] * gz[3]);
+      const double ex = uu * txx + vv * txy + ww * txz - qx;
+      const double ey = uu * txy + vv * tyy + ww * tyz - qy;
+      const double ez = uu * txz + vv * tyz + ww * tzz - qz;
 #pragma unroll
       for (int dd = 0; dd < 3; ++dd) {
-        const double mx = m9[3 * dd], my = m9[3 * dd + 1], mz = m9[3 * dd + 2];
-        const double na = sqrt(mx * mx + my * my + mz * mz);
-        s += fabs(uu * mx + vv * my + ww * mz) + c * na + na * na * fv;
+        const double nx = m9[3 * dd] * J, ny = m9[3 * dd + 1] * J, nz = m9[3 * dd + 2] * J;
+        a.vflux[4 * dd + 0][o] = nx * txx + ny * txy + nz * txz;
+        a.vflux[4 * dd + 1][o] = nx * txy + ny * tyy + nz * tyz;
+        a.vflux[4 * dd + 2][o] = nx * txz + ny * tyz + nz * tzz;
+        a.vflux[4 * dd + 3][o] = nx * ex + ny * ey + nz * ez;
       }
-      sg = s;
-      has = true;
+      const int i = gi - NG, j = gj - NG, kk = k - NG;
+      if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && kk >= 0 && kk < d.KM) {
+        const double rr = __ldg(a.prim[0] + o), pp = __ldg(a.prim[4] + o);
+        const double c = sqrt(a.gamma * pp / rr);
+        const double fv = a.dt_full ? 2.0 * mu * a.C_dt_v / rr
+                                    : 2.0 * mu * a.C_dt_v * sqrt(uu * uu + vv * vv + ww * ww) / c / rr;
+        double s = 0.0;
+#pragma unroll
+        for (int dd = 0; dd < 3; ++dd) {
+          const double mx = m9[3 * dd], my = m9[3 * dd + 1], mz = m9[3 * dd + 2];
+          const double na = sqrt(mx * mx + my * my + mz * mz);
+          s += fabs(uu * mx + vv * my + ww * mz) + c * na + na * na * fv;
+        }
+        if (s != s) nanseen = true;
+        else if (!has || s > sg) sg = s;
+        has = true;
+      }
     }
+    __syncthreads();  // plane k and ring slot k-2 are no longer read
+    if (more) {
+      put_ring(k + 3, rn);
+      put_plane(k + 1, hn);
+    }
+    __syncthreads();
   }
   if (a.sigma) {
-    const bool nan = has && (sg != sg);
+    const bool nan = nanseen;
     double m = (has && !nan) ? sg : 0.0;
     const unsigned anyhas = __ballot_sync(0xffffffffu, has);
     const unsigned anynan = __ballot_sync(0xffffffffu, nan);
@@ -150,40 +271,44 @@ __global__ void __launch_bounds__(256) visc_div_kernel(const ViscArgs a) {
 }
 
 __global__ void __launch_bounds__(256) visc_div_batched(const ViscArgs* args, const int* cta, int nblocks) {
-  int lo = 0, hi = nblocks - 1;  // the last b with cta[b] <= blockIdx.x
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(cta + mid) <= (int)blockIdx.x) lo = mid;
-    else hi = mid - 1;
-  }
+  const int lo = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const ViscArgs& a = args[lo];
   if (a.check_done && a.st->done) return;
   visc_div_body(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);
 }
 
-__global__ void __launch_bounds__(128) visc_node_kernel(const ViscArgs a) {
+__global__ void __launch_bounds__(VT, 2) visc_node_kernel(const ViscArgs a) {
   if (a.check_done && a.st->done) return;
-  visc_node_body(a, blockIdx.x * (long)blockDim.x + threadIdx.x);
+  extern __shared__ __align__(16) unsigned char vraw[];
+  visc_node_tile(a, blockIdx.x, *reinterpret_cast<ViscSmem*>(vraw));
 }
 
 // Many blocks in one launch: block b owns CTAs cta[b] .. cta[b+1]-1, args[b]
 // are its ViscArgs.
-__global__ void __launch_bounds__(128) visc_node_batched(const ViscArgs* args, const int* cta, int nblocks) {
-  int lo = 0, hi = nblocks - 1;  // the last b with cta[b] <= blockIdx.x
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(cta + mid) <= (int)blockIdx.x) lo = mid;
-    else hi = mid - 1;
-  }
+__global__ void __launch_bounds__(VT, 2) visc_node_batched(const ViscArgs* args, const int* cta, int nblocks) {
+  const int lo = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const ViscArgs& a = args[lo];
   if (a.check_done && a.st->done) return;
-  visc_node_body(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);
+  extern __shared__ __align__(16) unsigned char vraw[];
+  visc_node_tile(a, (int)blockIdx.x - __ldg(cta + lo), *reinterpret_cast<ViscSmem*>(vraw));
+}
+
+cudaError_t visc_prepare() {
+  static bool done = false;
+  if (done) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(visc_node_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(ViscSmem));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(visc_node_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(ViscSmem));
+  done = e == cudaSuccess;
+  return e;
 }
 
 }  // namespace
 
 cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s) {
-  visc_node_kernel<<<visc_ctas(a.d), 128, 0, s>>>(a);
+  cudaError_t e = visc_prepare();
+  if (e != cudaSuccess) return e;
+  visc_node_kernel<<<visc_ctas(a), VT, sizeof(ViscSmem), s>>>(a);
   visc_div_kernel<<<visc_div_ctas(a.d), 256, 0, s>>>(a);
   return cudaGetLastError();
 }
@@ -193,15 +318,29 @@ int visc_div_ctas(const Dims& d) {
   return (int)((n + 255) / 256);
 }
 
-int visc_ctas(const Dims& d) {
-  const long n = (long)(d.IG - 2) * (d.JG - 2) * (d.KG - 2);
-  return (int)((n + 127) / 128);
+int visc_kchunk(const Dims& d, int nsm) {
+  // chunks enough for about four waves of 2 CTAs per SM, at least 16 planes
+  // each (each chunk loads 5 planes ahead of its first)
+  const int VK = d.KG - 2;
+  const long tiles = (long)((d.IG - 2 + VTI - 1) / VTI) * ((d.JG - 2 + VTJ - 1) / VTJ);
+  const long want = (8L * nsm + tiles - 1) / tiles;
+  int kc = (int)((VK + want - 1) / want);
+  if (kc < 16) kc = 16;
+  return kc < VK ? kc : VK;
+}
+
+int visc_ctas(const ViscArgs& a) {
+  const Dims& d = a.d;
+  const int VK = d.KG - 2;
+  return ((d.IG - 2 + VTI - 1) / VTI) * ((d.JG - 2 + VTJ - 1) / VTJ) * ((VK + a.kc - 1) / a.kc);
 }
 
 cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas,
                                 const int* dcta, int dtotal, cudaStream_t s) {
   if (total_ctas <= 0) return cudaSuccess;
-  visc_node_batched<<<total_ctas, 128, 0, s>>>(args, cta, nblocks);
+  cudaError_t e = visc_prepare();
+  if (e != cudaSuccess) return e;
+  visc_node_batched<<<total_ctas, VT, sizeof(ViscSmem), s>>>(args, cta, nblocks);
   visc_div_batched<<<dtotal, 256, 0, s>>>(args, dcta, nblocks);
   return cudaGetLastError();
 }

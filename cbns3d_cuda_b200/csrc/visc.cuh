@@ -19,13 +19,16 @@ struct ViscArgs {
   StepState* st;
   int check_done;
   int sigma;                 // accumulate the spectral-radius max over the grid nodes
+  int kc;                    // node kernel: k planes per CTA (visc_kchunk)
 };
 
 // The node fluxes, then their divergence (two kernels).
 cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s);
+// k planes per CTA of the node kernel for a block on a device of nsm SMs.
+int visc_kchunk(const Dims& d, int nsm);
 // The same for many blocks in one launch: args and cta are device tables,
-// block b owning CTAs cta[b] .. cta[b+1]-1, cta[b+1] - cta[b] = visc_ctas(its Dims).
-int visc_ctas(const Dims& d);
+// block b owning CTAs cta[b] .. cta[b+1]-1, cta[b+1] - cta[b] = visc_ctas(its args).
+int visc_ctas(const ViscArgs& a);
 // The divergence kernel's CTAs for one block (cta tables of the batched divergence launch).
 int visc_div_ctas(const Dims& d);
 cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas,

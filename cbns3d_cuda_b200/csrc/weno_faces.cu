@@ -81,13 +81,13 @@ __device__ __forceinline__ void cursor_set(const Dims& d, long nfi, long nfj, lo
 // List the faces whose decision is set.  One 16-byte load of decisions per
 // thread; a CTA-wide scan of the counts and one global atomic per CTA place
 // the CTA's faces in the list, in face order within the CTA.
-__global__ void __launch_bounds__(LT) weno_list_kernel(const Dims d, const unsigned char* __restrict__ mask, long nf,
-                                                       StepState* st, int2* __restrict__ list, int check_done) {
+__device__ __forceinline__ void list_body(const Dims& d, const unsigned char* __restrict__ mask, long nf, StepState* st,
+                                          int2* __restrict__ list, int check_done, unsigned bx) {
   __shared__ int wsum[LT / 32];
   __shared__ int cbase;
   if (check_done && st->done) return;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const long f0 = (long)blockIdx.x * LCH + (long)t * LB;
+  const long f0 = (long)bx * LCH + (long)t * LB;
   unsigned bits = 0;
   if (f0 + LB <= nf) {
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(mask + f0));
@@ -140,79 +140,102 @@ __global__ void __launch_bounds__(LT) weno_list_kernel(const Dims d, const unsig
   }
 }
 
+__global__ void __launch_bounds__(LT) weno_list_kernel(const Dims d, const unsigned char* __restrict__ mask, long nf,
+                                                       StepState* st, int2* __restrict__ list, int check_done) {
+  list_body(d, mask, nf, st, list, check_done, blockIdx.x);
+}
+
+// Many blocks: zero every block's count, then list every block's faces (block
+// b owning CTAs cta[b] .. cta[b+1]-1).
+__global__ void weno_list_reset_batched(const ListArgs* args, int nblocks) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < nblocks && !(args[b].check_done && args[b].st->done)) args[b].st->weno_listed = 0;
+}
+
+__global__ void __launch_bounds__(LT) weno_list_batched(const ListArgs* args, const int* cta, int nblocks) {
+  const int b = block_of_cta(cta, nblocks, (int)blockIdx.x);
+  const ListArgs& a = args[b];
+  list_body(a.d, a.mask, a.nf, a.st, a.list, a.check_done, blockIdx.x - (unsigned)__ldg(cta + b));
+}
+
+// The WENO5 flux of one face of a's stage input into a.wflux: face w of the
+// list (or, with all set, face w of the block).  Each thread stages its face's
+// stencil in FP32 in its own column of shared memory (my, stride WT), so the
+// flux reads it there instead of keeping it in registers.
+__device__ __forceinline__ void weno_face(const StageArgs& a, bool all, long w, const int2* list, float* my) {
+  const Dims& d = a.d;
+  const long VOL = d.VOL;
+  long e, oa;
+  int kind;
+  if (all) {
+    const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
+    const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
+    FaceCursor c;
+    cursor_set(d, nfi, nfj, w, c);
+    e = w;
+    kind = c.kind;
+    oa = c.oa;
+  } else {
+    const int2 le = __ldg(list + w);
+    e = le.x;
+    kind = (int)((unsigned)le.y >> 30);
+    oa = (long)((unsigned)le.y & 0x3fffffffu);
+  }
+  long o0, s;  // first stencil node and the stride along the face normal
+  float nx, ny, nz;
+  if (kind == 0) {
+    // i-face between node oa and the next along i
+    o0 = oa - 2;
+    s = 1;
+    nx = 0.5f * (__ldg(a.area32[0] + oa) + __ldg(a.area32[0] + oa + 1));
+    ny = 0.5f * (__ldg(a.area32[1] + oa) + __ldg(a.area32[1] + oa + 1));
+    nz = 0.5f * (__ldg(a.area32[2] + oa) + __ldg(a.area32[2] + oa + 1));
+  } else if (kind == 1) {
+    // j-face between node oa and the next along j
+    o0 = oa - 2 * d.PX;
+    s = d.PX;
+    nx = 0.5f * (__ldg(a.area32[3] + oa) + __ldg(a.area32[3] + oa + d.PX));
+    ny = 0.5f * (__ldg(a.area32[4] + oa) + __ldg(a.area32[4] + oa + d.PX));
+    nz = 0.5f * (__ldg(a.area32[5] + oa) + __ldg(a.area32[5] + oa + d.PX));
+  } else {
+    // k-face between node oa and the next along k
+    o0 = oa - 2 * d.PL;
+    s = d.PL;
+    nx = 0.5f * ((float)__ldg(a.area[6] + oa) + (float)__ldg(a.area[6] + oa + d.PL));
+    ny = 0.5f * ((float)__ldg(a.area[7] + oa) + (float)__ldg(a.area[7] + oa + d.PL));
+    nz = 0.5f * ((float)__ldg(a.area[8] + oa) + (float)__ldg(a.area[8] + oa + d.PL));
+  }
+  // the stencil in FP32: all 30 loads in flight at once, each value converted once
+  {
+    const double* sp = a.src + o0;
+#pragma unroll
+    for (int q = 0; q < NEQ; ++q)
+#pragma unroll
+      for (int p = 0; p < 6; ++p) my[(q * 6 + p) * WT] = (float)__ldg(sp + q * VOL + p * s);
+  }
+  auto ld = [&](int p, int q) -> float { return my[(q * 6 + p) * WT]; };
+  const FluxConsts<float> C{(float)a.gamma, (float)a.gam1, (float)a.gam1_inv};
+  float f[5];
+  face_flux<float>(ld, nx, ny, nz, C, f);
+  float* out = a.wflux + 8 * e;
+  *reinterpret_cast<float4*>(out) = make_float4(f[0], f[1], f[2], f[3]);
+  out[4] = f[4];
+}
+
 // One thread per listed face (grid-stride over the list, whose length is on
 // the device), or per face while force_weno is set.  Built for 3 CTAs per SM
 // (80 registers): the faces' stencil loads are the wait, and 24 warps per SM
-// hide more of it than 16 (10% faster on the bench grid).  Each thread stages
-// its face's stencil in FP32 in its own column of shared memory (30 KB per
-// CTA), so the flux reads it there instead of keeping it in registers.
-__global__ void __launch_bounds__(WT, 3) weno_faces_kernel(const StageArgs a, int mode, long nf, const int2* list) {
+// hide more of it than 16 (10% faster on the bench grid); the staged stencils
+// take 30 KB of shared memory per CTA.
+__global__ void __launch_bounds__(WT, 3) weno_faces_kernel(const __grid_constant__ StageArgs a, int mode, long nf,
+                                                           const int2* list) {
   __shared__ float stn[NEQ * 6][WT];
   const StepState* st = a.st;
   if (mode != 0 && st->done) return;
   const bool all = st->force_weno != 0;
   const long cnt = all ? nf : (long)st->weno_listed;
-  const Dims& d = a.d;
-  const long VOL = d.VOL;
-  const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
-  const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
-  const FluxConsts<float> C{(float)a.gamma, (float)a.gam1, (float)a.gam1_inv};
-  for (long w = (long)blockIdx.x * WT + threadIdx.x; w < cnt; w += (long)gridDim.x * WT) {
-    long e, oa;
-    int kind;
-    if (all) {
-      FaceCursor c;
-      cursor_set(d, nfi, nfj, w, c);
-      e = w;
-      kind = c.kind;
-      oa = c.oa;
-    } else {
-      const int2 le = __ldg(list + w);
-      e = le.x;
-      kind = (int)((unsigned)le.y >> 30);
-      oa = (long)((unsigned)le.y & 0x3fffffffu);
-    }
-    long o0, s;  // first stencil node and the stride along the face normal
-    float nx, ny, nz;
-    if (kind == 0) {
-      // i-face between node oa and the next along i
-      o0 = oa - 2;
-      s = 1;
-      nx = 0.5f * (__ldg(a.area32[0] + oa) + __ldg(a.area32[0] + oa + 1));
-      ny = 0.5f * (__ldg(a.area32[1] + oa) + __ldg(a.area32[1] + oa + 1));
-      nz = 0.5f * (__ldg(a.area32[2] + oa) + __ldg(a.area32[2] + oa + 1));
-    } else if (kind == 1) {
-      // j-face between node oa and the next along j
-      o0 = oa - 2 * d.PX;
-      s = d.PX;
-      nx = 0.5f * (__ldg(a.area32[3] + oa) + __ldg(a.area32[3] + oa + d.PX));
-      ny = 0.5f * (__ldg(a.area32[4] + oa) + __ldg(a.area32[4] + oa + d.PX));
-      nz = 0.5f * (__ldg(a.area32[5] + oa) + __ldg(a.area32[5] + oa + d.PX));
-    } else {
-      // k-face between node oa and the next along k
-      o0 = oa - 2 * d.PL;
-      s = d.PL;
-      nx = 0.5f * ((float)__ldg(a.area[6] + oa) + (float)__ldg(a.area[6] + oa + d.PL));
-      ny = 0.5f * ((float)__ldg(a.area[7] + oa) + (float)__ldg(a.area[7] + oa + d.PL));
-      nz = 0.5f * ((float)__ldg(a.area[8] + oa) + (float)__ldg(a.area[8] + oa + d.PL));
-    }
-    // the stencil in FP32, staged in this thread's column of shared memory:
-    // all 30 loads in flight at once, each value converted once
-    float* my = &stn[0][threadIdx.x];
-    {
-      const double* sp = a.src + o0;
-#pragma unroll
-      for (int q = 0; q < NEQ; ++q)
-#pragma unroll
-        for (int p = 0; p < 6; ++p) my[(q * 6 + p) * WT] = (float)__ldg(sp + q * VOL + p * s);
-    }
-    auto ld = [&](int p, int q) -> float { return my[(q * 6 + p) * WT]; };
-    float f[5];
-    face_flux<float>(ld, nx, ny, nz, C, f);
-    float* out = a.wflux + 8 * e;
-    *reinterpret_cast<float4*>(out) = make_float4(f[0], f[1], f[2], f[3]);
-    out[4] = f[4];
-  }
+  for (long w = (long)blockIdx.x * WT + threadIdx.x; w < cnt; w += (long)gridDim.x * WT)
+    weno_face(a, all, w, list, &stn[0][threadIdx.x]);
 }
 
 int g_weno_grid = 0;  // persistent grid of the evaluation kernel: resident CTAs of the device
@@ -235,6 +258,14 @@ cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfac
   cudaError_t e = cudaMemsetAsync(&st->weno_listed, 0, sizeof(unsigned), s);
   if (e != cudaSuccess || nfaces <= 0) return e;
   weno_list_kernel<<<(unsigned)((nfaces + LCH - 1) / LCH), LT, 0, s>>>(d, mask, nfaces, st, list, check_done);
+  return cudaGetLastError();
+}
+
+int weno_list_ctas(long nfaces) { return (int)((nfaces + LCH - 1) / LCH); }
+
+cudaError_t launch_weno_list_batched(const ListArgs* args, const int* cta, int nblocks, int total, cudaStream_t s) {
+  weno_list_reset_batched<<<(nblocks + 255) / 256, 256, 0, s>>>(args, nblocks);
+  if (total > 0) weno_list_batched<<<total, LT, 0, s>>>(args, cta, nblocks);
   return cudaGetLastError();
 }
 

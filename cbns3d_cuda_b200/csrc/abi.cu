@@ -60,6 +60,9 @@ struct cbns_ctx {
   int pending_src = -1;  // buffer given to calc_numerical_flux, consumed by update_rk3
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
+  // bumped whenever a captured step of this context goes stale (a setting its
+  // kernels were captured with changed): a batch holding it captures anew
+  unsigned long long graph_gen = 0;
   int g_q = -1, g_p = -1, g_s = -1;
   int ntile_i = 1, ntile_j = 1, kchunk = 1;
   int stage_variant = 0;  // compiled occupancy variant of the stage kernel (cbns_autotune)
@@ -348,6 +351,7 @@ void drop_graph(cbns_ctx* c) {
   if (c->graph) cudaGraphDestroy(c->graph);
   c->gexec = nullptr;
   c->graph = nullptr;
+  ++c->graph_gen;
 }
 
 // The arguments of one context's sensor kernels (sensor_launch, and the
@@ -584,6 +588,7 @@ struct cbns_batch {
   int dil_total = 0, aud_total = 0, list_total = 0;
   long items_total[2] = {0, 0};
   std::vector<int> roles;     // (lq, lp, ls) per block at capture
+  std::vector<unsigned long long> gens;  // the blocks' graph_gen at capture
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
 };
@@ -856,11 +861,14 @@ int batch_run(cbns_batch* b, unsigned nsteps, double t_end, bool wait, unsigned*
   bool stale = !b->gexec;
   for (size_t i = 0; i < b->blk.size() && !stale; ++i) {
     const cbns_ctx* c = b->blk[i];
-    stale = b->roles[3 * i] != c->lq || b->roles[3 * i + 1] != c->lp || b->roles[3 * i + 2] != c->ls;
+    stale = b->roles[3 * i] != c->lq || b->roles[3 * i + 1] != c->lp || b->roles[3 * i + 2] != c->ls ||
+            b->gens[i] != c->graph_gen;
   }
   if (stale) {
     batch_drop_graph(b);
     RET(batch_tables(b));
+    b->gens.clear();
+    for (const cbns_ctx* c : b->blk) b->gens.push_back(c->graph_gen);
     std::vector<unsigned long long> l0;
     for (cbns_ctx* c : b->blk) l0.push_back(c->launches);
     CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));

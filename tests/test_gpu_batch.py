@@ -98,3 +98,26 @@ def test_batch_rejects_mixed_blocks():
     c = Block(make_params(*cs[1].shape, **cs[1].params, precision=PREC_SPLIT))  # no metrics yet
     with pytest.raises(CbnsError):
         Batch([a, c])
+
+
+def test_batch_follows_block_settings():
+    """A setting changed on a block after the batch captured its step (here the
+    sensor's network interval, which sets the widening width) reaches the
+    batch's next run: the batch captures the step anew."""
+    cs, _ = cases.case_batch(3, seed=5, size_lo=(20, 14, 10), size_hi=(36, 24, 16), viscous=False)
+    alone = [_block(c, PREC_HYBRID) for c in cs]
+    together = [_block(c, PREC_HYBRID) for c in cs]
+    for b in alone:
+        assert b.run(4) == 4
+        b.sensor_interval(1)
+        assert b.run(3) == 3
+    with Batch(together) as bt:
+        assert bt.run(4) == 4
+        for b in together:
+            b.sensor_interval(1)
+        assert bt.run(3) == 3
+    for a, b in zip(alone, together):
+        ma, mb = a.sensor_mask()[0], b.sensor_mask()[0]
+        assert np.mean(ma != mb) <= 1e-3
+        qa, qb = a.get_conservative(), b.get_conservative()
+        assert np.max(np.abs(qb - qa)) <= 1e-6 * np.max(np.abs(qa))

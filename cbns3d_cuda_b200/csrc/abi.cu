@@ -239,6 +239,7 @@ ViscArgs visc_args(cbns_ctx* c, bool check_done, bool sigma) {
   fill_met(c, a.met);
   for (int m = 0; m < 12; ++m) a.vflux[m] = c->f.vflux[m];
   for (int m = 0; m < 4; ++m) a.dfv[m] = c->f.dfv[m];
+  a.f32 = c->ph.precision != CBNS_PREC_FP64;
   a.visdiv = c->ph.visdiv;
   a.mu = c->f.prim[6];
   a.st = c->st;
@@ -826,7 +827,7 @@ int batch_enqueue_body(cbns_batch* b) {
       }
       if (b->visc) {
         CK(launch_visc_batched(b->visc_tab + k * nb, b->visc_cta, nb, b->visc_total, b->div_cta, b->div_total,
-                               b->stream));
+                               b->fp32, b->stream));
         b->blk[0]->launches += 2;
       }
       continue;

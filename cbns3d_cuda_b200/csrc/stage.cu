@@ -426,7 +426,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
     if (VISC && MODE != 0 && col_valid && k + 1 < ke) {
       const long o = node_off(d, ci, cj, k + 1);
 #pragma unroll
-      for (int n = 0; n < 4; ++n) prefetch_l2(a.dfv[n] + o);
+      for (int n = 0; n < 4; ++n) prefetch_l2(reinterpret_cast<const AreaT<R>*>(a.dfv[n]) + o);
     }
     // the FP32 kernels ask L2 for the next plane's RK operands and 1/J now, so
     // the update's loads one plane later find them there
@@ -598,7 +598,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
       if (VISC) {
         // the viscous flux divergence, formed by visc_div_kernel (visc.cu)
 #pragma unroll
-        for (int n = 0; n < 4; ++n) df[n + 1] -= __ldg(a.dfv[n] + o);
+        for (int n = 0; n < 4; ++n) df[n + 1] -= (double)__ldg(reinterpret_cast<const AreaT<R>*>(a.dfv[n]) + o);
       }
       const double iJ = (kEarly && MODE != 0) ? piJ : __ldg(a.area[9] + o);
       if (MODE == 0) {

@@ -28,7 +28,7 @@ struct StageArgs {
   double* out;         // stage output (5 fields), or the dense RHS array in mode 0
   const double* met[10];
   const double* area[10];  // J*grad(xi|eta|zeta) per node, then 1/J
-  const double* dfv[4];    // viscous: the divergence of the node fluxes (visc.cu)
+  const double* dfv[4];    // viscous: the divergence of the node fluxes (visc.cu; FP32 elements in the FP32 kernels)
   double* prim[6];     // viscous: rho,u,v,w,p,T of the new interior state
   StepState* st;       // dt, done flag, spectral-radius max
   const unsigned char* mask;  // hybrid: per-face sensor decision (null: plain flux everywhere)

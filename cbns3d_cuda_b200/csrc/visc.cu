@@ -73,6 +73,7 @@ __device__ __forceinline__ void halo_node(int h, int i0, int j0, int& gi, int& g
 // CTA `cta` of one block's node-kernel grid (tiles in i, then j, then k chunks).
 // Every thread of the CTA calls this (block-wide barriers; the spectral-radius
 // maximum is a warp reduction).
+template <typename V>
 __device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscSmem& sm) {
   const Dims& d = a.d;
   const int IG = d.IG, JG = d.JG, KG = d.KG;
@@ -198,10 +199,10 @@ __device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscS
 #pragma unroll
       for (int dd = 0; dd < 3; ++dd) {
         const double nx = m9[3 * dd] * J, ny = m9[3 * dd + 1] * J, nz = m9[3 * dd + 2] * J;
-        a.vflux[4 * dd + 0][o] = nx * txx + ny * txy + nz * txz;
-        a.vflux[4 * dd + 1][o] = nx * txy + ny * tyy + nz * tyz;
-        a.vflux[4 * dd + 2][o] = nx * txz + ny * tyz + nz * tzz;
-        a.vflux[4 * dd + 3][o] = nx * ex + ny * ey + nz * ez;
+        reinterpret_cast<V*>(a.vflux[4 * dd + 0])[o] = (V)(nx * txx + ny * txy + nz * txz);
+        reinterpret_cast<V*>(a.vflux[4 * dd + 1])[o] = (V)(nx * txy + ny * tyy + nz * tyz);
+        reinterpret_cast<V*>(a.vflux[4 * dd + 2])[o] = (V)(nx * txz + ny * tyz + nz * tzz);
+        reinterpret_cast<V*>(a.vflux[4 * dd + 3])[o] = (V)(nx * ex + ny * ey + nz * ez);
       }
       const int i = gi - NG, j = gj - NG, kk = k - NG;
       if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && kk >= 0 && kk < d.KM) {
@@ -240,16 +241,20 @@ __device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscS
   }
 }
 
-// 4th-order central derivative of a node field along a stride, at offset o.
-__device__ __forceinline__ double d4(const double* f, long o, long s) {
-  return (1.0 / 12.0) * __ldg(f + o - 2 * s) - (2.0 / 3.0) * __ldg(f + o - s) + (2.0 / 3.0) * __ldg(f + o + s) -
-         (1.0 / 12.0) * __ldg(f + o + 2 * s);
+// 4th-order central derivative of a node field along a stride, at offset o
+// (in the storage type V).
+template <typename V>
+__device__ __forceinline__ V d4(const double* fd, long o, long s) {
+  const V* f = reinterpret_cast<const V*>(fd);
+  return V(1.0 / 12.0) * __ldg(f + o - 2 * s) - V(2.0 / 3.0) * __ldg(f + o - s) + V(2.0 / 3.0) * __ldg(f + o + s) -
+         V(1.0 / 12.0) * __ldg(f + o + 2 * s);
 }
 
 // Interior node e (i fastest): the divergence of the node fluxes; the
 // reference takes the i-derivative at (i,j-1,k-1), the j-derivative at
 // (i-1,j,k-1), the k-derivative at (i-1,j-1,k) (CBNS_VISDIV_REFERENCE), or
 // all three at the node (CBNS_VISDIV_CENTERED).
+template <typename V>
 __device__ __forceinline__ void visc_div_body(const ViscArgs& a, long e) {
   const Dims& d = a.d;
   const int NI = d.IM - 2, NJ = d.JM - 2;
@@ -262,43 +267,53 @@ __device__ __forceinline__ void visc_div_body(const ViscArgs& a, long e) {
   const long oi = o - sh * (d.PX + d.PL), oj = o - sh * (1 + d.PL), ok = o - sh * (1 + d.PX);
 #pragma unroll
   for (int n = 0; n < 4; ++n)
-    a.dfv[n][o] = d4(a.vflux[n], oi, 1) + d4(a.vflux[4 + n], oj, d.PX) + d4(a.vflux[8 + n], ok, d.PL);
+    reinterpret_cast<V*>(a.dfv[n])[o] =
+        d4<V>(a.vflux[n], oi, 1) + d4<V>(a.vflux[4 + n], oj, d.PX) + d4<V>(a.vflux[8 + n], ok, d.PL);
 }
 
+template <typename V>
 __global__ void __launch_bounds__(256) visc_div_kernel(const ViscArgs a) {
   if (a.check_done && a.st->done) return;
-  visc_div_body(a, blockIdx.x * (long)blockDim.x + threadIdx.x);
+  visc_div_body<V>(a, blockIdx.x * (long)blockDim.x + threadIdx.x);
 }
 
+template <typename V>
 __global__ void __launch_bounds__(256) visc_div_batched(const ViscArgs* args, const int* cta, int nblocks) {
   const int lo = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const ViscArgs& a = args[lo];
   if (a.check_done && a.st->done) return;
-  visc_div_body(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);
+  visc_div_body<V>(a, ((long)blockIdx.x - __ldg(cta + lo)) * blockDim.x + threadIdx.x);
 }
 
+template <typename V>
 __global__ void __launch_bounds__(VT, 2) visc_node_kernel(const ViscArgs a) {
   if (a.check_done && a.st->done) return;
   extern __shared__ __align__(16) unsigned char vraw[];
-  visc_node_tile(a, blockIdx.x, *reinterpret_cast<ViscSmem*>(vraw));
+  visc_node_tile<V>(a, blockIdx.x, *reinterpret_cast<ViscSmem*>(vraw));
 }
 
 // Many blocks in one launch: block b owns CTAs cta[b] .. cta[b+1]-1, args[b]
 // are its ViscArgs.
+template <typename V>
 __global__ void __launch_bounds__(VT, 2) visc_node_batched(const ViscArgs* args, const int* cta, int nblocks) {
   const int lo = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const ViscArgs& a = args[lo];
   if (a.check_done && a.st->done) return;
   extern __shared__ __align__(16) unsigned char vraw[];
-  visc_node_tile(a, (int)blockIdx.x - __ldg(cta + lo), *reinterpret_cast<ViscSmem*>(vraw));
+  visc_node_tile<V>(a, (int)blockIdx.x - __ldg(cta + lo), *reinterpret_cast<ViscSmem*>(vraw));
 }
 
 cudaError_t visc_prepare() {
   static bool done = false;
   if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(visc_node_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(ViscSmem));
+  const int sm = (int)sizeof(ViscSmem);
+  cudaError_t e = cudaFuncSetAttribute(visc_node_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(visc_node_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, sizeof(ViscSmem));
+    e = cudaFuncSetAttribute(visc_node_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(visc_node_batched<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(visc_node_batched<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   done = e == cudaSuccess;
   return e;
 }
@@ -308,8 +323,13 @@ cudaError_t visc_prepare() {
 cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s) {
   cudaError_t e = visc_prepare();
   if (e != cudaSuccess) return e;
-  visc_node_kernel<<<visc_ctas(a), VT, sizeof(ViscSmem), s>>>(a);
-  visc_div_kernel<<<visc_div_ctas(a.d), 256, 0, s>>>(a);
+  if (a.f32) {
+    visc_node_kernel<float><<<visc_ctas(a), VT, sizeof(ViscSmem), s>>>(a);
+    visc_div_kernel<float><<<visc_div_ctas(a.d), 256, 0, s>>>(a);
+  } else {
+    visc_node_kernel<double><<<visc_ctas(a), VT, sizeof(ViscSmem), s>>>(a);
+    visc_div_kernel<double><<<visc_div_ctas(a.d), 256, 0, s>>>(a);
+  }
   return cudaGetLastError();
 }
 
@@ -336,12 +356,17 @@ int visc_ctas(const ViscArgs& a) {
 }
 
 cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas,
-                                const int* dcta, int dtotal, cudaStream_t s) {
+                                const int* dcta, int dtotal, bool f32, cudaStream_t s) {
   if (total_ctas <= 0) return cudaSuccess;
   cudaError_t e = visc_prepare();
   if (e != cudaSuccess) return e;
-  visc_node_batched<<<total_ctas, VT, sizeof(ViscSmem), s>>>(args, cta, nblocks);
-  visc_div_batched<<<dtotal, 256, 0, s>>>(args, dcta, nblocks);
+  if (f32) {
+    visc_node_batched<float><<<total_ctas, VT, sizeof(ViscSmem), s>>>(args, cta, nblocks);
+    visc_div_batched<float><<<dtotal, 256, 0, s>>>(args, dcta, nblocks);
+  } else {
+    visc_node_batched<double><<<total_ctas, VT, sizeof(ViscSmem), s>>>(args, cta, nblocks);
+    visc_div_batched<double><<<dtotal, 256, 0, s>>>(args, dcta, nblocks);
+  }
   return cudaGetLastError();
 }
 

@@ -12,8 +12,9 @@ struct ViscArgs {
   double qc;                 // -1/(Pr (gamma-1) M^2): heat-flux factor before mu/Re
   const double* prim[6];     // rho,u,v,w,p,T
   const double* met[10];
-  double* vflux[12];         // E0..E3, F0..F3, G0..G3
-  double* dfv[4];            // their divergence at the interior nodes
+  double* vflux[12];         // E0..E3, F0..F3, G0..G3 (FP32 elements when f32)
+  double* dfv[4];            // their divergence at the interior nodes (FP32 elements when f32)
+  int f32;                   // FP32-flux precisions: node fluxes and divergence stored (and differenced) in FP32
   int visdiv;                // CBNS_VISDIV_*
   double* mu;
   StepState* st;
@@ -32,6 +33,6 @@ int visc_ctas(const ViscArgs& a);
 // The divergence kernel's CTAs for one block (cta tables of the batched divergence launch).
 int visc_div_ctas(const Dims& d);
 cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblocks, int total_ctas,
-                                const int* dcta, int dtotal, cudaStream_t s);
+                                const int* dcta, int dtotal, bool f32, cudaStream_t s);
 
 }  // namespace cbns

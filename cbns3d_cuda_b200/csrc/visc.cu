@@ -38,19 +38,23 @@ constexpr int CW = VTI + 2 * VH, CJ = VTJ + 2 * VH;
 constexpr int VHALO = 2 * VH * VTJ + 2 * VH * VTI;  // 240 halo nodes: i strips, then j strips
 static_assert(VHALO <= VT, "one halo node per thread");
 
+// T: the node arithmetic and the staged fields (double for the plain path,
+// float for the FP32-flux precisions)
+template <typename T>
 struct ViscSmem {
-  double c[4][CJ][CW];            // plane k with its halo (corners unused)
-  double ring[VR][4][VTJ][VTI];   // the tile on planes k-2 .. k+2, slot = plane mod 5
+  T c[4][CJ][CW];            // plane k with its halo (corners unused)
+  T ring[VR][4][VTJ][VTI];   // the tile on planes k-2 .. k+2, slot = plane mod 5
 };
 
 // derivative from the values v(-3) .. v(+3) along the axis (only those the
 // stencil uses are read), at ghosted index g of n: the reference's 4th-order
 // stencils, one-sided at g = 1 and g = n - 2 (src/gradient_kernel.cu:135-255)
-template <typename V>
-__device__ __forceinline__ double dgv(const V& v, int g, int n) {
-  if (g == 1) return -5.0 / 6.0 * v(0) - 0.25 * v(-1) + 1.5 * v(1) - 0.5 * v(2) + (1.0 / 12.0) * v(3);
-  if (g == n - 2) return (5.0 / 6.0) * v(0) - 1.0 / 12.0 * v(-3) + 0.5 * v(-2) - 1.5 * v(-1) + 0.25 * v(1);
-  return (1.0 / 12.0) * v(-2) - 2.0 / 3.0 * v(-1) + (2.0 / 3.0) * v(1) - 1.0 / 12.0 * v(2);
+template <typename T, typename A>
+__device__ __forceinline__ T dgv(const A& v, int g, int n) {
+  if (g == 1) return T(-5.0 / 6.0) * v(0) - T(0.25) * v(-1) + T(1.5) * v(1) - T(0.5) * v(2) + T(1.0 / 12.0) * v(3);
+  if (g == n - 2)
+    return T(5.0 / 6.0) * v(0) - T(1.0 / 12.0) * v(-3) + T(0.5) * v(-2) - T(1.5) * v(-1) + T(0.25) * v(1);
+  return T(1.0 / 12.0) * v(-2) - T(2.0 / 3.0) * v(-1) + T(2.0 / 3.0) * v(1) - T(1.0 / 12.0) * v(2);
 }
 
 // halo node h of the tile at (i0, j0): ghosted (gi, gj) and its place in c
@@ -74,7 +78,8 @@ __device__ __forceinline__ void halo_node(int h, int i0, int j0, int& gi, int& g
 // Every thread of the CTA calls this (block-wide barriers; the spectral-radius
 // maximum is a warp reduction).
 template <typename V>
-__device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscSmem& sm) {
+__device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscSmem<V>& sm) {
+  using T = V;  // the arithmetic follows the storage
   const Dims& d = a.d;
   const int IG = d.IG, JG = d.JG, KG = d.KG;
   const int nti = (IG - 2 + VTI - 1) / VTI, ntj = (JG - 2 + VTJ - 1) / VTJ;
@@ -85,7 +90,7 @@ __device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscS
   const int gi = i0 + tx, gj = j0 + ty;
   const bool own = gi <= IG - 1 && gj <= JG - 1;        // a node of the ghosted box: kept in the ring
   const bool valid = gi <= IG - 2 && gj <= JG - 2;      // a node whose fluxes this thread forms
-  const long sj = d.PX, sk = d.PL;
+  const long sk = d.PL;
   const double* F[4] = {a.prim[1], a.prim[2], a.prim[3], a.prim[5]};
   const long o_own = node_off(d, gi - NG, gj - NG, -NG);  // plane 0 of this thread's column
   int hgi = 0, hgj = 0, hcy = 0, hcx = 0;
@@ -94,26 +99,26 @@ __device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscS
   const bool hin = hal && hgi >= 0 && hgi <= IG - 1 && hgj >= 0 && hgj <= JG - 1;
   const long o_hal = hin ? node_off(d, hgi - NG, hgj - NG, -NG) : 0;
 
-  double rn[4], hn[4];
-  auto load_ring = [&](int p, double v[4]) {
+  T rn[4], hn[4];
+  auto load_ring = [&](int p, T v[4]) {
     if (own && p >= 0 && p <= KG - 1) {
 #pragma unroll
-      for (int f = 0; f < 4; ++f) v[f] = __ldg(F[f] + o_own + p * sk);
+      for (int f = 0; f < 4; ++f) v[f] = (T)__ldg(F[f] + o_own + p * sk);
     }
   };
-  auto load_halo = [&](int p, double v[4]) {
+  auto load_halo = [&](int p, T v[4]) {
     if (hin) {
 #pragma unroll
-      for (int f = 0; f < 4; ++f) v[f] = __ldg(F[f] + o_hal + p * sk);
+      for (int f = 0; f < 4; ++f) v[f] = (T)__ldg(F[f] + o_hal + p * sk);
     }
   };
-  auto put_ring = [&](int p, const double v[4]) {
+  auto put_ring = [&](int p, const T v[4]) {
     if (own && p >= 0 && p <= KG - 1) {
 #pragma unroll
       for (int f = 0; f < 4; ++f) sm.ring[p % VR][f][ty][tx] = v[f];
     }
   };
-  auto put_plane = [&](int p, const double h[4]) {  // c <- plane p: halo from h, the tile from the ring
+  auto put_plane = [&](int p, const T h[4]) {  // c <- plane p: halo from h, the tile from the ring
     if (hin) {
 #pragma unroll
       for (int f = 0; f < 4; ++f) sm.c[f][hcy][hcx] = h[f];
@@ -143,79 +148,88 @@ __device__ __forceinline__ void visc_node_tile(const ViscArgs& a, int cta, ViscS
     }
     if (valid) {
       const long o = o_own + k * sk;
-      double m9[9];
+      T m9[9];
 #pragma unroll
-      for (int m = 0; m < 9; ++m) m9[m] = __ldg(a.met[m] + o);
-      const double J = __ldg(a.met[9] + o);
-      double gx[4], ge[4], gz[4];
+      for (int m = 0; m < 9; ++m) m9[m] = (T)__ldg(a.met[m] + o);
+      const T J = (T)__ldg(a.met[9] + o);
+      T gx[4], ge[4], gz[4];
       const int s0 = (k + VR - 2) % VR, s1 = (k + VR - 1) % VR, s3 = (k + 1) % VR, s4 = (k + 2) % VR;
 #pragma unroll
       for (int f = 0; f < 4; ++f) {
-        const double (*cp)[CW] = sm.c[f];
+        const T (*cp)[CW] = sm.c[f];
         const int y = VH + ty, x = VH + tx;
-        gx[f] = dgv([&](int q) { return cp[y][x + q]; }, gi, IG);
-        ge[f] = dgv([&](int q) { return cp[y + q][x]; }, gj, JG);
+        gx[f] = dgv<T>([&](int q) { return cp[y][x + q]; }, gi, IG);
+        ge[f] = dgv<T>([&](int q) { return cp[y + q][x]; }, gj, JG);
         // along k: the ring; the one-sided stencils of planes 1 and KG-2 reach
         // a third plane (4 and KG-5), read from global memory
-        gz[f] = dgv(
-            [&](int q) {
+        gz[f] = dgv<T>(
+            [&](int q) -> T {
               switch (q) {
                 case -2: return sm.ring[s0][f][ty][tx];
                 case -1: return sm.ring[s1][f][ty][tx];
                 case 0: return cp[y][x];
                 case 1: return sm.ring[s3][f][ty][tx];
                 case 2: return sm.ring[s4][f][ty][tx];
-                default: return __ldg(F[f] + o + q * sk);
+                default: return (T)__ldg(F[f] + o + q * sk);
               }
             },
             k, KG);
       }
-      const double uu = sm.c[0][VH + ty][VH + tx], vv = sm.c[1][VH + ty][VH + tx], ww = sm.c[2][VH + ty][VH + tx];
-      const double Tl = sm.c[3][VH + ty][VH + tx];
-      const double mu = (1.0 + a.C_T_inf) / (Tl + a.C_T_inf) * sqrt(Tl * Tl * Tl);
-      a.mu[o] = mu;
+      const T uu = sm.c[0][VH + ty][VH + tx], vv = sm.c[1][VH + ty][VH + tx], ww = sm.c[2][VH + ty][VH + tx];
+      const T Tl = sm.c[3][VH + ty][VH + tx];
+      const T CT = (T)a.C_T_inf;
+      const T mu = (T(1) + CT) / (Tl + CT) * sqrt(Tl * Tl * Tl);
+      a.mu[o] = (double)mu;
       // chain rule: d/dx = xi_x d/dxi + eta_x d/deta + zeta_x d/dzeta, etc.
-      const double ux = gx[0] * m9[0] + ge[0] * m9[3] + gz[0] * m9[6];
-      const double uy = gx[0] * m9[1] + ge[0] * m9[4] + gz[0] * m9[7];
-      const double uz = gx[0] * m9[2] + ge[0] * m9[5] + gz[0] * m9[8];
-      const double vx = gx[1] * m9[0] + ge[1] * m9[3] + gz[1] * m9[6];
-      const double vy = gx[1] * m9[1] + ge[1] * m9[4] + gz[1] * m9[7];
-      const double vz = gx[1] * m9[2] + ge[1] * m9[5] + gz[1] * m9[8];
-      const double wx = gx[2] * m9[0] + ge[2] * m9[3] + gz[2] * m9[6];
-      const double wy = gx[2] * m9[1] + ge[2] * m9[4] + gz[2] * m9[7];
-      const double wz = gx[2] * m9[2] + ge[2] * m9[5] + gz[2] * m9[8];
-      const double mr = mu * a.Re_inv;
-      const double txx = (2.0 / 3.0) * mr * (2.0 * ux - vy - wz);
-      const double tyy = (2.0 / 3.0) * mr * (2.0 * vy - ux - wz);
-      const double tzz = (2.0 / 3.0) * mr * (2.0 * wz - ux - vy);
-      const double txy = mr * (uy + vx), txz = mr * (uz + wx), tyz = mr * (vz + wy);
-      const double kq = mr * a.qc;
-      const double qx = kq * (m9[0] * gx[3] + m9[3] * ge[3] + m9[6] * gz[3]);
-      const double qy = kq * (m9[1] * gx[3] + m9[4] * ge[3] + m9[7] * gz[3]);
-      const double qz = kq * (m9[2] * gx[3] + m9[5] * ge[3] + m9[8] * gz[3]);
-      const double ex = uu * txx + vv * txy + ww * txz - qx;
-      const double ey = uu * txy + vv * tyy + ww * tyz - qy;
-      const double ez = uu * txz + vv * tyz + ww * tzz - qz;
+      const T ux = gx[0] * m9[0] + ge[0] * m9[3] + gz[0] * m9[6];
+      const T uy = gx[0] * m9[1] + ge[0] * m9[4] + gz[0] * m9[7];
+      const T uz = gx[0] * m9[2] + ge[0] * m9[5] + gz[0] * m9[8];
+      const T vx = gx[1] * m9[0] + ge[1] * m9[3] + gz[1] * m9[6];
+      const T vy = gx[1] * m9[1] + ge[1] * m9[4] + gz[1] * m9[7];
+      const T vz = gx[1] * m9[2] + ge[1] * m9[5] + gz[1] * m9[8];
+      const T wx = gx[2] * m9[0] + ge[2] * m9[3] + gz[2] * m9[6];
+      const T wy = gx[2] * m9[1] + ge[2] * m9[4] + gz[2] * m9[7];
+      const T wz = gx[2] * m9[2] + ge[2] * m9[5] + gz[2] * m9[8];
+      const T mr = mu * (T)a.Re_inv;
+      const T txx = T(2.0 / 3.0) * mr * (T(2) * ux - vy - wz);
+      const T tyy = T(2.0 / 3.0) * mr * (T(2) * vy - ux - wz);
+      const T tzz = T(2.0 / 3.0) * mr * (T(2) * wz - ux - vy);
+      const T txy = mr * (uy + vx), txz = mr * (uz + wx), tyz = mr * (vz + wy);
+      const T kq = mr * (T)a.qc;
+      const T qx = kq * (m9[0] * gx[3] + m9[3] * ge[3] + m9[6] * gz[3]);
+      const T qy = kq * (m9[1] * gx[3] + m9[4] * ge[3] + m9[7] * gz[3]);
+      const T qz = kq * (m9[2] * gx[3] + m9[5] * ge[3] + m9[8] * gz[3]);
+      const T ex = uu * txx + vv * txy + ww * txz - qx;
+      const T ey = uu * txy + vv * tyy + ww * tyz - qy;
+      const T ez = uu * txz + vv * tyz + ww * tzz - qz;
 #pragma unroll
       for (int dd = 0; dd < 3; ++dd) {
-        const double nx = m9[3 * dd] * J, ny = m9[3 * dd + 1] * J, nz = m9[3 * dd + 2] * J;
-        reinterpret_cast<V*>(a.vflux[4 * dd + 0])[o] = (V)(nx * txx + ny * txy + nz * txz);
-        reinterpret_cast<V*>(a.vflux[4 * dd + 1])[o] = (V)(nx * txy + ny * tyy + nz * tyz);
-        reinterpret_cast<V*>(a.vflux[4 * dd + 2])[o] = (V)(nx * txz + ny * tyz + nz * tzz);
-        reinterpret_cast<V*>(a.vflux[4 * dd + 3])[o] = (V)(nx * ex + ny * ey + nz * ez);
+        const T nx = m9[3 * dd] * J, ny = m9[3 * dd + 1] * J, nz = m9[3 * dd + 2] * J;
+        reinterpret_cast<V*>(a.vflux[4 * dd + 0])[o] = nx * txx + ny * txy + nz * txz;
+        reinterpret_cast<V*>(a.vflux[4 * dd + 1])[o] = nx * txy + ny * tyy + nz * tyz;
+        reinterpret_cast<V*>(a.vflux[4 * dd + 2])[o] = nx * txz + ny * tyz + nz * tzz;
+        reinterpret_cast<V*>(a.vflux[4 * dd + 3])[o] = nx * ex + ny * ey + nz * ez;
       }
       const int i = gi - NG, j = gj - NG, kk = k - NG;
       if (a.sigma && i >= 0 && i < d.IM && j >= 0 && j < d.JM && kk >= 0 && kk < d.KM) {
+        // the spectral radius for the next dt, in FP64 from the FP64 fields
+        // whatever T is (src/time_step_kernel.cu:13-96)
         const double rr = __ldg(a.prim[0] + o), pp = __ldg(a.prim[4] + o);
+        const bool t64 = sizeof(T) == 8;
+        const double ud = t64 ? (double)uu : __ldg(a.prim[1] + o), vd = t64 ? (double)vv : __ldg(a.prim[2] + o),
+                     wd = t64 ? (double)ww : __ldg(a.prim[3] + o), Td = t64 ? (double)Tl : __ldg(a.prim[5] + o);
+        const double mud = t64 ? (double)mu : (1.0 + a.C_T_inf) / (Td + a.C_T_inf) * sqrt(Td * Td * Td);
         const double c = sqrt(a.gamma * pp / rr);
-        const double fv = a.dt_full ? 2.0 * mu * a.C_dt_v / rr
-                                    : 2.0 * mu * a.C_dt_v * sqrt(uu * uu + vv * vv + ww * ww) / c / rr;
+        const double fv = a.dt_full ? 2.0 * mud * a.C_dt_v / rr
+                                    : 2.0 * mud * a.C_dt_v * sqrt(ud * ud + vd * vd + wd * wd) / c / rr;
         double s = 0.0;
 #pragma unroll
         for (int dd = 0; dd < 3; ++dd) {
-          const double mx = m9[3 * dd], my = m9[3 * dd + 1], mz = m9[3 * dd + 2];
+          const double mx = t64 ? (double)m9[3 * dd] : __ldg(a.met[3 * dd] + o);
+          const double my = t64 ? (double)m9[3 * dd + 1] : __ldg(a.met[3 * dd + 1] + o);
+          const double mz = t64 ? (double)m9[3 * dd + 2] : __ldg(a.met[3 * dd + 2] + o);
           const double na = sqrt(mx * mx + my * my + mz * mz);
-          s += fabs(uu * mx + vv * my + ww * mz) + c * na + na * na * fv;
+          s += fabs(ud * mx + vd * my + wd * mz) + c * na + na * na * fv;
         }
         if (s != s) nanseen = true;
         else if (!has || s > sg) sg = s;
@@ -286,34 +300,35 @@ __global__ void __launch_bounds__(256) visc_div_batched(const ViscArgs* args, co
 }
 
 template <typename V>
-__global__ void __launch_bounds__(VT, 2) visc_node_kernel(const ViscArgs a) {
+__global__ void __launch_bounds__(VT, sizeof(V) == 4 ? 3 : 2) visc_node_kernel(const ViscArgs a) {
   if (a.check_done && a.st->done) return;
   extern __shared__ __align__(16) unsigned char vraw[];
-  visc_node_tile<V>(a, blockIdx.x, *reinterpret_cast<ViscSmem*>(vraw));
+  visc_node_tile<V>(a, blockIdx.x, *reinterpret_cast<ViscSmem<V>*>(vraw));
 }
 
 // Many blocks in one launch: block b owns CTAs cta[b] .. cta[b+1]-1, args[b]
 // are its ViscArgs.
 template <typename V>
-__global__ void __launch_bounds__(VT, 2) visc_node_batched(const ViscArgs* args, const int* cta, int nblocks) {
+__global__ void __launch_bounds__(VT, sizeof(V) == 4 ? 3 : 2) visc_node_batched(const ViscArgs* args, const int* cta,
+                                                                               int nblocks) {
   const int lo = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const ViscArgs& a = args[lo];
   if (a.check_done && a.st->done) return;
   extern __shared__ __align__(16) unsigned char vraw[];
-  visc_node_tile<V>(a, (int)blockIdx.x - __ldg(cta + lo), *reinterpret_cast<ViscSmem*>(vraw));
+  visc_node_tile<V>(a, (int)blockIdx.x - __ldg(cta + lo), *reinterpret_cast<ViscSmem<V>*>(vraw));
 }
 
 cudaError_t visc_prepare() {
   static bool done = false;
   if (done) return cudaSuccess;
-  const int sm = (int)sizeof(ViscSmem);
-  cudaError_t e = cudaFuncSetAttribute(visc_node_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  const int s64 = (int)sizeof(ViscSmem<double>), s32 = (int)sizeof(ViscSmem<float>);
+  cudaError_t e = cudaFuncSetAttribute(visc_node_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(visc_node_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    e = cudaFuncSetAttribute(visc_node_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(visc_node_batched<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    e = cudaFuncSetAttribute(visc_node_batched<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(visc_node_batched<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    e = cudaFuncSetAttribute(visc_node_batched<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32);
   done = e == cudaSuccess;
   return e;
 }
@@ -324,10 +339,10 @@ cudaError_t launch_visc(const ViscArgs& a, cudaStream_t s) {
   cudaError_t e = visc_prepare();
   if (e != cudaSuccess) return e;
   if (a.f32) {
-    visc_node_kernel<float><<<visc_ctas(a), VT, sizeof(ViscSmem), s>>>(a);
+    visc_node_kernel<float><<<visc_ctas(a), VT, sizeof(ViscSmem<float>), s>>>(a);
     visc_div_kernel<float><<<visc_div_ctas(a.d), 256, 0, s>>>(a);
   } else {
-    visc_node_kernel<double><<<visc_ctas(a), VT, sizeof(ViscSmem), s>>>(a);
+    visc_node_kernel<double><<<visc_ctas(a), VT, sizeof(ViscSmem<double>), s>>>(a);
     visc_div_kernel<double><<<visc_div_ctas(a.d), 256, 0, s>>>(a);
   }
   return cudaGetLastError();
@@ -361,10 +376,10 @@ cudaError_t launch_visc_batched(const ViscArgs* args, const int* cta, int nblock
   cudaError_t e = visc_prepare();
   if (e != cudaSuccess) return e;
   if (f32) {
-    visc_node_batched<float><<<total_ctas, VT, sizeof(ViscSmem), s>>>(args, cta, nblocks);
+    visc_node_batched<float><<<total_ctas, VT, sizeof(ViscSmem<float>), s>>>(args, cta, nblocks);
     visc_div_batched<float><<<dtotal, 256, 0, s>>>(args, dcta, nblocks);
   } else {
-    visc_node_batched<double><<<total_ctas, VT, sizeof(ViscSmem), s>>>(args, cta, nblocks);
+    visc_node_batched<double><<<total_ctas, VT, sizeof(ViscSmem<double>), s>>>(args, cta, nblocks);
     visc_div_batched<double><<<dtotal, 256, 0, s>>>(args, dcta, nblocks);
   }
   return cudaGetLastError();

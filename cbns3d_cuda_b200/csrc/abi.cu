@@ -659,7 +659,7 @@ int batch_sensor_tables(cbns_batch* b) {
     lt[i] = ss.li;
     dc[i + 1] = dc[i] + sensor_dilate_ctas(c->d);
     ac[i + 1] = ac[i] + sensor_audit_ctas(ss.au);
-    lc[i + 1] = lc[i] + weno_list_ctas(c->nfaces);
+    lc[i + 1] = lc[i] + weno_list_ctas(c->d);
     long n0, n1;
     sensor_mask_items(c->d, &n0, &n1);
     ip[i + 1] = ip[i] + n0;

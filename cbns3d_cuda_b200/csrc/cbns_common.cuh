@@ -67,7 +67,7 @@ struct StepState {
   unsigned long long audit_faces; // hybrid: faces the audit re-evaluated
   float audit_max;                // hybrid: largest relative flux difference the audit saw
   int sensor_fail;                // hybrid: a tensor-core wait timed out
-  unsigned weno_listed;           // hybrid: length of the step's list of WENO5 faces
+  unsigned weno_listed[3];        // hybrid: lengths of the step's lists of WENO5 i-, j- and k-faces
   int stage_fail;                 // a stage kernel's TMA wait timed out (the state is not valid)
 };
 

@@ -56,7 +56,8 @@ struct BatchStage {
 cudaError_t launch_stage(const StageArgs& a, int mode, bool visc, bool fp32, int variant, cudaStream_t s);
 int stage_variants(bool fp32, bool hybrid);
 // Hybrid: list the faces whose decision byte is set (once per step, after the
-// decisions are final; st->weno_listed receives the count) ...
+// decisions are final; each face kind in its own list, st->weno_listed[kind]
+// receiving its length) ...
 cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfaces, StepState* st, int2* list,
                              bool check_done, cudaStream_t s);
 // ... and evaluate the listed faces (every face while force_weno is set) into
@@ -66,7 +67,7 @@ cudaError_t launch_weno_faces(const StageArgs& a, int mode, long nfaces, const i
 // Size the evaluation kernel's grid (once, outside any stream capture).
 cudaError_t weno_prepare();
 // The lists of many blocks in one launch (after zeroing each block's count):
-// block b owns CTAs cta[b] .. cta[b+1]-1 of total, weno_list_ctas(its faces) of them.
+// block b owns CTAs cta[b] .. cta[b+1]-1 of total, weno_list_ctas(its Dims) of them.
 struct ListArgs {
   Dims d;
   const unsigned char* mask;
@@ -75,7 +76,7 @@ struct ListArgs {
   int2* list;
   int check_done;
 };
-int weno_list_ctas(long nfaces);
+int weno_list_ctas(const Dims& d);
 cudaError_t launch_weno_list_batched(const ListArgs* args, const int* cta, int nblocks, int total, cudaStream_t s);
 // modes 1..3 only; hybrid: the StageArgs carry decision masks.
 cudaError_t launch_stage_batched(const BatchStage& b, int mode, bool visc, bool fp32, bool hybrid, cudaStream_t s);

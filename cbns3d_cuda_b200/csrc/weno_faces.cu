@@ -78,16 +78,47 @@ __device__ __forceinline__ void cursor_set(const Dims& d, long nfi, long nfj, lo
   }
 }
 
-// List the faces whose decision is set.  One 16-byte load of decisions per
-// thread; a CTA-wide scan of the counts and one global atomic per CTA place
-// the CTA's faces in the list, in face order within the CTA.
+// The faces of one kind: the first face index and the count (i-faces, then
+// j-faces, then k-faces in the global face numbering).
+__host__ __device__ __forceinline__ void kind_range(const Dims& d, int kind, long* first, long* count) {
+  const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
+  const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
+  const long nfk = (long)(d.IM - 2) * (d.JM - 2) * (d.KM - 1);
+  *first = kind == 0 ? 0 : (kind == 1 ? nfi : nfi + nfj);
+  *count = kind == 0 ? nfi : (kind == 1 ? nfj : nfk);
+}
+
+// CTAs of the list kernel for one kind: chunks of LCH faces from the kind's
+// first face rounded down to a 16-byte boundary of the mask.
+__host__ __device__ __forceinline__ int list_ctas_kind(const Dims& d, int kind) {
+  long first, count;
+  kind_range(d, kind, &first, &count);
+  const long a = first & ~15L;
+  return (int)((first + count - a + LCH - 1) / LCH);
+}
+
+// List the faces whose decision is set, each kind in its own list (the list
+// array's range from the kind's first face index on), so that the evaluation
+// pass can walk the three kinds side by side, plane by plane.  One 16-byte
+// load of decisions per thread; a CTA-wide scan of the counts and one global
+// atomic per CTA place the CTA's faces in its kind's list, in face order
+// within the CTA.
 __device__ __forceinline__ void list_body(const Dims& d, const unsigned char* __restrict__ mask, long nf, StepState* st,
                                           int2* __restrict__ list, int check_done, unsigned bx) {
   __shared__ int wsum[LT / 32];
   __shared__ int cbase;
   if (check_done && st->done) return;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const long f0 = (long)bx * LCH + (long)t * LB;
+  int kind = 0;
+  unsigned chunk = bx;
+  for (; kind < 2; ++kind) {
+    const unsigned ck = (unsigned)list_ctas_kind(d, kind);
+    if (chunk < ck) break;
+    chunk -= ck;
+  }
+  long first, count;
+  kind_range(d, kind, &first, &count);
+  const long f0 = (first & ~15L) + (long)chunk * LCH + (long)t * LB;  // 16-byte aligned
   unsigned bits = 0;
   if (f0 + LB <= nf) {
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(mask + f0));
@@ -101,6 +132,10 @@ __device__ __forceinline__ void list_body(const Dims& d, const unsigned char* __
     for (int b = 0; b < LB && f0 + b < nf; ++b)
       if (__ldg(mask + f0 + b)) bits |= 1u << b;
   }
+  // only this kind's faces
+#pragma unroll
+  for (int b = 0; b < LB; ++b)
+    if (f0 + b < first || f0 + b >= first + count) bits &= ~(1u << b);
   const int n = __popc(bits);
   int incl = n;
 #pragma unroll
@@ -117,18 +152,20 @@ __device__ __forceinline__ void list_body(const Dims& d, const unsigned char* __
       wsum[w] = tot;
       tot += c;
     }
-    cbase = tot ? (int)atomicAdd(&st->weno_listed, (unsigned)tot) : 0;
+    cbase = tot ? (int)atomicAdd(&st->weno_listed[kind], (unsigned)tot) : 0;
   }
   __syncthreads();
-  int pos = cbase + wsum[warp] + incl - n;
+  long pos = first + cbase + wsum[warp] + incl - n;
   if (!bits) return;
   const long nfi = (long)(d.IM - 1) * (d.JM - 2) * (d.KM - 2);
   const long nfj = (long)(d.IM - 2) * (d.JM - 1) * (d.KM - 2);
+  // the cursor starts at the thread's first face of this kind
+  const int b0 = __ffs(bits) - 1;
   FaceCursor c;
-  cursor_set(d, nfi, nfj, f0, c);
-  for (int b = 0; b < LB; ++b) {
+  cursor_set(d, nfi, nfj, f0 + b0, c);
+  for (int b = b0; b < LB; ++b) {
     if ((bits >> b) & 1u) list[pos++] = list_entry(c.e, c.kind, c.oa);
-    if (b == LB - 1) break;
+    if (b == LB - 1 || !(bits >> (b + 1))) break;
     // advance to face f0 + b + 1
     if (c.e + 1 == c.kind_end || c.i + 1 == c.ni) {
       cursor_set(d, nfi, nfj, c.e + 1, c);  // next kind, or next row (which may start a new plane)
@@ -149,7 +186,8 @@ __global__ void __launch_bounds__(LT) weno_list_kernel(const Dims d, const unsig
 // b owning CTAs cta[b] .. cta[b+1]-1).
 __global__ void weno_list_reset_batched(const ListArgs* args, int nblocks) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < nblocks && !(args[b].check_done && args[b].st->done)) args[b].st->weno_listed = 0;
+  if (b < nblocks && !(args[b].check_done && args[b].st->done))
+    for (int k = 0; k < 3; ++k) args[b].st->weno_listed[k] = 0;
 }
 
 __global__ void __launch_bounds__(LT) weno_list_batched(const ListArgs* args, const int* cta, int nblocks) {
@@ -222,20 +260,38 @@ __device__ __forceinline__ void weno_face(const StageArgs& a, bool all, long w, 
   out[4] = f[4];
 }
 
-// One thread per listed face (grid-stride over the list, whose length is on
-// the device), or per face while force_weno is set.  Built for 3 CTAs per SM
-// (80 registers): the faces' stencil loads are the wait, and 24 warps per SM
-// hide more of it than 16 (10% faster on the bench grid); the staged stencils
-// take 30 KB of shared memory per CTA.
+// One thread per listed face, or per face while force_weno is set.  The CTAs
+// are shared out among the three kinds' lists in proportion to their lengths
+// (at least one for a kind with faces), and each kind's CTAs walk its list
+// grid-stride, so the three kinds advance through the grid's planes side by
+// side and the stencils they share stay in L2.  Built for 3 CTAs per SM (80
+// registers): the faces' stencil loads are the wait, and 24 warps per SM hide
+// more of it than 16 (10% faster on the bench grid); the staged stencils take
+// 30 KB of shared memory per CTA.
 __global__ void __launch_bounds__(WT, 3) weno_faces_kernel(const __grid_constant__ StageArgs a, int mode, long nf,
                                                            const int2* list) {
   __shared__ float stn[NEQ * 6][WT];
   const StepState* st = a.st;
   if (mode != 0 && st->done) return;
   const bool all = st->force_weno != 0;
-  const long cnt = all ? nf : (long)st->weno_listed;
-  for (long w = (long)blockIdx.x * WT + threadIdx.x; w < cnt; w += (long)gridDim.x * WT)
-    weno_face(a, all, w, list, &stn[0][threadIdx.x]);
+  long first[3], len[3];
+  for (int k = 0; k < 3; ++k) {
+    long cnt;
+    kind_range(a.d, k, &first[k], &cnt);
+    len[k] = all ? cnt : (long)st->weno_listed[k];
+  }
+  const long tot = len[0] + len[1] + len[2];
+  if (tot == 0) return;
+  const int G = gridDim.x;
+  int b1 = (int)((len[0] * G + tot - 1) / tot), b2 = (int)(((len[0] + len[1]) * G + tot - 1) / tot);
+  b1 = min(max(b1, len[0] > 0 ? 1 : 0), G - (len[1] > 0 ? 1 : 0) - (len[2] > 0 ? 1 : 0));
+  b2 = min(max(b2, b1 + (len[1] > 0 ? 1 : 0)), G - (len[2] > 0 ? 1 : 0));
+  const int c = blockIdx.x;
+  const int k = c < b1 ? 0 : (c < b2 ? 1 : 2);
+  const int base = k == 0 ? 0 : (k == 1 ? b1 : b2);
+  const int g = k == 0 ? b1 : (k == 1 ? b2 - b1 : G - b2);
+  for (long w = (long)(c - base) * WT + threadIdx.x; w < len[k]; w += (long)g * WT)
+    weno_face(a, all, first[k] + w, list, &stn[0][threadIdx.x]);
 }
 
 int g_weno_grid = 0;  // persistent grid of the evaluation kernel: resident CTAs of the device
@@ -255,13 +311,13 @@ cudaError_t weno_prepare() {
 
 cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfaces, StepState* st, int2* list,
                              bool check_done, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(&st->weno_listed, 0, sizeof(unsigned), s);
+  cudaError_t e = cudaMemsetAsync(st->weno_listed, 0, sizeof(st->weno_listed), s);
   if (e != cudaSuccess || nfaces <= 0) return e;
-  weno_list_kernel<<<(unsigned)((nfaces + LCH - 1) / LCH), LT, 0, s>>>(d, mask, nfaces, st, list, check_done);
+  weno_list_kernel<<<(unsigned)weno_list_ctas(d), LT, 0, s>>>(d, mask, nfaces, st, list, check_done);
   return cudaGetLastError();
 }
 
-int weno_list_ctas(long nfaces) { return (int)((nfaces + LCH - 1) / LCH); }
+int weno_list_ctas(const Dims& d) { return list_ctas_kind(d, 0) + list_ctas_kind(d, 1) + list_ctas_kind(d, 2); }
 
 cudaError_t launch_weno_list_batched(const ListArgs* args, const int* cta, int nblocks, int total, cudaStream_t s) {
   weno_list_reset_batched<<<(nblocks + 255) / 256, 256, 0, s>>>(args, nblocks);

@@ -582,11 +582,11 @@ struct cbns_batch {
   DilateArgs* dil_tab = nullptr;     // 3 passes x nblocks
   AuditArgs* aud_tab = nullptr;      // nblocks
   ListArgs* list_tab = nullptr;      // nblocks
-  int* dil_cta = nullptr;            // nblocks + 1
+  int* dil_cta = nullptr;            // 3 passes x (nblocks + 1)
   int* aud_cta = nullptr;            // nblocks + 1
   int* list_cta = nullptr;           // nblocks + 1
   long* ipre = nullptr;              // 2 x (nblocks + 1): sweep work items of the two kinds
-  int dil_total = 0, aud_total = 0, list_total = 0;
+  int dil_total[3] = {0, 0, 0}, aud_total = 0, list_total = 0;
   long items_total[2] = {0, 0};
   std::vector<int> roles;     // (lq, lp, ls) per block at capture
   std::vector<unsigned long long> gens;  // the blocks' graph_gen at capture
@@ -631,7 +631,7 @@ int batch_sensor_tables(cbns_batch* b) {
     auto up = [](size_t x) { return (x + 255) / 256 * 256; };
     const size_t o1 = up(nb * sizeof(MaskArgs)), o2 = o1 + up(3 * nb * sizeof(DilateArgs)),
                  o3 = o2 + up(nb * sizeof(AuditArgs)), o4 = o3 + up(nb * sizeof(ListArgs)),
-                 o5 = o4 + up((nb + 1) * sizeof(int)), o6 = o5 + up((nb + 1) * sizeof(int)),
+                 o5 = o4 + up(3 * (nb + 1) * sizeof(int)), o6 = o5 + up((nb + 1) * sizeof(int)),
                  o7 = o6 + up((nb + 1) * sizeof(int)), o8 = o7 + up(2 * (nb + 1) * sizeof(long));
     CK(cudaMalloc(&b->stables, o8));
     char* t = static_cast<char*>(b->stables);
@@ -648,7 +648,7 @@ int batch_sensor_tables(cbns_batch* b) {
   std::vector<DilateArgs> dt(3 * nb);
   std::vector<AuditArgs> at(nb);
   std::vector<ListArgs> lt(nb);
-  std::vector<int> dc(nb + 1, 0), ac(nb + 1, 0), lc(nb + 1, 0);
+  std::vector<int> dc(3 * (nb + 1), 0), ac(nb + 1, 0), lc(nb + 1, 0);
   std::vector<long> ip(2 * (nb + 1), 0);
   for (int i = 0; i < nb; ++i) {
     cbns_ctx* c = b->blk[i];
@@ -657,7 +657,8 @@ int batch_sensor_tables(cbns_batch* b) {
     for (int dim = 0; dim < 3; ++dim) dt[dim * nb + i] = ss.w[dim];
     at[i] = ss.au;
     lt[i] = ss.li;
-    dc[i + 1] = dc[i] + sensor_dilate_ctas(c->d);
+    for (int dim = 0; dim < 3; ++dim)
+      dc[dim * (nb + 1) + i + 1] = dc[dim * (nb + 1) + i] + sensor_dilate_ctas(c->d, dim);
     ac[i + 1] = ac[i] + sensor_audit_ctas(ss.au);
     lc[i + 1] = lc[i] + weno_list_ctas(c->d);
     long n0, n1;
@@ -665,7 +666,7 @@ int batch_sensor_tables(cbns_batch* b) {
     ip[i + 1] = ip[i] + n0;
     ip[nb + 1 + i + 1] = ip[nb + 1 + i] + n1;
   }
-  b->dil_total = dc[nb];
+  for (int dim = 0; dim < 3; ++dim) b->dil_total[dim] = dc[dim * (nb + 1) + nb];
   b->aud_total = ac[nb];
   b->list_total = lc[nb];
   b->items_total[0] = ip[nb];
@@ -674,7 +675,7 @@ int batch_sensor_tables(cbns_batch* b) {
   CK(cudaMemcpyAsync(b->dil_tab, dt.data(), 3 * nb * sizeof(DilateArgs), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->aud_tab, at.data(), nb * sizeof(AuditArgs), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->list_tab, lt.data(), nb * sizeof(ListArgs), cudaMemcpyHostToDevice, b->stream));
-  CK(cudaMemcpyAsync(b->dil_cta, dc.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
+  CK(cudaMemcpyAsync(b->dil_cta, dc.data(), 3 * (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->aud_cta, ac.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->list_cta, lc.data(), (nb + 1) * sizeof(int), cudaMemcpyHostToDevice, b->stream));
   CK(cudaMemcpyAsync(b->ipre, ip.data(), 2 * (nb + 1) * sizeof(long), cudaMemcpyHostToDevice, b->stream));
@@ -778,7 +779,8 @@ int batch_enqueue_body(cbns_batch* b) {
     CK(launch_sensor_mask_batched(b->mask_tab, b->ipre, b->ipre + nb + 1, b->items_total[0], b->items_total[1], nb,
                                   b->stream));
     for (int dim = 0; dim < 3; ++dim)
-      CK(launch_sensor_dilate_batched(b->dil_tab + dim * nb, b->dil_cta, nb, b->dil_total, b->stream));
+      CK(launch_sensor_dilate_batched(b->dil_tab + dim * nb, b->dil_cta + dim * (nb + 1), nb, b->dil_total[dim],
+                                      b->stream));
     CK(launch_sensor_audit_batched(b->aud_tab, b->aud_cta, nb, b->aud_total, b->stream));
     CK(launch_weno_list_batched(b->list_tab, b->list_cta, nb, b->list_total, b->stream));
     b->blk[0]->launches += 8;

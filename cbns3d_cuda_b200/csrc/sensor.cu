@@ -204,66 +204,86 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float* __restrict__ 
 }
 
 // ---------------------------------------------------------------- widening
-// Grid: x over the faces of a line along i, y over groups of DL lines along
-// j, z over (direction, k); no index division per face.
-constexpr int DL = 16;
-__device__ __forceinline__ dim3 dilate_grid(const Dims& d) {
-  return dim3((unsigned)((d.IM - 1 + 127) / 128), (unsigned)((d.JM - 1 + DL - 1) / DL), (unsigned)(3 * (d.KM - 1)));
+// Grid of one pass: x over the faces of a line along i (128 per CTA), y over
+// groups of lines along the walked direction, z over (face direction, the
+// third index).  Pass dim 0 and 1: the thread walks j (lines along j, groups
+// of DLJ), the CTA holds k; pass dim 2: the thread walks k (groups of DLK),
+// the CTA holds j.  So the widening of passes 1 and 2 runs along the thread's
+// own walk as a sliding window sum (two loads per face whatever the width),
+// and that of pass 0 along i across the lanes of a warp (shuffles, loads only
+// at the warp's edges).  No index division per face.
+constexpr int DLJ = 16, DLK = 32;
+__host__ __device__ __forceinline__ dim3 dilate_grid(const Dims& d, int dim) {
+  const unsigned gx = (unsigned)((d.IM - 1 + 127) / 128);
+  if (dim == 2) return dim3(gx, (unsigned)((d.KM - 1 + DLK - 1) / DLK), (unsigned)(3 * (d.JM - 1)));
+  return dim3(gx, (unsigned)((d.JM - 1 + DLJ - 1) / DLJ), (unsigned)(3 * (d.KM - 1)));
 }
 
-// CTA (bx, by, bz) of one block's widening grid
+// CTA (bx, by, bz) of one block's widening grid for pass a.dim
 __device__ __forceinline__ void dilate_body(const DilateArgs& a, unsigned bx, unsigned by, unsigned bz) {
   if (a.check_done && a.st->done) return;
-  if (a.hold || !sensor_step(a.st, a.every)) {
-    // decisions of an earlier step: only the statistics
-    if (a.count) {
-      const Dims& d = a.d;
-      const int dir = bz / (d.KM - 1), x2 = bz % (d.KM - 1);
-      const int n0 = dir == 0 ? d.IM - 1 : d.IM - 2, n1 = dir == 1 ? d.JM - 1 : d.JM - 2;
-      const int n2 = dir == 2 ? d.KM - 1 : d.KM - 2;
-      const int first = dir == 0 ? 0 : (dir == 1 ? (d.IM - 1) * (d.JM - 2) * (d.KM - 2)
-                                                 : (d.IM - 1) * (d.JM - 2) * (d.KM - 2) +
-                                                       (d.IM - 2) * (d.JM - 1) * (d.KM - 2));
-      const int x0 = bx * 128 + threadIdx.x;
-      unsigned cnt = 0;
-      if (x2 < n2 && x0 < n0) {
-        const int y0 = by * DL, y1 = min(n1, y0 + DL);
-        for (int x1 = y0; x1 < y1; ++x1) cnt += __ldg(a.out + first + x0 + n0 * (x1 + n1 * x2));
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-      if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&a.st->weno_faces, (unsigned long long)cnt);
-    }
-    return;
-  }
   const Dims& d = a.d;
   const int IM = d.IM, JM = d.JM, KM = d.KM;
-  const int dir = bz / (KM - 1), x2 = bz % (KM - 1);
-  const int x0 = bx * 128 + threadIdx.x;
+  const bool walk_k = a.dim == 2;
+  const int zc = walk_k ? JM - 1 : KM - 1;
+  const int dir = (int)bz / zc, fixed = (int)bz % zc;
   // extents (n0, n1, n2) and first index of this direction's faces
   const int n0 = dir == 0 ? IM - 1 : IM - 2, n1 = dir == 1 ? JM - 1 : JM - 2, n2 = dir == 2 ? KM - 1 : KM - 2;
-  const int first = dir == 0 ? 0 : (dir == 1 ? (IM - 1) * (JM - 2) * (KM - 2)
-                                             : (IM - 1) * (JM - 2) * (KM - 2) + (IM - 2) * (JM - 1) * (KM - 2));
-  if (x2 >= n2) return;  // uniform per CTA
+  const long first = dir == 0 ? 0
+                              : (dir == 1 ? (long)(IM - 1) * (JM - 2) * (KM - 2)
+                                          : (long)(IM - 1) * (JM - 2) * (KM - 2) + (long)(IM - 2) * (JM - 1) * (KM - 2));
+  if (fixed >= (walk_k ? n1 : n2)) return;  // uniform per CTA
+  const int x0 = (int)bx * 128 + (int)threadIdx.x;
   const bool valid = x0 < n0;
-  const int w = a.dim == dir ? a.along : a.across;
-  const int len = a.dim == 0 ? n0 : (a.dim == 1 ? n1 : n2);
-  const int stride = a.dim == 0 ? 1 : (a.dim == 1 ? n0 : n0 * n1);
+  // the thread's walk: positions q0 .. q1-1 along j (walk_k: along k), face
+  // index base + q * step
+  const int nq = walk_k ? n2 : n1, dl = walk_k ? DLK : DLJ;
+  const int q0 = (int)by * dl, q1 = min(nq, q0 + dl);
+  const long step = walk_k ? (long)n0 * n1 : (long)n0;
+  const long base = first + x0 + (walk_k ? (long)n0 * fixed : (long)n0 * n1 * fixed);
   unsigned cnt = 0;
-  const unsigned char* __restrict__ in = a.in;
-  unsigned char* __restrict__ out = a.out;
-  const int y0 = by * DL, y1 = min(n1, y0 + DL);
-  if (valid) {
-    // all lines' loads are independent: let them be in flight together
-#pragma unroll 4
-    for (int x1 = y0; x1 < y1; ++x1) {
-      const int e = first + x0 + n0 * (x1 + n1 * x2);
-      const int pos = a.dim == 0 ? x0 : (a.dim == 1 ? x1 : x2);
-      unsigned char dec = 0;
-      const int lo = max(-w, -pos), hi = min(w, len - 1 - pos);
-      for (int o = lo; o <= hi; ++o) dec |= __ldg(in + e + o * stride);
-      out[e] = dec;
-      cnt += dec;
+  if (a.hold || !sensor_step(a.st, a.every)) {
+    // decisions of an earlier step: only the statistics
+    if (a.count && valid)
+      for (int q = q0; q < q1; ++q) cnt += __ldg(a.out + base + q * step);
+  } else {
+    const unsigned char* __restrict__ in = a.in;
+    unsigned char* __restrict__ out = a.out;
+    const int w = a.dim == dir ? a.along : a.across;
+    if (a.dim == 0) {
+      // along i, across the warp's lanes
+      const int lane = threadIdx.x & 31;
+      for (int q = q0; q < q1; ++q) {
+        const long e = base + q * step;
+        const unsigned v = valid ? __ldg(in + e) : 0u;
+        unsigned dec = v;
+        if (w <= 31) {
+          for (int o = 1; o <= w; ++o) {
+            unsigned l = __shfl_up_sync(0xffffffffu, v, o), r = __shfl_down_sync(0xffffffffu, v, o);
+            if (lane < o) l = (valid && x0 - o >= 0) ? __ldg(in + e - o) : 0u;  // left of the warp
+            if (lane + o > 31) r = (valid && x0 + o < n0) ? __ldg(in + e + o) : 0u;  // right of the warp
+            dec |= l | r;
+          }
+        } else if (valid) {
+          const int lo = max(-w, -x0), hi = min(w, n0 - 1 - x0);
+          for (int o = lo; o <= hi; ++o) dec |= __ldg(in + e + o);
+        }
+        if (valid) {
+          out[e] = (unsigned char)dec;
+          cnt += dec;
+        }
+      }
+    } else if (valid) {
+      // along the walk: a sliding window sum of the 0/1 decisions
+      int sum = 0;
+      for (int q = max(0, q0 - w); q <= min(nq - 1, q0 + w); ++q) sum += __ldg(in + base + q * step);
+      for (int q = q0; q < q1; ++q) {
+        const unsigned dec = sum > 0 ? 1u : 0u;
+        out[base + q * step] = (unsigned char)dec;
+        cnt += dec;
+        if (q - w >= 0) sum -= __ldg(in + base + (q - w) * step);
+        if (q + 1 + w < nq) sum += __ldg(in + base + (q + 1 + w) * step);
+      }
     }
   }
   if (a.count) {
@@ -278,11 +298,11 @@ __global__ void __launch_bounds__(128) sensor_dilate_kernel(const DilateArgs a) 
 }
 
 // Many blocks in one launch: block b owns CTAs cta[b] .. cta[b+1]-1, args[b]
-// are its DilateArgs.
+// are its DilateArgs (all of one pass).
 __global__ void __launch_bounds__(128) sensor_dilate_batched(const DilateArgs* args, const int* cta, int nblocks) {
   const int b = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const DilateArgs& a = args[b];
-  const dim3 g = dilate_grid(a.d);
+  const dim3 g = dilate_grid(a.d, a.dim);
   const unsigned l = blockIdx.x - (unsigned)__ldg(cta + b);
   dilate_body(a, l % g.x, (l / g.x) % g.y, l / (g.x * g.y));
 }
@@ -385,14 +405,13 @@ cudaError_t launch_sensor_audit(const AuditArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-int sensor_dilate_ctas(const Dims& d) {
-  return ((d.IM - 1 + 127) / 128) * ((d.JM - 1 + DL - 1) / DL) * (3 * (d.KM - 1));
+int sensor_dilate_ctas(const Dims& d, int dim) {
+  const dim3 g = dilate_grid(d, dim);
+  return (int)(g.x * g.y * g.z);
 }
 
 cudaError_t launch_sensor_dilate(const DilateArgs& a, cudaStream_t s) {
-  const dim3 grid((unsigned)((a.d.IM - 1 + 127) / 128), (unsigned)((a.d.JM - 1 + DL - 1) / DL),
-                  (unsigned)(3 * (a.d.KM - 1)));
-  sensor_dilate_kernel<<<grid, 128, 0, s>>>(a);
+  sensor_dilate_kernel<<<dilate_grid(a.d, a.dim), 128, 0, s>>>(a);
   return cudaGetLastError();
 }
 

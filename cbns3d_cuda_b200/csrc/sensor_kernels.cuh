@@ -88,7 +88,7 @@ cudaError_t launch_sensor_dilate(const DilateArgs& a, cudaStream_t s);
 // block's count below.  Mask: ipre[b] .. ipre[b+1]-1 are block b's work items
 // of each kind (sensor_mask_items); every block's MaskArgs::params must hold
 // the same network (it is loaded once per CTA, from args[0]).
-int sensor_dilate_ctas(const Dims& d);
+int sensor_dilate_ctas(const Dims& d, int dim);  // pass dim's grid
 int sensor_audit_ctas(const AuditArgs& a);
 void sensor_mask_items(const Dims& d, long* items0, long* items1);
 cudaError_t launch_sensor_dilate_batched(const DilateArgs* args, const int* cta, int nblocks, int total,

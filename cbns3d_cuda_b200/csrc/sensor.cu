@@ -210,8 +210,8 @@ __global__ void __launch_bounds__(GT) mlp_grad_kernel(const float* __restrict__ 
 // of DLJ), the CTA holds k; pass dim 2: the thread walks k (groups of DLK),
 // the CTA holds j.  So the widening of passes 1 and 2 runs along the thread's
 // own walk as a sliding window sum (two loads per face whatever the width),
-// and that of pass 0 along i across the lanes of a warp (shuffles, loads only
-// at the warp's edges).  No index division per face.
+// and that of pass 0 along i from a line segment staged in shared memory with
+// its halo.  No index division per face.
 constexpr int DLJ = 16, DLK = 32;
 __host__ __device__ __forceinline__ dim3 dilate_grid(const Dims& d, int dim) {
   const unsigned gx = (unsigned)((d.IM - 1 + 127) / 128);
@@ -251,19 +251,26 @@ __device__ __forceinline__ void dilate_body(const DilateArgs& a, unsigned bx, un
     unsigned char* __restrict__ out = a.out;
     const int w = a.dim == dir ? a.along : a.across;
     if (a.dim == 0) {
-      // along i, across the warp's lanes
-      const int lane = threadIdx.x & 31;
+      // along i: each line's 128 faces and a halo of w either side staged in
+      // shared memory (coalesced), then each thread ORs its window there
+      constexpr int WMAX = 16;
+      __shared__ unsigned char row[128 + 2 * WMAX];
+      const int t = threadIdx.x;
+      const int xb = (int)bx * 128;  // first face of the CTA's segment
       for (int q = q0; q < q1; ++q) {
-        const long e = base + q * step;
-        const unsigned v = valid ? __ldg(in + e) : 0u;
-        unsigned dec = v;
-        if (w <= 31) {
-          for (int o = 1; o <= w; ++o) {
-            unsigned l = __shfl_up_sync(0xffffffffu, v, o), r = __shfl_down_sync(0xffffffffu, v, o);
-            if (lane < o) l = (valid && x0 - o >= 0) ? __ldg(in + e - o) : 0u;  // left of the warp
-            if (lane + o > 31) r = (valid && x0 + o < n0) ? __ldg(in + e + o) : 0u;  // right of the warp
-            dec |= l | r;
+        const long e = base + q * step;  // this thread's face (x0 = xb + t)
+        unsigned dec = 0;
+        if (w <= WMAX) {
+          __syncthreads();  // the previous line's window reads are done
+          row[WMAX + t] = valid ? __ldg(in + e) : 0;
+          if (t < WMAX) {
+            const int xl = xb - WMAX + t, xr = xb + 128 + t;  // halo faces
+            row[t] = (xl >= 0 && xl < n0) ? __ldg(in + e - WMAX) : 0;
+            row[WMAX + 128 + t] = (xr < n0) ? __ldg(in + e + 128) : 0;
           }
+          __syncthreads();
+          if (valid)
+            for (int o = -w; o <= w; ++o) dec |= row[WMAX + t + o];
         } else if (valid) {
           const int lo = max(-w, -x0), hi = min(w, n0 - 1 - x0);
           for (int o = lo; o <= hi; ++o) dec |= __ldg(in + e + o);

@@ -95,6 +95,37 @@ __device__ __forceinline__ R weno5(R a, R b, R c, R d, R e) {
   }
 }
 
+// FP64 WENO5-JS values of the two sides of one characteristic field at once,
+// sharing one division: with the low side's value n_l/d_l and the high
+// side's n_h/d_h (weno5's numerator and denominator), 1/(d_l d_h) times d_h
+// and d_l gives both (simultaneous inversion, Montgomery 1987).  The
+// denominators are 6 (a1 + a2 + a3) with a_k ~ 1/s_k^2 scaled by s1^2 s2^2
+// s3^2, s_k >= 1e-6, so their product stays far inside the FP64 range.
+__device__ __forceinline__ void weno5_pair(double a, double b, double c, double d, double e, double f,
+                                           double* lo, double* hi) {
+  // low side from a b c d e, high side from f e d c b
+  auto nd = [](double a, double b, double c, double d, double e, double* n, double* den) {
+    const double eps = 1.0e-6, c13 = 13.0 / 12.0;
+    const double d1 = a - 2.0 * b + c, e1 = a - 4.0 * b + 3.0 * c;
+    const double d2 = b - 2.0 * c + d, e2 = b - d;
+    const double d3 = c - 2.0 * d + e, e3 = 3.0 * c - 4.0 * d + e;
+    const double s1 = c13 * d1 * d1 + 0.25 * e1 * e1 + eps;
+    const double s2 = c13 * d2 * d2 + 0.25 * e2 * e2 + eps;
+    const double s3 = c13 * d3 * d3 + 0.25 * e3 * e3 + eps;
+    const double p1 = 2.0 * a - 7.0 * b + 11.0 * c, p2 = -b + 5.0 * c + 2.0 * d, p3 = 2.0 * c + 5.0 * d - e;
+    const double t1 = s1 * s1, t2 = s2 * s2, t3 = s3 * s3;
+    const double a1 = 0.1 * (t2 * t3), a2 = 0.6 * (t1 * t3), a3 = 0.3 * (t1 * t2);
+    *n = a1 * p1 + a2 * p2 + a3 * p3;
+    *den = 6.0 * (a1 + a2 + a3);
+  };
+  double nl, dl, nh, dh;
+  nd(a, b, c, d, e, &nl, &dl);
+  nd(f, e, d, c, b, &nh, &dh);
+  const double r = 1.0 / (dl * dh);
+  *lo = nl * (dh * r);
+  *hi = nh * (dl * r);
+}
+
 // Local Lax-Friedrichs flux from the two reconstructed states (the reference's
 // lf_flux with R = the high side H, L = the low side): the component-wise
 // Cartesian wave-speed bound, flux = (F_L + F_H - ws (U_H - U_L)) / 2.
@@ -216,10 +247,7 @@ __device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const 
       W[4][p] = mx * f1 + my * f2 + mz * f3 - qm * f0;
     }
 #pragma unroll
-    for (int s = 0; s < 5; ++s) {
-      wl[s] = weno5<R>(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4]);
-      wh[s] = weno5<R>(W[s][5], W[s][4], W[s][3], W[s][2], W[s][1]);
-    }
+    for (int s = 0; s < 5; ++s) weno5_pair(W[s][0], W[s][1], W[s][2], W[s][3], W[s][4], W[s][5], &wl[s], &wh[s]);
   } else {
     {
       R W[3][6];

@@ -20,8 +20,11 @@
 //     (w0,w2 = A +- B, w1 = f0 - 2A, w3,w4 = tangential momenta) and the right
 //     eigenvectors likewise, instead of 5x5 matrix products;
 //   * each WENO5 value costs one division (weights scaled by the product of
-//     the squared smoothness indicators) in FP64; the FP32 form uses fast
-//     reciprocals.
+//     the squared smoothness indicators); in FP64 the two sides of a field
+//     share it, and so do the two densities of the Roe average and of the
+//     reconstructed states (simultaneous inversion), and the second tangent
+//     is normalised with the product of the other two norms; the FP32 form
+//     uses fast reciprocals.
 // FP32 reciprocals and square roots are the approximate hardware forms (PTX
 // rcp.approx.ftz / sqrt.approx.ftz, within 2 ulp): the FP32 flux carries ~1e-7
 // relative error anyway, and the correctly rounded forms cost a Newton step and
@@ -150,6 +153,29 @@ __device__ __forceinline__ void lf_flux_prims(R Lr, R Lu, R Lv, R Lw, R Lp, R Hr
   out[4] = R(0.5) * (mL * HL + mH * HH - ws * (EH - EL));
 }
 
+// The same with the densities' reciprocals given (the FP64 face flux forms
+// them together).
+template <typename R>
+__device__ __forceinline__ void lf_flux_prims_inv(R Lr, R Lu, R Lv, R Lw, R Lp, R Hr, R Hu, R Hv, R Hw, R Hp, R iLr, R iHr, R nx,
+                                              R ny, R nz, const FluxConsts<R>& C, R out[5]) {
+  const R gamma = C.gamma, gam1_inv = C.gam1_inv;
+  const R kH = Hu * Hu + Hv * Hv + Hw * Hw, kL = Lu * Lu + Lv * Lv + Lw * Lw;
+  const R cH = sqrt_(gamma * Hp * iHr), cL = sqrt_(gamma * Lp * iLr);
+  const R HH = cH * cH * gam1_inv + R(0.5) * kH, HL = cL * cL * gam1_inv + R(0.5) * kL;
+  const R EH = Hp * gam1_inv + R(0.5) * Hr * kH, EL = Lp * gam1_inv + R(0.5) * Lr * kL;
+  const R qH = Hu * nx + Hv * ny + Hw * nz, qL = Lu * nx + Lv * ny + Lw * nz;
+  const R sx = fmax(fabs(Hu) + cH, fabs(Lu) + cL);
+  const R sy = fmax(fabs(Hv) + cH, fabs(Lv) + cL);
+  const R sz = fmax(fabs(Hw) + cH, fabs(Lw) + cL);
+  const R ws = fabs(sx * nx + sy * ny + sz * nz);
+  const R mL = Lr * qL, mH = Hr * qH;
+  out[0] = R(0.5) * (mL + mH - ws * (Hr - Lr));
+  out[1] = R(0.5) * (mL * Lu + Lp * nx + mH * Hu + Hp * nx - ws * (Hr * Hu - Lr * Lu));
+  out[2] = R(0.5) * (mL * Lv + Lp * ny + mH * Hv + Hp * ny - ws * (Hr * Hv - Lr * Lv));
+  out[3] = R(0.5) * (mL * Lw + Lp * nz + mH * Hw + Hp * nz - ws * (Hr * Hw - Lr * Lw));
+  out[4] = R(0.5) * (mL * HL + mH * HH - ws * (EH - EL));
+}
+
 // Flux through the face between stencil points 2 (node a) and 3 (node b).
 // ld(p, n) returns conservative variable n at stencil point p (p = 0..5 are the
 // nodes a-2 .. b+2 along the face normal).  (nx,ny,nz) is the face area vector
@@ -162,7 +188,22 @@ __device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const 
   // node primitives at a and b (the reference reads them from the primitive
   // arrays, which hold exactly these values on every node a face touches)
   R ra, ua, va, wa, pa, rb, ub, vb, wb, pb, ira, irb;
-  {
+  if constexpr (sizeof(R) == 8) {
+    // both densities' reciprocals from one division
+    ra = ld(2, 0);
+    rb = ld(3, 0);
+    const R rab = rcp_(ra * rb);
+    ira = rb * rab;
+    irb = ra * rab;
+    ua = ld(2, 1) * ira;
+    va = ld(2, 2) * ira;
+    wa = ld(2, 3) * ira;
+    pa = gam1 * (ld(2, 4) - R(0.5) * ra * (ua * ua + va * va + wa * wa));
+    ub = ld(3, 1) * irb;
+    vb = ld(3, 2) * irb;
+    wb = ld(3, 3) * irb;
+    pb = gam1 * (ld(3, 4) - R(0.5) * rb * (ub * ub + vb * vb + wb * wb));
+  } else {
     ra = ld(2, 0);
     ira = rcp_(ra);
     ua = ld(2, 1) * ira;
@@ -201,7 +242,10 @@ __device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const 
     lx *= il;
     ly *= il;
     lz *= il;
-    const R im = rsqrt(mx * mx + my * my + mz * mz);
+    // |m| = |l| |n| in both branches above (m = n x l up to sign)
+    R im;
+    if constexpr (sizeof(R) == 8) im = il * in;
+    else im = rsqrt(mx * mx + my * my + mz * mz);
     mx *= im;
     my *= im;
     mz *= im;
@@ -295,23 +339,45 @@ __device__ __forceinline__ void face_flux(const LD& ld, R nx, R ny, R nz, const 
       q[3] = ww * q[0] + uz * d + lz * w[3] + mz * w[4];
       q[4] = H * s + qn * d + hq * w[1] + ql * w[3] + qm * w[4];
     };
-    back(wl);
-    Lr = q[0];
-    {
-      const R i = rcp_(Lr);
-      Lu = q[1] * i;
-      Lv = q[2] * i;
-      Lw = q[3] * i;
-      Lp = gam1 * (q[4] - R(0.5) * Lr * (Lu * Lu + Lv * Lv + Lw * Lw));
-    }
-    back(wh);
-    Hr = q[0];
-    {
-      const R i = rcp_(Hr);
-      Hu = q[1] * i;
-      Hv = q[2] * i;
-      Hw = q[3] * i;
+    if constexpr (sizeof(R) == 8) {
+      // both sides' densities inverted with one division
+      back(wl);
+      R lq[5];
+#pragma unroll
+      for (int n = 0; n < 5; ++n) lq[n] = q[n];
+      back(wh);
+      Lr = lq[0];
+      Hr = q[0];
+      const R rlh = rcp_(Lr * Hr), iL = Hr * rlh, iH = Lr * rlh;
+      Lu = lq[1] * iL;
+      Lv = lq[2] * iL;
+      Lw = lq[3] * iL;
+      Lp = gam1 * (lq[4] - R(0.5) * Lr * (Lu * Lu + Lv * Lv + Lw * Lw));
+      Hu = q[1] * iH;
+      Hv = q[2] * iH;
+      Hw = q[3] * iH;
       Hp = gam1 * (q[4] - R(0.5) * Hr * (Hu * Hu + Hv * Hv + Hw * Hw));
+      lf_flux_prims_inv<R>(Lr, Lu, Lv, Lw, Lp, Hr, Hu, Hv, Hw, Hp, iL, iH, nx, ny, nz, C, out);
+      return;
+    } else {
+      back(wl);
+      Lr = q[0];
+      {
+        const R i = rcp_(Lr);
+        Lu = q[1] * i;
+        Lv = q[2] * i;
+        Lw = q[3] * i;
+        Lp = gam1 * (q[4] - R(0.5) * Lr * (Lu * Lu + Lv * Lv + Lw * Lw));
+      }
+      back(wh);
+      Hr = q[0];
+      {
+        const R i = rcp_(Hr);
+        Hu = q[1] * i;
+        Hv = q[2] * i;
+        Hw = q[3] * i;
+        Hp = gam1 * (q[4] - R(0.5) * Hr * (Hu * Hu + Hv * Hv + Hw * Hw));
+      }
     }
   }
 

@@ -67,8 +67,9 @@ struct RowSmem {
 // The window sweeps stream each column's nodes through a per-thread ring of
 // SW_D slots filled by asynchronous copies (cp.async), SW_D faces ahead: slot
 // u % SW_D holds the 5 state values of node f0+3+u and the area vector of
-// node f0+1+u for face f0+u.
-constexpr int SW_D = 4;
+// node f0+1+u for face f0+u.  Two slots keep the sweep at 5 CTAs per SM (16
+// KB of ring; four slots and 4 CTAs per SM measured 2% slower).
+constexpr int SW_D = 2;
 struct WinSmem {
   double v[SW_D][8][SW_T];
 };
@@ -347,9 +348,10 @@ __device__ __forceinline__ void mask_teardown(const MaskSmem& m, int t) {
 }
 
 // KIND 0: the i-face rows; KIND 1: the j- and k-face window sweeps (two
-// launches, so that each path gets its own register allocation).
+// launches, so that each path gets its own register allocation; both at 5
+// CTAs per SM).
 template <int KIND>
-__global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(const MaskArgs a) {
+__global__ void __launch_bounds__(SW_T, 5) sensor_mask_kernel(const MaskArgs a) {
   if ((a.check_done && a.st->done) || !sensor_step(a.st, a.every)) return;
   const int t = threadIdx.x;
   const MaskSmem m = mask_setup(a.params, t);
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_kernel(co
 // carries the same network).  After a tensor-core wait timed out, a CTA
 // marks the block of each item it still owns as failed (WENO5 everywhere).
 template <int KIND>
-__global__ void __launch_bounds__(SW_T, KIND == 0 ? 5 : 4) sensor_mask_batched(const MaskArgs* args, const long* ipre,
+__global__ void __launch_bounds__(SW_T, 5) sensor_mask_batched(const MaskArgs* args, const long* ipre,
                                                                               int nblocks) {
   const int t = threadIdx.x;
   const long total = ipre[nblocks];
@@ -401,7 +403,7 @@ constexpr int kMaskSmem0 = (int)(sizeof(tc::Smem) + sizeof(RowSmem)) + 128;
 constexpr int kMaskSmem1 = (int)(sizeof(tc::Smem) + sizeof(WinSmem)) + 128;
 // at most 8 CTAs per SM hold TMEM (64 columns each of 512); the two launches
 // of a sweep run back to back on the stream
-constexpr long kMaskCap0 = 148L * 5, kMaskCap1 = 148L * 4;
+constexpr long kMaskCap0 = 148L * 5, kMaskCap1 = 148L * 5;
 
 cudaError_t mask_prepare() {
   static bool attr = false;

@@ -414,6 +414,7 @@ SensorSet sensor_set(cbns_ctx* c, const double* q, bool check_done, bool every_s
   l.st = c->st;
   l.list = c->wlist;
   l.check_done = check_done;
+  l.every = every;
   return ss;
 }
 
@@ -447,7 +448,7 @@ int sensor_launch(cbns_ctx* c, const double* q, bool check_done, bool every_step
   n += 1;
   if (!hold) {
     Prof p(c, PK_WENO);
-    CK(launch_weno_list(c->d, c->mask, c->nfaces, c->st, c->wlist, check_done, c->stream));
+    CK(launch_weno_list(c->d, c->mask, c->nfaces, c->st, c->wlist, check_done, ss.m.every, c->stream));
     n += 1;
   }
   c->launches += n;  // sensor sweeps, widening passes, the audit, the WENO5-face list

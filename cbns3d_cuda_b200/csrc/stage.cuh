@@ -59,7 +59,7 @@ int stage_variants(bool fp32, bool hybrid);
 // decisions are final; each face kind in its own list, st->weno_listed[kind]
 // receiving its length) ...
 cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfaces, StepState* st, int2* list,
-                             bool check_done, cudaStream_t s);
+                             bool check_done, unsigned every, cudaStream_t s);
 // ... and evaluate the listed faces (every face while force_weno is set) into
 // a.wflux, where the stage kernel reads them: before each hybrid stage-kernel
 // launch, on the same input.
@@ -75,6 +75,7 @@ struct ListArgs {
   StepState* st;
   int2* list;
   int check_done;
+  unsigned every;  // the network's interval (MaskArgs::every): the lists are rebuilt on its steps only
 };
 int weno_list_ctas(const Dims& d);
 cudaError_t launch_weno_list_batched(const ListArgs* args, const int* cta, int nblocks, int total, cudaStream_t s);

@@ -20,6 +20,7 @@
 // compute for it.
 #include "cbns_common.cuh"
 #include "face_flux.cuh"
+#include "sensor_kernels.cuh"
 #include "stage.cuh"
 
 namespace cbns {
@@ -102,12 +103,13 @@ __host__ __device__ __forceinline__ int list_ctas_kind(const Dims& d, int kind) 
 // pass can walk the three kinds side by side, plane by plane.  One 16-byte
 // load of decisions per thread; a CTA-wide scan of the counts and one global
 // atomic per CTA place the CTA's faces in its kind's list, in face order
-// within the CTA.
+// within the CTA.  The decisions change only on the steps the network runs
+// (sensor_step), so on the others the lists of the last such step stand.
 __device__ __forceinline__ void list_body(const Dims& d, const unsigned char* __restrict__ mask, long nf, StepState* st,
-                                          int2* __restrict__ list, int check_done, unsigned bx) {
+                                          int2* __restrict__ list, int check_done, unsigned every, unsigned bx) {
   __shared__ int wsum[LT / 32];
   __shared__ int cbase;
-  if (check_done && st->done) return;
+  if ((check_done && st->done) || !sensor_step(st, every)) return;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   int kind = 0;
   unsigned chunk = bx;
@@ -178,22 +180,28 @@ __device__ __forceinline__ void list_body(const Dims& d, const unsigned char* __
 }
 
 __global__ void __launch_bounds__(LT) weno_list_kernel(const Dims d, const unsigned char* __restrict__ mask, long nf,
-                                                       StepState* st, int2* __restrict__ list, int check_done) {
-  list_body(d, mask, nf, st, list, check_done, blockIdx.x);
+                                                       StepState* st, int2* __restrict__ list, int check_done,
+                                                       unsigned every) {
+  list_body(d, mask, nf, st, list, check_done, every, blockIdx.x);
+}
+
+// Zero the lists' lengths on the steps the lists are built anew.
+__global__ void weno_list_reset(StepState* st, int check_done, unsigned every) {
+  if (threadIdx.x < 3 && !(check_done && st->done) && sensor_step(st, every)) st->weno_listed[threadIdx.x] = 0;
 }
 
 // Many blocks: zero every block's count, then list every block's faces (block
 // b owning CTAs cta[b] .. cta[b+1]-1).
 __global__ void weno_list_reset_batched(const ListArgs* args, int nblocks) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < nblocks && !(args[b].check_done && args[b].st->done))
+  if (b < nblocks && !(args[b].check_done && args[b].st->done) && sensor_step(args[b].st, args[b].every))
     for (int k = 0; k < 3; ++k) args[b].st->weno_listed[k] = 0;
 }
 
 __global__ void __launch_bounds__(LT) weno_list_batched(const ListArgs* args, const int* cta, int nblocks) {
   const int b = block_of_cta(cta, nblocks, (int)blockIdx.x);
   const ListArgs& a = args[b];
-  list_body(a.d, a.mask, a.nf, a.st, a.list, a.check_done, blockIdx.x - (unsigned)__ldg(cta + b));
+  list_body(a.d, a.mask, a.nf, a.st, a.list, a.check_done, a.every, blockIdx.x - (unsigned)__ldg(cta + b));
 }
 
 // The WENO5 flux of one face of a's stage input into a.wflux: face w of the
@@ -310,10 +318,10 @@ cudaError_t weno_prepare() {
 }
 
 cudaError_t launch_weno_list(const Dims& d, const unsigned char* mask, long nfaces, StepState* st, int2* list,
-                             bool check_done, cudaStream_t s) {
-  cudaError_t e = cudaMemsetAsync(st->weno_listed, 0, sizeof(st->weno_listed), s);
-  if (e != cudaSuccess || nfaces <= 0) return e;
-  weno_list_kernel<<<(unsigned)weno_list_ctas(d), LT, 0, s>>>(d, mask, nfaces, st, list, check_done);
+                             bool check_done, unsigned every, cudaStream_t s) {
+  weno_list_reset<<<1, 32, 0, s>>>(st, check_done, every);
+  if (nfaces > 0)
+    weno_list_kernel<<<(unsigned)weno_list_ctas(d), LT, 0, s>>>(d, mask, nfaces, st, list, check_done, every);
   return cudaGetLastError();
 }
 

@@ -64,6 +64,7 @@ struct StepState {
   int force_weno;                 // hybrid: the audit rejected this step's sensor decisions
   unsigned audit_fail_steps;      // hybrid: steps whose sensor decisions the audit rejected
   unsigned long long weno_faces;  // hybrid: faces sent to WENO5 (summed over steps)
+  unsigned long long weno_last;   // hybrid: faces the last widening sent to WENO5 (the held steps' count)
   unsigned long long audit_faces; // hybrid: faces the audit re-evaluated
   float audit_max;                // hybrid: largest relative flux difference the audit saw
   int sensor_fail;                // hybrid: a tensor-core wait timed out

@@ -222,6 +222,13 @@ __host__ __device__ __forceinline__ dim3 dilate_grid(const Dims& d, int dim) {
 // CTA (bx, by, bz) of one block's widening grid for pass a.dim
 __device__ __forceinline__ void dilate_body(const DilateArgs& a, unsigned bx, unsigned by, unsigned bz) {
   if (a.check_done && a.st->done) return;
+  const bool lead = bx == 0 && by == 0 && bz == 0 && threadIdx.x == 0;
+  if (a.hold || !sensor_step(a.st, a.every)) {
+    // decisions of an earlier step: only the statistics, that step's count
+    if (a.count && lead) atomicAdd(&a.st->weno_faces, a.st->weno_last);
+    return;
+  }
+  if (a.dim == 0 && lead) a.st->weno_last = 0;  // the last pass counts anew
   const Dims& d = a.d;
   const int IM = d.IM, JM = d.JM, KM = d.KM;
   const bool walk_k = a.dim == 2;
@@ -242,11 +249,7 @@ __device__ __forceinline__ void dilate_body(const DilateArgs& a, unsigned bx, un
   const long step = walk_k ? (long)n0 * n1 : (long)n0;
   const long base = first + x0 + (walk_k ? (long)n0 * fixed : (long)n0 * n1 * fixed);
   unsigned cnt = 0;
-  if (a.hold || !sensor_step(a.st, a.every)) {
-    // decisions of an earlier step: only the statistics
-    if (a.count && valid)
-      for (int q = q0; q < q1; ++q) cnt += __ldg(a.out + base + q * step);
-  } else {
+  {
     const unsigned char* __restrict__ in = a.in;
     unsigned char* __restrict__ out = a.out;
     const int w = a.dim == dir ? a.along : a.across;
@@ -296,7 +299,10 @@ __device__ __forceinline__ void dilate_body(const DilateArgs& a, unsigned bx, un
   if (a.count) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&a.st->weno_faces, (unsigned long long)cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) {
+      atomicAdd(&a.st->weno_faces, (unsigned long long)cnt);
+      atomicAdd(&a.st->weno_last, (unsigned long long)cnt);
+    }
   }
 }
 

@@ -233,6 +233,7 @@ def device_pass(case, precision, K, W, torch, dist, clocks=None, keep_state=Fals
     stream = torch.cuda.Stream()  # a real stream: the legacy default stream cannot be graph-captured
     b.set_stream(stream.cuda_stream)
     out = {"variant": b.autotune()}
+    out["kchunk"] = b.stage_kchunk()
     b.set_time(0.0)
     b.run(W)
     if precision == PREC_HYBRID:
@@ -485,7 +486,7 @@ def run_ours(a):
                        "sensor": {"weights": os.path.relpath(a.sensor, ROOT), "tau": SENSOR[1]}},
             "rho_l2_vs_fp64": l2_h, "rho_linf_vs_fp64": linf_h,
             "plain_vs_reference_linf": ref_cmp["max"] if ref_cmp else None,
-            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "stage_variant": p64["variant"],
+            "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "stage_variant": p64["variant"], "stage_kchunk": p64["kchunk"],
                                "kernels": kern_ms(kern64),
                                "roofline_hbm": {"achieved": ach64, "peak": peak, "unit": "GB/s",
                                                 "frac": (ach64 / peak) if ach64 else None, "traffic": traffic64},
@@ -496,13 +497,13 @@ def run_ours(a):
                                                  "nominal": FP64_NOMINAL_TFLOPS},
                                "e2e": e2e64, "plain_vs_reference": ref_cmp},
                       "split": {"value": value32, "ms_per_step": ms32 / K, "rho_l2_vs_fp64": l2_32,
-                                "rho_linf_vs_fp64": linf_32, "stage_variant": variant32,
+                                "rho_linf_vs_fp64": linf_32, "stage_variant": variant32, "stage_kchunk": p32["kchunk"],
                                 "kernels": kern_ms(kern32)},
                       "hybrid": {"value": value, "ms_per_step": msh / K, "rho_l2_vs_fp64": l2_h,
                                  "rho_linf_vs_fp64": linf_h, "weno_face_fraction": weno_frac,
                                  "audit_rejected_steps": stats["audit_fail_steps"],
                                  "audit_faces": stats["audit_faces"], "audit_max_rel_diff": stats["audit_max"],
-                                 "sensor_timeouts": stats["sensor_fail"], "stage_variant": varianth,
+                                 "sensor_timeouts": stats["sensor_fail"], "stage_variant": varianth, "stage_kchunk": ph["kchunk"],
                                  "kernels": kern_ms(kernh)},
                       "batch": batch,
                       "hybrid_over_fp64": value / value64, "hybrid_over_split": value / value32},

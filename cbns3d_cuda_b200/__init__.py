@@ -225,6 +225,13 @@ class Block:
         _abi.check(self.lib.cbns_stage_variant(self.h, int(variant), C.byref(n)), "cbns_stage_variant")
         return n.value
 
+    def stage_kchunk(self, kchunk: int = -1) -> int:
+        """Use k chunks of `kchunk` planes in the stage kernel (-1: only
+        query); returns the chunk in use."""
+        n = C.c_int()
+        _abi.check(self.lib.cbns_stage_kchunk(self.h, int(kchunk), C.byref(n)), "cbns_stage_kchunk")
+        return n.value
+
     # timing -----------------------------------------------------------------
     def prof_enable(self, on=True):
         _abi.check(self.lib.cbns_prof_enable(self.h, int(on)), "cbns_prof_enable")

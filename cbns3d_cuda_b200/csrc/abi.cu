@@ -65,7 +65,7 @@ struct cbns_ctx {
   unsigned long long graph_gen = 0;
   int g_q = -1, g_p = -1, g_s = -1;
   int ntile_i = 1, ntile_j = 1, kchunk = 1;
-  int stage_variant = 0;  // compiled occupancy variant of the stage kernel (cbns_autotune)
+  int stage_variant = 0;  // compiled variant of the stage kernel (set in cbns_create, cbns_autotune)
   int nsm = 148;          // SMs of the device
   StageMaps tm[3];        // FP32 precisions: TMA maps of the stage kernel, per state buffer
   // hybrid flux: the learned sensor's parameters and per-face decisions
@@ -146,6 +146,17 @@ int kchunk_by_waves(int ntiles, int nint, int slots, double warm) {
   return best_k;
 }
 
+// The chunk for about `waves` waves of `slots` CTAs, chunks of at least 8 planes.
+// Many short waves balance CTAs of unequal cost (tiles cut by the grid's edge,
+// WENO5 faces gathered unevenly): on a 256 x 256 x 128 grid the FP64 kernel
+// runs fastest at about 9 waves (13-plane chunks), 3.5% faster than at 4.6
+// waves (26-plane chunks) and 10% faster than in one wave.
+int kchunk_for_waves(int ntiles, int nint, int slots, double waves) {
+  const int want = (int)std::ceil(waves * slots / ntiles);
+  const int nchunk = std::max(1, std::min(want, nint / 8));
+  return (nint + nchunk - 1) / nchunk;
+}
+
 // The default: about four CTAs per slot of 2 CTAs per SM, chunks of at least 8 planes.
 int kchunk_default(int ntiles, int nint, int nsm) {
   const int nchunk = std::max(1, std::min((4 * 2 * nsm + ntiles - 1) / ntiles, nint / 8));
@@ -154,12 +165,13 @@ int kchunk_default(int ntiles, int nint, int nsm) {
 
 // Candidate chunkings for cbns_autotune at `per_sm` CTAs per SM (distinct values).
 std::vector<int> kchunk_candidates(const cbns_ctx* c, int per_sm) {
-  const int ntiles = c->ntile_i * c->ntile_j, nint = c->d.KM - 2;
+  const int ntiles = c->ntile_i * c->ntile_j, nint = c->d.KM - 2, slots = c->nsm * per_sm;
   std::vector<int> v = {kchunk_default(ntiles, nint, c->nsm)};
-  for (double warm : {0.5, 2.0}) {
-    const int kc = kchunk_by_waves(ntiles, nint, c->nsm * per_sm, warm);
+  auto add = [&v](int kc) {
     if (std::find(v.begin(), v.end(), kc) == v.end()) v.push_back(kc);
-  }
+  };
+  for (double warm : {0.5, 2.0}) add(kchunk_by_waves(ntiles, nint, slots, warm));
+  for (double waves : {4.0, 6.0, 9.0, 12.0}) add(kchunk_for_waves(ntiles, nint, slots, waves));
   return v;
 }
 
@@ -1100,8 +1112,15 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaGetLastError();
-    c->kchunk = kchunk_default(ntiles, nint, c->nsm);
   }
+  // until cbns_autotune says otherwise, the variants and chunks it picks on
+  // B200 for grids of a few million nodes: FP64 stages by TMA (about 10%
+  // faster than the synchronous variant) and the split precision runs 2 CTAs
+  // per SM, both with about 9 waves of CTAs; the hybrid runs 3 per SM (8%
+  // faster than 2) with chunks sized by the wave count and warm-up
+  c->stage_variant = p->precision == CBNS_PREC_SPLIT ? 0 : 1;
+  c->kchunk = p->precision == CBNS_PREC_HYBRID ? kchunk_by_waves(ntiles, nint, c->nsm * 3, 0.5)
+                                               : kchunk_for_waves(ntiles, nint, c->nsm * 2, 9.0);
   stage_prepare();
   if (p->precision == CBNS_PREC_HYBRID) (void)weno_prepare();
   if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
@@ -1599,23 +1618,43 @@ int cbns_autotune(cbns_ctx* c, int* chosen) {
   }
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  int best = 0, best_kc = c->kchunk;
-  float best_ms = 1e30f;
-  for (int v = 0; v < nv; ++v) {
-    // FP32 variant v runs 2 + v CTAs per SM, the FP64 ones 2; each with its candidate k chunks
-    for (int kc : kchunk_candidates(c, fp32 ? 2 + v : 2)) {
-      c->stage_variant = v;
-      c->kchunk = kc;
-      const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
-      RET(stage_launch(c, a, 0));  // warm-up
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    g_last = "cudaEventCreate failed";
+    return CBNS_ERR_CUDA;
+  }
+  // the faster of two rounds of three RHS launches after one warm-up launch
+  auto time_it = [&](int v, int kc, float* ms) -> int {
+    c->stage_variant = v;
+    c->kchunk = kc;
+    const StageArgs a = stage_args(c, c->qb[c->lq], nullptr, nullptr, c->staging, false);
+    RET(stage_launch(c, a, 0));
+    *ms = 1e30f;
+    for (int round = 0; round < 2; ++round) {
       CK(cudaEventRecord(e0, c->stream));
       for (int r = 0; r < 3; ++r) RET(stage_launch(c, a, 0));
       CK(cudaEventRecord(e1, c->stream));
       CK(cudaEventSynchronize(e1));
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, e0, e1));
+      *ms = std::min(*ms, t);
+    }
+    return CBNS_OK;
+  };
+  // the context's current pair stays unless another is more than 1% faster:
+  // the candidates' RHS-only times differ by about that much where their full
+  // steps rank the other way
+  const int v0 = c->stage_variant, kc0 = c->kchunk;
+  int best = v0, best_kc = kc0, rc = CBNS_OK;
+  float best_ms = 0.f;
+  rc = time_it(v0, kc0, &best_ms);
+  for (int v = 0; v < nv && rc == CBNS_OK; ++v) {
+    // FP32 variant v runs 2 + v CTAs per SM, the FP64 ones 2; each with its candidate k chunks
+    for (int kc : kchunk_candidates(c, fp32 ? 2 + v : 2)) {
+      if (v == v0 && kc == kc0) continue;
       float ms = 0.f;
-      CK(cudaEventElapsedTime(&ms, e0, e1));
-      if (ms < best_ms) {
+      if ((rc = time_it(v, kc, &ms)) != CBNS_OK) break;
+      if (ms < 0.99f * best_ms) {
         best_ms = ms;
         best = v;
         best_kc = kc;
@@ -1627,6 +1666,7 @@ int cbns_autotune(cbns_ctx* c, int* chosen) {
   c->stage_variant = best;
   c->kchunk = best_kc;
   drop_graph(c);
+  if (rc != CBNS_OK) return rc;
   if (chosen) *chosen = best;
   return CBNS_OK;
 }
@@ -1646,6 +1686,19 @@ int cbns_stage_variant(cbns_ctx* c, int variant, int* count) {
     c->stage_variant = variant;
     drop_graph(c);
   }
+  return CBNS_OK;
+}
+
+int cbns_stage_kchunk(cbns_ctx* c, int kchunk, int* current) {
+  if (!c) return CBNS_ERR_ARG;
+  if (kchunk != -1) {
+    if (kchunk < 1 || kchunk > c->d.KM - 2) return CBNS_ERR_ARG;
+    if (kchunk != c->kchunk) {
+      c->kchunk = kchunk;
+      drop_graph(c);
+    }
+  }
+  if (current) *current = c->kchunk;
   return CBNS_OK;
 }
 

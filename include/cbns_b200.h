@@ -367,15 +367,22 @@ int cbns_batch_run(cbns_batch* batch, unsigned nsteps, double t_end, unsigned* s
 int cbns_batch_run_async(cbns_batch* batch, unsigned nsteps, double t_end);
 
 /* Pick, by timing on the current state, the fastest compiled variant of the
- * stage kernel for this context's precision (the state is not modified);
+ * stage kernel for this context's precision and its k chunk (the state is not
+ * modified; the current pair stays unless another is more than 1% faster);
  * *chosen (may be null) receives the variant index.  Later steps use it. */
 int cbns_autotune(cbns_ctx* ctx, int* chosen);
 /* Use compiled variant `variant` of the stage kernel (0 .. count-1; count from
  * *count when not null, variant -1 only queries it).  FP64: 0 stages each
  * plane synchronously, 1 by TMA (the same arithmetic, to the rounding of a
  * separate compilation); FP32:
- * 2 + variant CTAs per SM.  No counterpart in the reference. */
+ * 2 + variant CTAs per SM.  A new context starts on variant 1 (FP64, hybrid)
+ * or 0 (split).  No counterpart in the reference. */
 int cbns_stage_variant(cbns_ctx* ctx, int variant, int* count);
+/* Use k chunks of `kchunk` planes in the stage kernel's work items (one CTA
+ * per tile and chunk; 1 .. KM-2, -1 only queries); *current (may be null)
+ * receives the chunk in use.  cbns_autotune sets it with the variant.  No
+ * counterpart in the reference. */
+int cbns_stage_kchunk(cbns_ctx* ctx, int kchunk, int* current);
 
 /* Per-kernel-group device timing with CUDA events on the launch stream.  Group
  * ids: 0 stage (fused sweep + RK update), 1 boundary conditions, 2 viscous

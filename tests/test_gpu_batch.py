@@ -4,7 +4,8 @@ persistent work-queue launch of the stage kernel per RK stage.
 The batch computes what each block computes alone — the same stage arithmetic,
 boundary conditions and per-block time step — so after several steps every
 block's state and time equal those of the block run by itself: bit for bit for
-the plain (FP64) path; for the split and hybrid paths the state agrees to the
+the plain (FP64) path (the block alone on the synchronously staged variant,
+as the batched FP64 kernel stages); for the split and hybrid paths the state agrees to the
 FP32 rounding of the flux, and the hybrid's sensor decisions agree but for
 faces at the threshold (the batched stage and sensor kernels are separate
 compilations of the same source, free to contract their FP32 products into
@@ -27,6 +28,8 @@ WEIGHTS = Path(__file__).resolve().parents[1] / "cbns3d_cuda_b200" / "data" / "s
 def _block(case, precision, nudge=0.0):
     p = dict(case.params)
     b = Block(make_params(*case.shape, **p, precision=precision))
+    if precision == PREC_FP64:
+        b.stage_variant(0)  # the batched FP64 kernel stages each plane synchronously
     b.calc_metrics(case.x, case.y, case.z)
     b.set_conservative(case.Q0)
     if p.get("viscous"):

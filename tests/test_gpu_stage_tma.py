@@ -75,4 +75,25 @@ def test_stage_variant_arguments():
     from cbns3d_cuda_b200._abi import CbnsError
     with pytest.raises(CbnsError):
         b.stage_variant(2)
+    assert 1 <= b.stage_kchunk() <= 8
+    assert b.stage_kchunk(3) == 3 and b.stage_kchunk() == 3
+    for bad in (0, 9, -2):
+        with pytest.raises(CbnsError):
+            b.stage_kchunk(bad)
     b.close()
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_fp64_k_chunk_leaves_results_unchanged(variant):
+    """Every chunk computes its planes' fluxes from the same ring of planes,
+    so the chunking changes only the work split: the same states bit for bit."""
+    c = CASES["vortex_partial"]()
+    out = []
+    for kc in (-1, 3, 17):
+        b = _block(c, variant)
+        b.stage_kchunk(kc)
+        assert b.run(4) == 4
+        out.append((b.get_conservative(), b.get_time()[0]))
+        b.close()
+    for q, t in out[1:]:
+        assert np.array_equal(q, out[0][0]) and t == out[0][1]

@@ -33,6 +33,8 @@ step; N_upd = (IM-2)(JM-2)(KM-2).
           DGEMM measured in the same run.
   cpu_baseline  the FP64 CPU oracle (OpenMP, all host cores) on a bounded
           sample, with the host's CPU model.
+  config  the workload alone (case, grid, cell-updates per step), the same
+          in both arms' lines; how an arm computes it is under `path`.
 
 --impl reference runs the reference's own build (oracle/_ref, compiled from its
 sources) on the same case through its own executable and times it from its
@@ -97,6 +99,9 @@ def args():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-blocks pass of the default line")
     ap.add_argument("--no-reference-check", action="store_true",
                     help="skip the plain path's comparison with the reference build")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep each context's starting stage variant and k chunk (under a profiler the "
+                         "autotuner's timings mean nothing)")
     ap.add_argument("--sensor", default=str(ROOT / "cbns3d_cuda_b200" / "data" / "sensor_weights.npz"))
     return ap.parse_args()
 
@@ -180,6 +185,7 @@ class Clocks:
 
 
 SENSOR = None  # (params, tau) of the trained sensor network
+NO_AUTOTUNE = False  # --no-autotune: keep each context's starting stage variant
 
 
 def load_sensor(path):
@@ -210,6 +216,13 @@ def init_block(case, precision):
     return b
 
 
+def workload_config(wl, case, n):
+    """The `config` of both arms' lines: the workload alone (how each arm
+    computes it goes under `path`)."""
+    return {"workload": wl, "grid": list(case.shape), "cell_updates_per_step": n,
+            "l2": "inputs larger than L2 (the grid's state and metric arrays)"}
+
+
 def n_updates(case):
     IM, JM, KM = case.shape
     return (IM - 2) * (JM - 2) * (KM - 2)
@@ -232,7 +245,10 @@ def device_pass(case, precision, K, W, torch, dist, clocks=None, keep_state=Fals
     b = init_block(case, precision)
     stream = torch.cuda.Stream()  # a real stream: the legacy default stream cannot be graph-captured
     b.set_stream(stream.cuda_stream)
-    out = {"variant": b.autotune()}
+    if NO_AUTOTUNE:  # the context's own starting variant and k chunk
+        out = {"variant": None}
+    else:
+        out = {"variant": b.autotune()}
     out["kchunk"] = b.stage_kchunk()
     b.set_time(0.0)
     b.run(W)
@@ -476,14 +492,13 @@ def run_ours(a):
             "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": msh / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 flux / f64 state", "data": "synthetic",
-            "config": {"workload": wl,
-                       "path": "learned-sensor hybrid: per face WENO5-char or linear upwind-5 flux (FP32), "
-                               "FP64 state, metrics, dt; sensor MLP on tcgen05 (BF16) every 3rd step, decisions "
-                               "held and widened in between; audit every step on a rotating 1/97 sample of the "
-                               "linear faces",
-                       "grid": list(case.shape), "cell_updates_per_step": N, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (3 state buffers + 10 metric arrays)",
-                       "sensor": {"weights": os.path.relpath(a.sensor, ROOT), "tau": SENSOR[1]}},
+            "config": workload_config(wl, case, N),
+            "path": "learned-sensor hybrid: per face WENO5-char or linear upwind-5 flux (FP32), "
+                    "FP64 state, metrics, dt; sensor MLP on tcgen05 (BF16) every 3rd step, decisions "
+                    "held and widened in between; audit every step on a rotating 1/97 sample of the "
+                    "linear faces",
+            "parallelism": f"replicas x{world}",
+            "sensor": {"weights": os.path.relpath(a.sensor, ROOT), "tau": SENSOR[1]},
             "rho_l2_vs_fp64": l2_h, "rho_linf_vs_fp64": linf_h,
             "plain_vs_reference_linf": ref_cmp["max"] if ref_cmp else None,
             "paths": {"fp64": {"value": value64, "ms_per_step": ms64 / K, "stage_variant": p64["variant"], "stage_kchunk": p64["kchunk"],
@@ -554,8 +569,8 @@ def run_reference(a):
         "impl": "reference", "metric": metric, "value": v, "unit": "cell-updates/s", "n_gpus": 1, "steps": K,
         "warmup": W, "ms_per_step": 1e3 * sec / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": wl, "path": "reference CUDA build (FP64), its own executable and time loop",
-                   "grid": list(case.shape), "cell_updates_per_step": N, "parallelism": "single GPU"},
+        "config": workload_config(wl, case, N),
+        "path": "reference CUDA build (FP64), its own executable and time loop", "parallelism": "single GPU",
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
                          "sample": f"{K} steps of the reference executable (GPU kernels, one host thread), "
                                    f"Elapsed Time of a {W + K}-step run minus a {W}-step run"},
@@ -585,7 +600,7 @@ def run_to_tend(a):
         b = init_block(case, prec)
         stream = torch.cuda.Stream()
         b.set_stream(stream.cuda_stream)
-        variant = b.autotune()
+        variant = None if NO_AUTOTUNE else b.autotune()
         b.set_time(0.0)
         if prec == PREC_HYBRID:
             b.sensor_stats_reset()
@@ -796,6 +811,7 @@ def run_batch(a):
 
 if __name__ == "__main__":
     a = args()
+    NO_AUTOTUNE = a.no_autotune
     if a.impl == "reference":
         run_reference(a)
     elif a.case == "batch":

@@ -21,8 +21,7 @@
 //     calls that overlap on the GPU (from several host threads at once) race
 //     on the array and must be serialised by the caller;
 //   * the device address of the array is looked up once per device, on that
-//     device's first call (with the device current); make that first call
-//     before any stream capture begins;
+//     device's first call (with the device current);
 //   * a failure returns CBNS_ERR_CUDA and records the CUDA error text for
 //     cbns_status_string, as the other entry points do.
 #include <cuda_runtime.h>

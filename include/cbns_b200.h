@@ -239,9 +239,9 @@ int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f,
  * share that array (it keeps the last call's contents; every element a call
  * reads it first writes), so calls overlapping on the GPU race and must be
  * serialised by the caller.  The first call on each device looks up the
- * array's device address (with that device current); make it before any
- * stream capture begins.  A CUDA failure returns CBNS_ERR_CUDA with its text
- * in cbns_status_string.  No counterpart in the reference. */
+ * array's device address (with that device current).  A CUDA failure returns
+ * CBNS_ERR_CUDA with its text in cbns_status_string.  No counterpart in the
+ * reference. */
 #define CBNS_NOALLOC_MAX_POINTS 262144u
 int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM, const double* f,
                                double* fx, double* fy, double* fz);

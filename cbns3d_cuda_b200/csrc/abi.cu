@@ -1127,10 +1127,21 @@ int cbns_create(const cbns_params* p, cbns_ctx** out) {
   // B200 for grids of a few million nodes: FP64 stages by TMA (about 10%
   // faster than the synchronous variant) and the split precision runs 2 CTAs
   // per SM, both with about 9 waves of CTAs; the hybrid runs 3 per SM (8%
-  // faster than 2) with chunks sized by the wave count and warm-up
+  // faster than 2) with chunks sized by the wave count and warm-up -- where
+  // that gives at least two full waves of CTAs; a smaller hybrid grid keeps 2
+  // per SM (its CTAs do not fill the GPU, and the 2-per-SM kernel holds more
+  // in registers)
   c->stage_variant = p->precision == CBNS_PREC_SPLIT ? 0 : 1;
-  c->kchunk = p->precision == CBNS_PREC_HYBRID ? kchunk_by_waves(ntiles, nint, c->nsm * 3, 0.5)
-                                               : kchunk_for_waves(ntiles, nint, c->nsm * 2, 9.0);
+  c->kchunk = kchunk_for_waves(ntiles, nint, c->nsm * 2, 9.0);
+  if (p->precision == CBNS_PREC_HYBRID) {
+    const int kc3 = kchunk_by_waves(ntiles, nint, c->nsm * 3, 0.5);
+    if ((long)ntiles * ((nint + kc3 - 1) / kc3) >= 2L * 3 * c->nsm) {
+      c->kchunk = kc3;
+    } else {
+      c->stage_variant = 0;
+      c->kchunk = kchunk_default(ntiles, nint, c->nsm);
+    }
+  }
   stage_prepare();
   if (p->precision == CBNS_PREC_HYBRID) (void)weno_prepare();
   if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess) {

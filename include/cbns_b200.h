@@ -375,8 +375,9 @@ int cbns_autotune(cbns_ctx* ctx, int* chosen);
  * *count when not null, variant -1 only queries it).  FP64: 0 stages each
  * plane synchronously, 1 by TMA (the same arithmetic, to the rounding of a
  * separate compilation); FP32:
- * 2 + variant CTAs per SM.  A new context starts on variant 1 (FP64, hybrid)
- * or 0 (split).  No counterpart in the reference. */
+ * 2 + variant CTAs per SM.  A new context starts on variant 1 (FP64; hybrid
+ * grids of at least two waves of 3-per-SM CTAs) or 0 (split, smaller hybrid
+ * grids).  No counterpart in the reference. */
 int cbns_stage_variant(cbns_ctx* ctx, int variant, int* count);
 /* Use k chunks of `kchunk` planes in the stage kernel's work items (one CTA
  * per tile and chunk; 1 .. KM-2, -1 only queries); *current (may be null)

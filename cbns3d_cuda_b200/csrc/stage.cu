@@ -62,6 +62,11 @@ constexpr int NC = TI * TJ;     // 240 columns
 constexpr int NT = 256;         // threads
 constexpr int NFI = (TI + 1) * TJ;  // 255 i-faces
 constexpr int NFJ = TI * (TJ + 1);  // 256 j-faces
+// the face rounds' thread mapping (face_a, face_b in stage_body): one j-face
+// per thread; i-faces on 7 warps of two 16-face rows and one of a row and the
+// 15 faces of the last column
+static_assert(NFJ == NT && TI == 16 && TJ == 15, "face mapping of the face rounds");
+static_assert(NFI == 7 * 32 + 16 + TJ, "face mapping of the face rounds");
 constexpr int NSX = (TI + 2) * TJ;  // i-face nodes (i0-1 .. i0+16)
 constexpr int NSY = TI * (TJ + 2);  // j-face nodes (j0-1 .. j0+15)
 constexpr int NHI = 2 * H * TJ, NHJ = 2 * H * TI;  // halo nodes of a plane: i-halo, j-halo
@@ -215,6 +220,31 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
     } else {
       face_flux<R>(ld, nx, ny, nz, C, out);
     }
+  };
+
+  // The i-face (round A) and j-face (round B) of this thread: half-warps take
+  // 16 faces of one row each, the two halves of a warp rows 8 apart, so that
+  // their reads of a plane row (pitch 22 floats) start 16 banks apart: the
+  // face rounds' shared-memory reads take 720 wavefronts per plane instead of
+  // 1,104 with faces numbered row by row.  Round A: warps 0-6 take rows w and
+  // w+8, faces 0..15; warp 7 row 7 and the fx = 16 face of rows 0..14.
+  auto face_a = [&](int& fx, int& fy) -> bool {
+    const int w = t >> 5, l = t & 31;
+    if (w < 7) {
+      fx = l & 15;
+      fy = w + 8 * (l >> 4);
+    } else if (l < 16) {
+      fx = l;
+      fy = 7;
+    } else {
+      fx = TI;
+      fy = l - 16;
+    }
+    return fy < TJ;
+  };
+  auto face_b = [&](int& fx, int& fy) {
+    fx = t & 15;
+    fy = (t >> 5) + 8 * ((t >> 4) & 1);
   };
 
   // column owned by this thread
@@ -380,13 +410,15 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
   auto mask_bits = [&](int k) -> unsigned {
     unsigned m = 0;
     if constexpr (HYB) {
-      if (t < NFI) {
-        const int fx = t % (TI + 1), fy = t / (TI + 1), ga = ti0 + fx - 1, gj = tj0 + fy;
+      int fx, fy;
+      if (face_a(fx, fy)) {
+        const int ga = ti0 + fx - 1, gj = tj0 + fy;
         if (ga <= d.IM - 2 && gj <= d.JM - 2)
           m |= __ldg(a.mask + ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1))) != 0;
       }
       {
-        const int fx = t % TI, fy = t / TI, gi = ti0 + fx, ga = tj0 + fy - 1;
+        face_b(fx, fy);
+        const int gi = ti0 + fx, ga = tj0 + fy - 1;
         if (gi <= d.IM - 2 && ga <= d.JM - 2)
           m |= (unsigned)(__ldg(a.mask + nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1))) != 0)
                << 1;
@@ -400,12 +432,15 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
   };
   auto prefetch_weno = [&](int k, unsigned m) {
     if constexpr (HYB) {
+      int fx, fy;
       if (m & 1u) {
-        const int fx = t % (TI + 1), fy = t / (TI + 1), ga = ti0 + fx - 1, gj = tj0 + fy;
+        face_a(fx, fy);
+        const int ga = ti0 + fx - 1, gj = tj0 + fy;
         prefetch_l1(a.wflux + 8 * (ga + (long)(d.IM - 1) * ((gj - 1) + (long)(d.JM - 2) * (k - 1))));
       }
       if (m & 2u) {
-        const int fx = t % TI, fy = t / TI, gi = ti0 + fx, ga = tj0 + fy - 1;
+        face_b(fx, fy);
+        const int gi = ti0 + fx, ga = tj0 + fy - 1;
         prefetch_l1(a.wflux + 8 * (nfi + (gi - 1) + (long)(d.IM - 2) * (ga + (long)(d.JM - 1) * (k - 1))));
       }
       if (m & 4u) prefetch_l1(a.wflux + 8 * (nfi + nfj + (ci - 1) + (long)(d.IM - 2) * ((cj - 1) + (long)(d.JM - 2) * k)));
@@ -540,8 +575,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
 
     R fkp[5];
     // round A: i-faces.  Face fx (0..TI) of row fy lies between tile columns fx-1 and fx.
-    if (t < NFI) {
-      const int fx = t % (TI + 1), fy = t / (TI + 1);
+    int fx, fy;
+    if (face_a(fx, fy)) {
       const int ga = ti0 + fx - 1, gj = tj0 + fy;
       if (ga <= d.IM - 2 && gj <= d.JM - 2) {
         auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + H][fx + p + X0]; };
@@ -554,8 +589,8 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const StageMaps* 
       }
     }
     // round B: j-faces.  Face fy (0..TJ) of column fx lies between tile rows fy-1 and fy.
-    if (t < NFJ) {
-      const int fx = t % TI, fy = t / TI;
+    {
+      face_b(fx, fy);
       const int gi = ti0 + fx, ga = tj0 + fy - 1;
       if (gi <= d.IM - 2 && ga <= d.JM - 2) {
         auto ld = [&](int p, int n) -> R { return (R)sm.plane[n][fy + p][fx + H + X0]; };

@@ -16,7 +16,7 @@ from ._abi import (BC_CHARACTERISTIC, BC_FARFIELD, BC_OGRID, BC_REFERENCE, DTV_F
                    CBNS_Q, CBNS_QP, PREC_FP64, PREC_HYBRID, PREC_SPLIT,
                    VISDIV_CENTERED, VISDIV_REFERENCE, CbnsError, Params)
 
-__all__ = ["Block", "Batch", "Params", "CbnsError", "CBNS_Q", "CBNS_QP", "PREC_FP64", "PREC_SPLIT", "PREC_HYBRID",
+__all__ = ["selftest_waits", "Block", "Batch", "Params", "CbnsError", "CBNS_Q", "CBNS_QP", "PREC_FP64", "PREC_SPLIT", "PREC_HYBRID",
            "VISDIV_REFERENCE", "VISDIV_CENTERED", "BC_REFERENCE", "BC_FARFIELD", "BC_CHARACTERISTIC", "BC_OGRID", "OGRID_WRAP",
            "DTV_REFERENCE", "DTV_FULL",
            "make_params"]
@@ -300,3 +300,14 @@ def calc_gradient(f: np.ndarray):
     out = [np.empty_like(a) for _ in range(3)]
     _abi.check(lib.cbns_calc_gradient(IM, JM, KM, _abi.dptr(a), *[_abi.dptr(o) for o in out]), "cbns_calc_gradient")
     return [o.reshape(f.shape) for o in out]
+
+
+def selftest_waits() -> dict:
+    """Run the bounded waits' time-out path on the GPU (cbns_selftest_waits):
+    whether the tensor-core MMA wait and the TMA transaction wait each reported
+    a time-out on a barrier nothing completes, and how long each took."""
+    lib = _abi.load()
+    a, b = C.c_int(-1), C.c_int(-1)
+    sa, sb = C.c_double(), C.c_double()
+    _abi.check(lib.cbns_selftest_waits(C.byref(a), C.byref(b), C.byref(sa), C.byref(sb)), "cbns_selftest_waits")
+    return {"mma_timed_out": a.value, "tma_timed_out": b.value, "mma_seconds": sa.value, "tma_seconds": sb.value}

@@ -100,6 +100,8 @@ SIGNATURES = [
     ("cbns_autotune", C.c_int, [_V, C.POINTER(C.c_int)]),
     ("cbns_stage_variant", C.c_int, [_V, C.c_int, C.POINTER(C.c_int)]),
     ("cbns_stage_kchunk", C.c_int, [_V, C.c_int, C.POINTER(C.c_int)]),
+    ("cbns_selftest_waits", C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double)]),
     ("cbns_synchronize", C.c_int, [_V]),
     ("cbns_sensor_sample", C.c_int,
      [_V, C.c_int, C.c_uint, C.c_uint, _V, _V, _V, _V, C.c_uint, C.POINTER(C.c_uint)]),

@@ -72,9 +72,9 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar) {
 }
 
 // Wait for the given phase with an iteration limit; false on timeout.  Each
-// try_wait may suspend the thread for up to SUSPEND_NS before it returns
-// false, so the wait costs few instructions and is bounded by about
-// WAIT_LIMIT x SUSPEND_NS.
+// try_wait may suspend the thread (SUSPEND_NS is the hint) before it returns
+// false, so the wait costs few instructions; it is bounded by WAIT_LIMIT
+// tries (4.2 s measured on a B200, whose try_wait suspends about 4 us).
 constexpr unsigned SUSPEND_NS = 1000;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned phase) {
   const unsigned a = smem_u32(bar);

@@ -246,6 +246,16 @@ int cbns_calc_gradient(unsigned IM, unsigned JM, unsigned KM, const double* f,
 int cbns_calc_gradient_noalloc(unsigned IM, unsigned JM, unsigned KM, const double* f,
                                double* fx, double* fy, double* fz);
 
+/* Self-test of the bounded waits' time-out path (no counterpart in the
+ * reference): one GPU thread waits on an mbarrier that no MMA completes (the
+ * sensor's tensor-core wait, both of its windows) and on a TMA transaction
+ * barrier that no copy completes (the stage kernel's plane wait).
+ * *mma_timed_out and *tma_timed_out receive 1 when the wait reported its
+ * time-out, as it must; *mma_seconds and *tma_seconds (may be null) how long
+ * each took on the GPU's clock.  Nothing faults or stays in flight: the
+ * kernel returns and the device stays usable.  Synchronous. */
+int cbns_selftest_waits(int* mma_timed_out, int* tma_timed_out, double* mma_seconds, double* tma_seconds);
+
 /* Learned shock sensor (no counterpart in the reference).  A network of
  * CBNS_SENSOR_NIN inputs, two hidden layers of CBNS_SENSOR_NHID ReLU units and
  * one sigmoid output estimates, per grid face, the probability that the face

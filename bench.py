@@ -540,6 +540,14 @@ def run_ours(a):
         dist.destroy_process_group()
 
 
+def ref_loop_seconds(runs, W, K):
+    """Seconds of K reference steps: the shortest time loop of the (W+K)-step
+    runs minus the shortest of the W-step runs (runs: step count -> the
+    Elapsed Time of each run)."""
+    elapsed = {n: min(v) for n, v in runs.items()}
+    return max(elapsed[W + K] - elapsed[W], 1e-9)
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -569,8 +577,7 @@ def run_reference(a):
                     return
                 el = [float(l.split("=")[1]) for l in r.stdout.splitlines() if l.startswith("Elapsed Time")]
                 runs.setdefault(n, []).append(el[-1])
-    elapsed = {n: min(v) for n, v in runs.items()}
-    sec = max(elapsed[W + K] - elapsed[W], 1e-9)
+    sec = ref_loop_seconds(runs, W, K)
     v = N * K / sec
     print(json.dumps({
         "impl": "reference", "metric": metric, "value": v, "unit": "cell-updates/s", "n_gpus": 1, "steps": K,

@@ -365,7 +365,9 @@ def reference_state(case, nsteps, timeout=1800):
         return cases.read_checkpoint(d / "checkpoint.dat")[1]
 
 
-def cpu_baseline(case, budget_s=15.0):
+def cpu_baseline(case, budget_s=10.0, max_steps=100):
+    """The FP64 oracle on the host cores: whole RK3 steps of the case until
+    about budget_s seconds of CPU work (at most max_steps)."""
     from cbns3d_cuda_b200 import make_params
     from oracle import oracle as orc
     cores = os.cpu_count() or 1
@@ -378,7 +380,7 @@ def cpu_baseline(case, budget_s=15.0):
         rc, t, n = o.solve(1, 1e30, t)
         steps += 1
         el = time.perf_counter() - t0
-        if el >= budget_s or steps >= 3:
+        if el >= budget_s or steps >= max_steps:
             break
     o.close()
     return {"value": n_updates(case) * steps / el, "unit": "cell-updates/s", "cores": int(os.environ["OMP_NUM_THREADS"]),
@@ -488,7 +490,7 @@ def run_ours(a):
 
     weno_frac = stats["weno_faces"] / (K * stats["faces_per_step"]) if stats["faces_per_step"] else None
     if rank == 0:
-        cpu = None if a.no_cpu_baseline else cpu_baseline(case)
+        cpu = None if (a.no_cpu_baseline or world > 1) else cpu_baseline(case)  # rank 0 at N = 1 only
         line = {
             "metric": "cell-updates/s: learned-hybrid FP32 vs plain FP64 WENO5, same B200, rho-L2<=1e-5",
             "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": K, "warmup": W,
